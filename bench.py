@@ -1,0 +1,328 @@
+"""Benchmark of the sparse solve on the single-large-mesh workload
+(torus 512 x 256 = 131,072 vertices, 8 seams, 2% handles, U(-0.2, 0.2)
+displacements, 3 RHS): solves/sec at 1e-8 relative residual in the mixed
+FP32 / FP64-refinement form, with the plain FP64 GPU PCG and the fused FP64
+PCG beside it, the roofline of the persistent solve kernel, and the CPU FP64
+baseline (the oracle) timed on this host.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 (torchrun) every rank solves its own replica of the workload; the
+single mesh does not shard, so there is no collective on the data path.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = "torus512x256_8seams_2pct_handles_3rhs"
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def algorithmic_bytes(info, stats, k, mixed):
+    """Bytes a solve must move (formulas of the scope table): per inner PCG
+    iteration one SpMV, the two IC(0) sweeps and 9 vector passes; per FP64
+    residual evaluation one FP64 SpMV; plus the FP64 right-hand side."""
+    n, nnz = info["n_free"], info["nnz_A"]
+    nnz_l = info["nnz_L"] + n
+    sv = 4 if mixed else 8
+    sx = 4 if mixed else 8
+    b_spmv = nnz * (sv + 4) + 4 * (n + 1) + 2 * n * k * sx
+    b_ic = 2 * (nnz_l * (sv + 4) + 4 * (n + 1) + 2 * n * k * sx)
+    b_iter = b_spmv + b_ic + 9 * n * k * sx
+    b_res = nnz * 12 + 4 * (n + 1) + 3 * n * k * 8
+    b_rhs = info["nnz_K"] * 12 + 4 * (info["n_verts"] + 1) + n * k * 8
+    return stats.iterations * b_iter + (stats.refinements + 1) * b_res + b_rhs
+
+
+def cpu_baseline(pos, tris, h, t, seconds=12.0):
+    """The oracle's FP64 IC(0)-PCG (the reference's CPU path restated), columns
+    on parallel threads; bounded sample of whole solves."""
+    from oracle import oracle as O
+    ref = O.System(pos, tris, h)
+    threads = min(3, os.cpu_count() or 1)
+    n = 0
+    t0 = time.perf_counter()
+    while True:
+        st, x, it, rel = ref.solve(t, mode=1, tol=1e-8, threads=threads)
+        n += 1
+        el = time.perf_counter() - t0
+        if el > seconds or n >= 200:
+            break
+    return {"value": n / el, "unit": "solves/s", "cores": threads, "kind": "port",
+            "sample": f"{n} whole FP64 IC(0)-PCG solves of the workload to 1e-8 ({el:.1f} s)"}
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the oracle (the reference's CPU path restated; the
+    reference's own C++ runtime is not in its snapshot) on the host cores."""
+    if rank != 0:
+        return
+    from tool_godot_curvenet_b200 import cut_mesh, synth
+    m, h, t = synth.config2()
+    tris, parent = cut_mesh(m.positions.shape[0], m.tris, m.loops)
+    pos = m.positions[parent]
+    from oracle import oracle as O
+    ref = O.System(pos, tris, h)
+    threads = min(3, os.cpu_count() or 1)
+    for _ in range(args.warmup):
+        ref.solve(t, mode=1, tol=1e-8, threads=threads)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        ref.solve(t, mode=1, tol=1e-8, threads=threads)
+        times.append(time.perf_counter() - t0)
+    ms = 1e3 * sum(times) / len(times)
+    v = 1e3 / ms
+    line = {"impl": "reference", "metric": "solves/sec at 1e-8 rel. residual (mixed FP32+FP64 refinement)",
+            "value": v, "unit": "solves/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (seeded torus, see synth.config2)",
+            "config": {"workload": WORKLOAD, "parallelism": "host threads over RHS columns"},
+            "cpu_baseline": {"value": v, "unit": "solves/s", "cores": threads, "kind": "port",
+                             "sample": f"{args.steps} whole FP64 IC(0)-PCG solves"},
+            "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    import torch.distributed as dist
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    torch.cuda.set_device(local)
+
+    from tool_godot_curvenet_b200 import CutMeshSolver, cut_mesh, synth
+    from tool_godot_curvenet_b200 import _lib as L
+
+    m, h, t = synth.config2()
+    tris, parent = cut_mesh(m.positions.shape[0], m.tris, m.loops)
+    pos = np.ascontiguousarray(m.positions[parent])
+    solver = CutMeshSolver(pos, tris, h, device=local)
+    info = solver.info()
+    stream = torch.cuda.ExternalStream(solver.stream(), device=local)
+    nv, k = pos.shape[0], 3
+    d_t = torch.from_numpy(t).to(f"cuda:{local}")
+    d_x = torch.empty((nv, k), dtype=torch.float64, device=f"cuda:{local}")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")  # > L2 (126 MB)
+
+    def one(precision, algo="fused", stats=False):
+        return solver.solve_device(k, d_t.data_ptr(), d_x.data_ptr(), stats=stats, mode="deform",
+                                   precision=precision, algo=algo, tol=1e-8)
+
+    # reference statistics of each variant (deterministic: same inputs, cold start)
+    st_mixed = one("mixed", stats=True)
+    st_fp64 = one("fp64", stats=True)
+    st_plain = one("fp64", "plain", stats=True)
+    for s in (st_mixed, st_fp64, st_plain):
+        if s.status != 0:
+            raise SystemExit(f"solve failed: status {s.status}")
+
+    def timed(precision, algo, steps, warmup):
+        with torch.cuda.stream(stream):
+            for _ in range(warmup):
+                one(precision, algo)
+            evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+            torch.cuda.synchronize()
+            if world > 1:
+                dist.barrier()
+            torch.cuda.synchronize()
+            for a, b in evs:
+                flush.fill_(1)  # L2 flush between timed solves (outside the events)
+                a.record(stream)
+                one(precision, algo)
+                b.record(stream)
+            torch.cuda.synchronize()
+            if world > 1:
+                dist.barrier()
+            torch.cuda.synchronize()
+        return [a.elapsed_time(b) for a, b in evs]
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    t_mixed = timed("mixed", "fused", args.steps, args.warmup)
+    clk = clocks.stop()
+    t_fp64 = timed("fp64", "fused", max(3, args.steps // 3), 2)
+    t_plain = timed("fp64", "plain", 3, 1)
+
+    # e2e: host (pinned) buffers through cn_solve, H2D of the targets and D2H of
+    # the deformed positions inside the timed region
+    import ctypes as C
+    h_t = torch.from_numpy(t.copy()).pin_memory()
+    h_x = torch.empty((nv, k), dtype=torch.float64).pin_memory()
+    o = CutMeshSolver.make_opts(mode="deform", precision="mixed", tol=1e-8)
+    stt = L.SolveStats()
+    DP = C.POINTER(C.c_double)
+
+    def e2e_one():
+        return L.lib().cn_solve(solver._h, k, C.cast(h_t.data_ptr(), DP), None, C.cast(h_x.data_ptr(), DP),
+                                C.byref(o), C.byref(stt))
+    for _ in range(args.warmup):
+        e2e_one()
+    e2e_ms = []
+    with torch.cuda.stream(stream):
+        for _ in range(args.steps):
+            flush.fill_(1)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            rc = e2e_one()
+            b.record(stream)
+            b.synchronize()
+            if rc != 0:
+                raise SystemExit(f"cn_solve failed {rc}")
+            e2e_ms.append(a.elapsed_time(b))
+
+    def maxred(v):
+        if world == 1:
+            return v
+        tt = torch.tensor([v], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        return float(tt.item())
+
+    ms_mixed = maxred(sum(t_mixed) / len(t_mixed))
+    ms_fp64 = maxred(sum(t_fp64) / len(t_fp64))
+    ms_plain = maxred(sum(t_plain) / len(t_plain))
+    ms_e2e = maxred(sum(e2e_ms) / len(e2e_ms))
+    peak, peak_kind = load_peaks()
+    bytes_mixed = algorithmic_bytes(info, st_mixed, k, True)
+    bytes_fp64 = algorithmic_bytes(info, st_fp64, k, False)
+    ach = bytes_mixed / (ms_mixed * 1e-3) / 1e9
+    traffic = None
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            tj = json.load(f)
+        traffic = tj.get("cn_persistent_solve_mixed", {}).get("dram_bytes_per_launch")
+    except Exception:
+        pass
+    if rank == 0:
+        x = d_x.cpu().numpy()
+        line = {
+            "metric": "solves/sec at 1e-8 rel. residual (mixed FP32+FP64 refinement)",
+            "value": world * 1e3 / ms_mixed,
+            "unit": "solves/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms_mixed,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32 inner / f64 residual",
+            "data": "synthetic (seeded torus, see tool_godot_curvenet_b200/synth.py config2)",
+            "config": {"workload": WORKLOAD, "n_verts": nv, "n_free": info["n_free"], "nnz_A": info["nnz_A"],
+                       "rhs": k, "tol": 1e-8, "precond": "IC(0), greedy-colour order",
+                       "n_levels": info["n_levels"], "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                       "l2": "flushed (256 MB write) before every timed solve, outside the events"},
+            "mixed": {"iterations": st_mixed.iterations, "refinements": st_mixed.refinements,
+                      "max_rel_residual": st_mixed.max_rel_residual},
+            "fp64_fused": {"solves_per_s": 1e3 / ms_fp64, "ms": ms_fp64, "iterations": st_fp64.iterations,
+                           "max_rel_residual": st_fp64.max_rel_residual},
+            "fp64_plain": {"solves_per_s": 1e3 / ms_plain, "ms": ms_plain, "iterations": st_plain.iterations,
+                           "note": "Jacobi-PCG, one kernel per primitive, dots folded on the host each iteration"},
+            "speedup_mixed_vs_fp64_plain": ms_plain / ms_mixed,
+            "speedup_mixed_vs_fp64_fused": ms_fp64 / ms_mixed,
+            "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                         "peak_kind": peak_kind, "traffic": traffic,
+                         "kernel": "k_solve_grid<float,3,4> (persistent solve)",
+                         "algorithmic_bytes_per_launch": bytes_mixed,
+                         "fp64_fused_achieved": bytes_fp64 / (ms_fp64 * 1e-3) / 1e9},
+            "e2e": {"value": world * 1e3 / ms_e2e, "unit": "solves/s", "h2d_bytes_per_step": int(h_t.numel() * 8),
+                    "d2h_bytes_per_step": int(h_x.numel() * 8)},
+            "gpu_launches": args.steps,
+            "clocks": clk,
+            "checksum": float(np.abs(x).sum()),
+        }
+        if not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(pos, tris, h, t)
+        print(json.dumps(line), flush=True)
+    solver.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

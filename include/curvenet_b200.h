@@ -1,0 +1,152 @@
+/* curvenet_b200.h -- C ABI of the B200 (sm_100a) sparse solve of the
+ * profile-curves deformer: cut-mesh cotangent-Laplacian assembly into CSR,
+ * IC(0) / Jacobi / HSC preconditioned CG in FP64 or FP32-with-FP64-refinement,
+ * the deform (Stage 2) and harmonic solves, batched solves and the adjoint.
+ *
+ * The reference's C++ runtime headers (src/curvenet/sparse_linalg.h,
+ * incomplete_cholesky.h, hierarchical_sparsify.h, cut_mesh_laplacian.h,
+ * harmonic_solve.h, deform_solve.h, gpu_cg_solver.h, gpu_cg_multi_solver.h)
+ * are not part of the reference snapshot; the Lean specification states that
+ * it mirrors them 1:1 (lean/Curvenet/SparseLinAlg.lean:24,
+ * lean/Curvenet/HalfedgeBuilder.lean:4).  Each entry point below cites the
+ * Lean function whose behaviour it takes over.
+ *
+ * Conventions: plain pointers and sizes only; every array is row-major;
+ * host arrays belong to the caller; a cn_handle owns its device memory, its
+ * CUDA stream, the factor and the warm-start state.  A handle is not
+ * thread-safe; distinct handles may be used from distinct threads.  Errors
+ * are status codes, never aborts.
+ */
+#ifndef CURVENET_B200_H
+#define CURVENET_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  CN_OK = 0,
+  CN_MAX_ITER = 1,            /* tolerance not reached within max_iter / max_refine */
+  CN_SINGULAR_COMPONENT = 2,  /* a connected component of the cut mesh has no handle */
+  CN_NONPOS_PIVOT = 3,        /* IC(0) pivot <= 0 and the diagonal-shift retries ran out */
+  CN_NAN = 4,                 /* non-finite input or iterate */
+  CN_BREAKDOWN = 5,           /* p.Ap <= 0 inside PCG */
+  CN_TIMEOUT = 6,             /* a bounded device-side wait ran out */
+  CN_BAD_INPUT = 7,
+  CN_CUDA_ERROR = 8,
+  CN_NO_DEVICE = 9
+} cn_status;
+
+typedef struct cn_system* cn_handle;
+typedef struct cn_batch* cn_batch_handle;
+
+/* Cut mesh: triangles on the cut vertex index space (seam vertices already
+ * duplicated), CCW, and the Dirichlet handle vertices. */
+typedef struct {
+  int32_t n_verts;
+  int32_t n_tris;
+  const double* positions; /* n_verts x 3 rest positions */
+  const int32_t* tris;     /* n_tris x 3 */
+  int32_t n_handles;
+  const int32_t* handles;  /* n_handles distinct vertex ids */
+} cn_mesh_desc;
+
+enum { CN_PRECOND_JACOBI = 0, CN_PRECOND_IC0 = 1, CN_PRECOND_HSC = 2 };
+enum { CN_ORDER_NATURAL = 0, CN_ORDER_COLOR = 1 };
+enum { CN_LAPLACIAN_COT = 0, CN_LAPLACIAN_ROBUST = 1 };
+enum { CN_PREC_FP64 = 0, CN_PREC_MIXED = 1 };
+enum { CN_MODE_HARMONIC = 0, CN_MODE_DEFORM = 1, CN_MODE_RHS = 2 };
+enum { CN_ALGO_FUSED = 0, CN_ALGO_PLAIN = 1 };
+
+typedef struct {
+  int32_t precond;       /* CN_PRECOND_* (default IC0) */
+  int32_t ordering;      /* CN_ORDER_* elimination order of IC(0) (default COLOR) */
+  int32_t laplacian;     /* CN_LAPLACIAN_* (default COT) */
+  double mollify_delta;  /* delta of the robust (mollified) Laplacian */
+  int32_t device;        /* CUDA device ordinal */
+  int32_t max_rhs;       /* largest k a solve will use (1..9), sizes the work vectors */
+  int32_t tune;          /* 1: autotune the launch shape for this system (cached) */
+  int32_t lanes;         /* 0: default/tuned; else lanes per row (1,2,4,8,16) */
+  int32_t block;         /* 0: default/tuned; else threads per block */
+  int32_t grid;          /* 0: default/tuned; else blocks of the persistent solve */
+} cn_build_opts;
+
+typedef struct {
+  int32_t precision;   /* CN_PREC_FP64 or CN_PREC_MIXED */
+  int32_t mode;        /* CN_MODE_HARMONIC, CN_MODE_DEFORM (targets) or CN_MODE_RHS */
+  int32_t algo;        /* CN_ALGO_FUSED (one persistent launch) or CN_ALGO_PLAIN */
+  double tol;          /* relative residual ||b - A x|| / ||b|| per column */
+  int32_t max_iter;    /* inner PCG iterations per refinement step */
+  int32_t max_refine;  /* FP64 residual refinements (mixed precision) */
+  double inner_tol;    /* mixed precision: inner relative tolerance */
+  int32_t warm_start;  /* 1: start from this handle's previous solution */
+} cn_solve_opts;
+
+typedef struct {
+  int32_t status;
+  int32_t iterations;    /* inner PCG iterations summed over refinements */
+  int32_t refinements;   /* FP64 residual evaluations after the first */
+  int32_t k;
+  double rel_residual[32]; /* final true relative residual of the first 32 columns */
+  double max_rel_residual;
+  double device_ms;      /* device time of the solve (CUDA events) */
+} cn_solve_stats;
+
+void cn_default_build_opts(cn_build_opts* o);
+void cn_default_solve_opts(cn_solve_opts* o);
+const char* cn_status_string(int32_t status);
+/* Text of the last error on this thread ("" if none). */
+const char* cn_last_error(void);
+
+/* Seam cut of an uncut triangle mesh along closed vertex loops.  Each loop
+ * vertex gets a copy (ids n_verts, n_verts+1, ... in loop order) and the
+ * faces on the left of the loop at that vertex move to the copy.  Host only.
+ * Replaces the cut-mesh construction of CutAlgorithm.lean:49-255 /
+ * CutMesh.lean:39-79 for profile-curve seams along mesh edges.
+ * tris_out: n_tris x 3; parent_out: capacity n_verts + total loop length. */
+cn_status cn_cut_mesh(int32_t n_verts, int32_t n_tris, const int32_t* tris, int32_t n_loops,
+                      const int32_t* loop_ptr, const int32_t* loop_verts, int32_t* tris_out,
+                      int32_t* parent_out, int32_t* n_verts_out);
+
+/* Assemble K = V^T L_h V (CutMeshLaplacian.lean:86-93) into CSR on the GPU,
+ * reduce to the free unknowns, order, and factor (IncompleteCholesky.lean:30-33;
+ * SlangCodegen/IncompleteCholesky.lean:9-12 for the level/colour schedule). */
+cn_status cn_build(const cn_mesh_desc* mesh, const cn_build_opts* opts, cn_handle* out);
+void cn_destroy(cn_handle h);
+
+/* Solve for k right-hand sides with host buffers.  targets: n_handles x k
+ * (modes HARMONIC/DEFORM) or, for CN_MODE_RHS, the free-row right-hand side
+ * n_free x k in vertex order of cn_export_csr's free_of.  x0 (nullable):
+ * n_verts x k initial guess.  x_out: n_verts x k with handles overlaid.
+ * HARMONIC = HarmonicSolve.lean:51-66 solveMulti; DEFORM = DeformSolve.lean:
+ * 123-135 Stage 2 with F_f = I; the PCG follows SparseLinAlg.lean:104-163. */
+cn_status cn_solve(cn_handle h, int32_t k, const double* targets, const double* x0,
+                   double* x_out, const cn_solve_opts* opts, cn_solve_stats* stats);
+
+/* Same with device buffers, enqueued on the handle's stream.  With stats ==
+ * NULL the call does not synchronise. */
+cn_status cn_solve_device(cn_handle h, int32_t k, const double* d_targets, double* d_x_out,
+                          const cn_solve_opts* opts, cn_solve_stats* stats);
+
+/* The handle's cudaStream_t. */
+void* cn_stream(cn_handle h);
+
+/* info[0..11] = n_free, nnz_A, nnz_L(strict), n_levels, nnz_K, n_verts,
+ * n_handles, grid, block, lanes, n_colors, device bytes held. */
+cn_status cn_system_info(cn_handle h, int64_t* info);
+
+/* Export the reduced matrix A = K[free, free] in solve order (free_of: row ->
+ * vertex), the IC(0) factor (rows: strictly-lower entries then the diagonal,
+ * the layout of IncompleteCholesky.lean factor3) and K over all vertices. */
+cn_status cn_export_csr(cn_handle h, int32_t* free_of, int32_t* rowptr, int32_t* colidx,
+                        double* vals);
+cn_status cn_export_factor(cn_handle h, int32_t* rowptr, int32_t* colidx, double* vals);
+cn_status cn_export_k(cn_handle h, int32_t* rowptr, int32_t* colidx, double* vals);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CURVENET_B200_H */

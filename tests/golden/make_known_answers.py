@@ -1,0 +1,215 @@
+"""Writes tests/golden/known_answers.json: the known-answer fixtures of the
+reference's own `native_decide` examples for the sparse-solve path.
+
+Each record carries the Lean file:line it comes from (relative to the
+reference project root), its inputs, the expected values and the tolerance
+the example states.  Values that the Lean examples state analytically
+(1/sqrt 3, sqrt 3 / 2, ...) are computed here in binary64.  Run:
+
+    python tests/golden/make_known_answers.py
+"""
+import json
+import math
+import os
+
+S3 = math.sqrt(3.0)
+TRI = [[0.0, 0.0, 0.0], [1.0, 0.0, 0.0], [0.5, 0.0, 0.8660254037844386]]
+SQUARE = [[0.0, 0.0, 0.0], [1.0, 0.0, 0.0], [1.0, 0.0, 1.0], [0.0, 0.0, 1.0]]
+PENT = [[math.cos(6.283185307179586 * k / 5.0), 0.0, math.sin(6.283185307179586 * k / 5.0)] for k in range(5)]
+STRIP = [[0.0, 0.0, 0.0], [1.0, 0.0, 0.0], [0.5, 0.0, 0.8660254037844386], [1.5, 0.0, 0.8660254037844386]]
+
+# Halfedge.lean:345-396 (target, twin, next, face); -1 = none
+HE_TRIANGLE = [[1, 5, 1, 0], [2, 4, 2, 0], [0, 3, 0, 0], [2, 2, 4, -1], [1, 1, 5, -1], [0, 0, 3, -1]]
+HE_QUAD = [[1, 7, 1, 0], [2, 6, 2, 0], [3, 5, 3, 0], [0, 4, 0, 0],
+           [3, 3, 5, -1], [2, 2, 6, -1], [1, 1, 7, -1], [0, 0, 4, -1]]
+HE_STRIP = [[1, 7, 1, 0], [2, 3, 2, 0], [0, 6, 0, 0], [1, 1, 4, 1], [3, 9, 5, 1], [2, 8, 3, 1],
+            [2, 2, 8, -1], [0, 0, 6, -1], [3, 5, 9, -1], [1, 4, 7, -1]]
+
+LAP4 = dict(rowPtr=[0, 2, 5, 8, 10], colIdx=[0, 1, 0, 1, 2, 1, 2, 3, 2, 3],
+            values=[2.0, -1.0, -1.0, 2.0, -1.0, -1.0, 2.0, -1.0, -1.0, 2.0])
+LAP4_DENSE = [2.0, -1.0, 0.0, 0.0, -1.0, 2.0, -1.0, 0.0, 0.0, -1.0, 2.0, -1.0, 0.0, 0.0, -1.0, 2.0]
+
+
+def rec(src, kind, **kw):
+    d = dict(src=src, kind=kind)
+    d.update(kw)
+    return d
+
+
+def main():
+    out = []
+    # ---------------------------------------------------------------- Laplacians
+    out += [
+        rec("PolygonLaplacian.lean:144-147", "tri_rowsum", pts=TRI, eps=1e-12),
+        rec("PolygonLaplacian.lean:149-152", "tri_symmetric", pts=TRI, eps=1e-12),
+        rec("PolygonLaplacian.lean:154-158", "tri_offdiag01", pts=TRI, expected=-1.0 / (2.0 * S3), eps=1e-12),
+        rec("PolygonLaplacian.lean:160-163", "poly_rowsum", pts=SQUARE, eps=1e-12),
+        rec("PolygonLaplacian.lean:165-168", "poly_symmetric", pts=SQUARE, eps=1e-12),
+        rec("PolygonLaplacian.lean:170-173", "poly_rowsum", pts=PENT, eps=1e-9),
+        rec("PolygonLaplacian.lean:175-178", "poly_symmetric", pts=PENT, eps=1e-9),
+        rec("RobustLaplacian.lean:168-170", "mollify_zero", delta=0.0, e=[1.0, 1.0, 1.0], eps=1e-12),
+        rec("RobustLaplacian.lean:172-175", "mollify_zero", delta=0.01, e=[1.0, 1.0, 1.0], eps=1e-12),
+        rec("RobustLaplacian.lean:177-186", "mollify_positive", delta=0.05, e=[1.0, 1.0, 1.99]),
+        rec("RobustLaplacian.lean:188-202", "mollify_margin", delta=0.05, e=[1.0, 1.0, 1.99], tol=1e-12),
+        rec("RobustLaplacian.lean:204-209", "cot_from_lengths", e=[1.0, 1.0, 1.0], expected=1.0 / S3, eps=1e-12),
+        rec("RobustLaplacian.lean:211-216", "cot_from_lengths", e=[1.0, S3, 2.0], expected=S3, eps=1e-9),
+        rec("RobustLaplacian.lean:218-223", "cot_from_lengths", e=[S3, 1.0, 2.0], expected=1.0 / S3, eps=1e-9),
+        rec("RobustLaplacian.lean:225-229", "cot_from_lengths", e=[2.0, 1.0, S3], expected=0.0, eps=1e-9),
+        rec("RobustLaplacian.lean:231-244", "robust_equals_embedded", pts=TRI, delta=0.0, eps=1e-12),
+        rec("RobustLaplacian.lean:246-250", "robust_rowsum", pts=TRI, delta=0.0, eps=1e-12),
+        rec("RobustLaplacian.lean:252-256", "robust_symmetric", pts=TRI, delta=0.0, eps=1e-12),
+        rec("RobustLaplacian.lean:258-276", "robust_finite",
+            pts=[[0.0, 0.0, 0.0], [1.0, 0.0, 0.0], [1.999999, 0.0, 0.0]], delta=0.01),
+    ]
+    # ---------------------------------------------------------------- topology
+    out += [
+        rec("Halfedge.lean:402-404", "manifold", nv=3, nf=1, he=HE_TRIANGLE),
+        rec("Halfedge.lean:402-404", "manifold", nv=4, nf=1, he=HE_QUAD),
+        rec("Halfedge.lean:402-404", "manifold", nv=4, nf=2, he=HE_STRIP),
+        rec("HalfedgeBuilder.lean:115-119", "builder", nv=3, tris=[[0, 1, 2]], n_he=6, nf=1),
+        rec("HalfedgeBuilder.lean:121-126", "builder", nv=4, tris=[[0, 1, 2], [2, 1, 3]], n_he=10, nf=2),
+        rec("HalfedgeBuilder.lean:128-136", "builder", nv=4, tris=[[0, 1, 2], [0, 2, 3], [0, 3, 1], [1, 3, 2]],
+            n_he=12, nf=4, all_twins=True),
+        rec("CutAlgorithm.lean:270-291", "surgery", base="triangle", ops=[["subdivide", 0]],
+            nv=4, n_he=8, nf=1, loops=[[0, 4]]),
+        rec("CutAlgorithm.lean:293-298", "surgery", base="quad", ops=[["subdivide", 0]], nv=5, n_he=10, nf=1),
+        rec("CutAlgorithm.lean:300-306", "surgery", base="triangle", ops=[["subdivide", 0], ["subdivide", 1]],
+            nv=5, n_he=10, nf=1),
+        rec("CutAlgorithm.lean:323-351", "surgery", base="quad", ops=[["split", 0, 2]],
+            nv=4, n_he=10, nf=2, loops=[[1, 3], [0, 3]]),
+        rec("CutAlgorithm.lean:362-370", "surgery", base="quad", ops=[["subdivide", 0], ["split", 1, 3]],
+            nv=5, n_he=12, nf=2),
+        rec("CutAlgorithm.lean:420-456", "surgery", base="triangle", ops=[["crack", 0]],
+            nv=4, n_he=8, nf=1, loops=[[0, 5]], crack=[6, 7]),
+        rec("CutAlgorithm.lean:462-507", "surgery", base="strip", ops=[["subdivide", 1], ["split", 2, 1], ["split", 3, 4]],
+            nv=5, n_he=16, nf=4, loops=[[0, 3]]),
+        rec("CutMesh.lean:157-164", "partition", he=HE_TRIANGLE, vkind=[0, 0, 0], expected=True),
+        rec("CutMesh.lean:157-164", "partition", he=HE_QUAD, vkind=[0, 0, 0, 0], expected=True),
+        rec("CutMesh.lean:187-188", "partition", he=HE_TRIANGLE, vkind=[1, 0, 0], expected=True),
+    ]
+    # ---------------------------------------------------------------- V^T L_h V
+    out += [
+        rec("CutMeshLaplacian.lean:305-316", "vtlhv", he=HE_TRIANGLE, nv=3, nf=1, vkind=[0, 0, 0], pos=TRI,
+            eps_rowsum=1e-12, eps_sym=1e-12),
+        rec("CutMeshLaplacian.lean:318-329", "vtlhv", he=HE_QUAD, nv=4, nf=1, vkind=[0, 0, 0, 0], pos=SQUARE,
+            eps_rowsum=1e-12, eps_sym=1e-12),
+        rec("CutMeshLaplacian.lean:339-350", "vtlhv", he=HE_STRIP, nv=4, nf=2, vkind=[0, 0, 0, 0], pos=STRIP,
+            eps_rowsum=1e-10, eps_sym=1e-10),
+        rec("CutMeshLaplacian.lean:352-361", "vtlhv", he=HE_TRIANGLE, nv=3, nf=1, vkind=[1, 0, 0], pos=TRI,
+            eps_sym=1e-10),
+    ]
+    # ---------------------------------------------------------------- dense LA
+    out += [
+        rec("DenseLinAlg.lean:297-302", "dense_solve", A=[1, 0, 0, 0, 1, 0, 0, 0, 1], b=[1, 2, 3], x=[1, 2, 3], eps=1e-12),
+        rec("DenseLinAlg.lean:305-312", "dense_solve", A=[2, 0, 0, 0, 3, 0, 0, 0, 4], b=[4, 9, 16], x=[2, 3, 4], eps=1e-12),
+        rec("DenseLinAlg.lean:314-319", "dense_solve", A=[2, 1, 1, 2], b=[3, 3], x=[1, 1], eps=1e-12),
+        rec("DenseLinAlg.lean:321-327", "dense_solve", A=[0, 1, 1, 0], b=[2, 3], x=[3, 2], eps=1e-12),
+        rec("DenseLinAlg.lean:329-338", "dense_residual", A=[2, 0, 1, 0, 3, 0, 1, 0, 4], b=[5, 6, 9], eps=1e-10),
+        rec("DenseLinAlg.lean:365-404", "lu_solve", A=[2, 1, 1, 2], b=[3, 3], x=[1, 1], eps=1e-12),
+        rec("DenseLinAlg.lean:396-404", "lu_solve", A=[0, 1, 1, 0], b=[2, 3], x=[3, 2], eps=1e-12),
+        rec("DenseLinAlg.lean:431-442", "lu_vs_ge", A=[4, 3, 0, 6, 3, 0, 0, 0, 1], b=[7, 9, 1], eps=1e-10),
+        rec("DenseLinAlg.lean:444-452", "cholesky", A=[4, 2, 2, 3], L=[2, 0, 1, math.sqrt(2.0)], eps=1e-12),
+        rec("DenseLinAlg.lean:463-472", "cholesky_solve", A=[4, 2, 2, 3], b=[10, 8], x=[1.75, 1.5], eps=1e-12),
+        rec("DenseLinAlg.lean:486-490", "cholesky_solve", A=[4, 2, 2, 3], b=[4, 3], x=[0.75, 0.5], eps=1e-12),
+        rec("DenseLinAlg.lean:474-483", "cholesky_vs_ge", A=LAP4_DENSE, b=[1, 0, 0, 0], eps=1e-10),
+    ]
+    # ---------------------------------------------------------------- CG (SparseLinAlg)
+    I3 = dict(rowPtr=[0, 1, 2, 3], colIdx=[0, 1, 2], values=[1.0, 1.0, 1.0])
+    D234 = dict(rowPtr=[0, 1, 2, 3], colIdx=[0, 1, 2], values=[2.0, 3.0, 4.0])
+    SPD2 = dict(rowPtr=[0, 2, 4], colIdx=[0, 1, 0, 1], values=[2.0, 1.0, 1.0, 2.0])
+    F07 = dict(rowPtr=[0, 2, 5, 7], colIdx=[0, 1, 0, 1, 2, 1, 2], values=[4.0, -1.0, -1.0, 4.0, -1.0, -1.0, 4.0])
+    out += [
+        rec("SparseLinAlg.lean:183-186", "spmv", A=I3, x=[1.0, 2.0, 3.0], y=[1.0, 2.0, 3.0], eps=1e-12),
+        rec("SparseLinAlg.lean:189-192", "cg", A=I3, b=[1.0, 2.0, 3.0], max_iter=10, tol=1e-12, x=[1.0, 2.0, 3.0], eps=1e-9),
+        rec("SparseLinAlg.lean:203-206", "cg", A=D234, b=[4.0, 9.0, 16.0], max_iter=10, tol=1e-12, x=[2.0, 3.0, 4.0], eps=1e-9),
+        rec("SparseLinAlg.lean:217-220", "cg", A=SPD2, b=[3.0, 3.0], max_iter=50, tol=1e-12, x=[1.0, 1.0], eps=1e-8),
+        rec("SparseLinAlg.lean:243-246", "cg", A=LAP4, b=[1.0, 0.0, 0.0, 0.0], max_iter=200, tol=1e-12,
+            x=[0.8, 0.6, 0.4, 0.2], eps=1e-7),
+        rec("SparseLinAlg.lean:251-260", "cg_vs_dense", A=LAP4, A_dense=LAP4_DENSE, b=[1.0, 2.0, 3.0, 4.0],
+            max_iter=200, tol=1e-12, eps=1e-7),
+        rec("SparseLinAlg.lean:265-269", "cg_warm_vs_cold", A=LAP4, b=[1.0, 2.0, 3.0, 4.0], x0=[0.0, 0.0, 0.0, 0.0],
+            max_iter=200, tol=1e-12, eps=1e-9),
+        rec("SparseLinAlg.lean:275-279", "cg_warm_exact", A=LAP4, b=[1.0, 0.0, 0.0, 0.0], x0=[0.8, 0.6, 0.4, 0.2],
+            max_iter=0, tol=1e-9, eps=1e-9),
+        rec("SparseLinAlg.lean:283-287", "cg_warm_vs_cold", A=LAP4, b=[1.0, 2.0, 3.0, 4.0], x0=[3.9, 6.9, 8.9, 6.9],
+            max_iter=200, tol=1e-12, eps=1e-7),
+        rec("Features/KnownKnowns/SolverKernels.lean:9-18", "cg_residual", A=F07, b=[1.0, 0.0, -1.0], max_iter=100,
+            tol=1e-12, rr_max=1e-9),
+    ]
+    # ---------------------------------------------------------------- IC(0)
+    ATRI = dict(rowPtr=[0, 2, 5, 7], colIdx=[0, 1, 0, 1, 2, 1, 2], values=[4.0, -1.0, -1.0, 4.0, -1.0, -1.0, 4.0])
+    AWIDE = dict(rowPtr=[0, 2, 5, 7], colIdx=[0, 1, 0, 1, 2, 1, 2],
+                 values=[1.0e-2, 1.0e-3, 1.0e-3, 1.0e0, 1.0e-2, 1.0e-2, 1.0e4])
+    out += [
+        rec("IncompleteCholesky.lean:142-151", "ic0_llt", A=ATRI, eps=1e-12),
+        rec("IncompleteCholesky.lean:153-166", "ic0_solve", A=ATRI, b=[3.0, 2.0, 5.0], eps=1e-10),
+        rec("IncompleteCholesky.lean:182-186", "ic0_llt", A=AWIDE, eps=1e-9),
+    ]
+    # ---------------------------------------------------------------- HSC
+    path3 = [[0, 1, 1.0], [1, 2, 2.0]]
+    star4 = [[0, 1, 1.0], [0, 2, 2.0], [0, 3, 3.0]]
+    tpl = [[0, 1, 1.0], [0, 2, 1.0], [1, 2, 1.0], [0, 3, 4.0]]
+    out += [
+        rec("HierarchicalSparsifyCompensate.lean:404-411", "hsc", edges=path3, elim=[1], n_edges=1,
+            weights=[[0, 2, 2.0 / 3.0]], eps=1e-12),
+        rec("HierarchicalSparsifyCompensate.lean:425-439", "hsc", edges=star4, elim=[0], n_edges=3,
+            weights=[[1, 2, 1.0 / 3.0], [1, 3, 0.5], [2, 3, 1.0]], eps=1e-12),
+        rec("HierarchicalSparsifyCompensate.lean:454-460", "hsc", edges=tpl, elim=[0],
+            weights=[[1, 2, 1.0 + 1.0 / 6.0], [1, 3, 4.0 / 6.0]], eps=1e-12),
+        rec("HierarchicalSparsifyCompensate.lean:466-470", "hsc", edges=[[0, 1, 1.5]], elim=[2], n_edges=1,
+            weights=[[0, 1, 1.5]], eps=1e-12),
+        rec("HierarchicalSparsifyCompensate.lean:475-479", "hsc", edges=path3, elim=[1, 0], n_edges=0, eps=1e-12),
+        rec("HierarchicalSparsifyCompensate.lean:485-488", "hsc", edges=star4, elim=[0], degree=[1, 5.0 / 6.0], eps=1e-12),
+    ]
+    # ---------------------------------------------------------------- colouring
+    out += [
+        rec("GraphColoring.lean:363-370", "color", adj=[[1, 2], [0, 2], [0, 1]], n_colors=3),
+        rec("GraphColoring.lean:372-379", "color", adj=[[1, 3], [0, 2], [1, 3], [0, 2]], n_colors=2),
+        rec("GraphColoring.lean:381-388", "color", adj=[[1], [0, 2], [1, 3], [2, 4], [3]], n_colors=2),
+        rec("GraphColoring.lean:390-397", "color", adj=[[1, 2, 3, 4], [0], [0], [0], [0]], n_colors=2),
+    ]
+    # ---------------------------------------------------------------- harmonic / deform solves
+    I9 = [1.0, 0.0, 0.0, 0.0, 1.0, 0.0, 0.0, 0.0, 1.0]
+    RZ = [0.0, -1.0, 0.0, 1.0, 0.0, 0.0, 0.0, 0.0, 1.0]
+    S2 = [2.0, 0.0, 0.0, 0.0, 2.0, 0.0, 0.0, 0.0, 2.0]
+    tws = dict(he=HE_TRIANGLE, nv=3, nf=1, tris=[[0, 1, 2]], sample_col=[0, -1, -1], pos=TRI, handles=[0])
+    out += [
+        rec("HarmonicSolve.lean:284-293", "harmonic", Fc=[5.0, 10.0, 15.0], k=3,
+            rows={"1": [5.0, 10.0, 15.0], "2": [5.0, 10.0, 15.0]}, eps=1e-9, **tws),
+        rec("HarmonicSolve.lean:298-309", "harmonic", Fc=I9, k=9, rows={"1": I9}, eps=1e-9, **tws),
+        rec("HarmonicSolve.lean:313-319", "harmonic", Fc=[7.0], k=1, rows={"1": [7.0], "2": [7.0]}, eps=1e-9, **tws),
+        rec("HarmonicSolve.lean:323-330", "harmonic", Fc=[1.0, 2.0, 3.0], k=3,
+            rows={"1": [1.0, 2.0, 3.0], "2": [1.0, 2.0, 3.0]}, eps=1e-9, **tws),
+        rec("HarmonicSolve.lean:334-344", "harmonic", Fc=RZ, k=9, rows={"1": RZ}, eps=1e-9, **tws),
+        rec("DeformSolve.lean:167-184", "deform", Fc=I9, Xc=[5.0, 0.0, 0.0],
+            rows={"1": [6.0, 0.0, 0.0], "2": [5.5, 0.0, 0.8660254037844386]}, eps=1e-9, **tws),
+        rec("DeformSolve.lean:187-195", "deform", Fc=I9, Xc=[0.0, 2.0, 0.0], rows={"1": [1.0, 2.0, 0.0]}, eps=1e-9, **tws),
+        rec("DeformSolve.lean:208-226", "deform", Fc=RZ, Xc=[0.0, 0.0, 0.0],
+            rows={"1": [0.0, 1.0, 0.0], "2": [0.0, 0.5, 0.8660254037844386]}, eps=1e-9, **tws),
+        rec("DeformSolve.lean:235-253", "deform", Fc=S2, Xc=[0.0, 0.0, 0.0],
+            rows={"1": [2.0, 0.0, 0.0], "2": [1.0, 0.0, 1.7320508075688772]}, eps=1e-9, **tws),
+    ]
+    # ---------------------------------------------------------------- curve-derived inputs
+    prest = [[-1.5, 0.0, 0.0], [-0.5, 0.0, 0.0], [0.5, 0.0, 0.0], [1.5, 0.0, 0.0]]
+    pposed = [[p[0] + 5.0, p[1], p[2]] for p in prest]
+    prot = [[-p[1], p[0], p[2]] for p in prest]
+    out += [
+        rec("EndToEndExample.lean:94-100", "bezier", P=prest, t=0.5, expected=[0.0, 0.0, 0.0], eps=1e-12),
+        rec("EndToEndExample.lean:98-100", "bezier", P=pposed, t=0.5, expected=[5.0, 0.0, 0.0], eps=1e-12),
+        rec("EndToEndExample.lean:108-112", "segment_gradient", P_rest=prest, P_posed=pposed, t=0.5, t_fwd=0.6,
+            F=I9, eps=1e-12),
+        rec("EndToEndExample.lean:182-190", "segment_gradient", P_rest=prest, P_posed=prot, t=0.5, t_fwd=0.6,
+            F=RZ, eps=1e-12),
+        rec("EndToEndExample.lean:144-152", "curve_deform", P_rest=prest, P_posed=pposed, t=0.5, t_fwd=0.6,
+            rows={"1": [6.0, 0.0, 0.0], "2": [5.5, 0.0, 0.8660254037844386]}, eps=1e-9, **tws),
+        rec("EndToEndExample.lean:202-211", "curve_deform", P_rest=prest, P_posed=prot, t=0.5, t_fwd=0.6,
+            rows={"1": [0.0, 1.0, 0.0], "2": [0.0, 0.5, 0.8660254037844386]}, eps=1e-9, **tws),
+    ]
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "known_answers.json")
+    with open(path, "w") as f:
+        json.dump(out, f, indent=1)
+    print(f"wrote {len(out)} fixtures to {path}")
+
+
+if __name__ == "__main__":
+    main()

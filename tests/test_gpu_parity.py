@@ -1,0 +1,211 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU FP64 oracle.
+
+Bars: sparsity pattern, cut topology, elimination order and assembled FP64
+values bit-exact; the FP64 IC(0) factor bit-exact (same order, no FMA
+contraction on either side); deformed positions within 1e-9 relative of the
+oracle in FP64 (both sides solved to 1e-13 relative residual) and within
+1e-6 relative in the mixed FP32/FP64-refinement form at 1e-8 residual."""
+import numpy as np
+import pytest
+
+from tests.helpers import rel_err, workload
+from tool_godot_curvenet_b200 import CnError, CutMeshSolver
+from tool_godot_curvenet_b200 import _lib as L
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-9
+MIXED_TOL = 1e-6
+
+
+def _dense_from(ptr, col, val, n):
+    D = np.zeros((n, n))
+    for i in range(n):
+        D[i, col[ptr[i]:ptr[i + 1]]] = val[ptr[i]:ptr[i + 1]]
+    return D
+
+
+@pytest.mark.parametrize("name", ["cyl_tiny", "c1", "torus_small"])
+@pytest.mark.parametrize("lap", ["cot", "robust"])
+def test_assembly_bit_exact(name, lap, oracle):
+    pos, tris, h, _ = workload(name)
+    kind = 1 if lap == "robust" else 0
+    with CutMeshSolver(pos, tris, h, laplacian=lap, mollify_delta=1e-3) as s:
+        p, c, v = s.export_k()
+    po, co, vo = oracle.assemble_csr(pos.shape[0], tris, pos, kind, 1e-3)
+    assert np.array_equal(p, po) and np.array_equal(c, co)
+    assert np.array_equal(v.view(np.uint64), vo.view(np.uint64))
+
+
+@pytest.mark.parametrize("name", ["cyl_tiny", "c1", "torus_small"])
+@pytest.mark.parametrize("ordering", ["color", "natural"])
+def test_reduction_order_and_factor_bit_exact(name, ordering, oracle):
+    pos, tris, h, _ = workload(name)
+    with CutMeshSolver(pos, tris, h, ordering=ordering) as s:
+        free_of, Ap, Ac, Av = s.export_csr()
+        Lp, Lc, Lv = s.export_factor()
+        info = s.info()
+    ref = oracle.System(pos, tris, h, ordering=1 if ordering == "color" else 0)
+    assert ref.status == 0
+    e = ref.export()
+    assert np.array_equal(free_of, e["free_of"])
+    assert np.array_equal(Ap, e["A"][0]) and np.array_equal(Ac, e["A"][1])
+    assert np.array_equal(Av.view(np.uint64), e["A"][2].view(np.uint64))
+    assert np.array_equal(Lp, e["L"][0]) and np.array_equal(Lc, e["L"][1])
+    assert np.array_equal(Lv.view(np.uint64), e["L"][2].view(np.uint64))
+    assert info["n_levels"] == ref.n_levels
+
+
+@pytest.mark.parametrize("name", ["cyl_tiny", "c1", "torus_small", "c3_0"])
+@pytest.mark.parametrize("precond", ["ic0", "jacobi"])
+def test_deform_solve_fp64_matches_oracle(name, precond, oracle):
+    pos, tris, h, t = workload(name)
+    t = t[:, :3]
+    ref = oracle.System(pos, tris, h, precond=1)
+    st, xo, _, _ = ref.solve(t, mode=1, tol=1e-13)
+    assert st == 0
+    with CutMeshSolver(pos, tris, h, precond=precond) as s:
+        r = s.solve(t, mode="deform", precision="fp64", tol=1e-13, max_iter=20000)
+    assert r.status == 0
+    assert np.all(r.rel_residual <= 1e-13)
+    assert rel_err(r.x, xo) <= FP64_TOL
+
+
+@pytest.mark.parametrize("name", ["cyl_tiny", "c1", "torus_small", "c3_0"])
+def test_deform_solve_mixed_matches_oracle(name, oracle):
+    pos, tris, h, t = workload(name)
+    t = t[:, :3]
+    ref = oracle.System(pos, tris, h)
+    st, xo, _, _ = ref.solve(t, mode=1, tol=1e-13)
+    with CutMeshSolver(pos, tris, h) as s:
+        r = s.solve(t, mode="deform", precision="mixed", tol=1e-8)
+    assert r.status == 0
+    assert np.all(r.rel_residual <= 1e-8)
+    assert rel_err(r.x, xo) <= MIXED_TOL
+
+
+@pytest.mark.parametrize("name", ["c1", "torus_small"])
+def test_harmonic_mode_matches_oracle(name, oracle):
+    pos, tris, h, t = workload(name)
+    t = t[:, :3]
+    ref = oracle.System(pos, tris, h)
+    st, xo, _, _ = ref.solve(t, mode=0, tol=1e-13)
+    with CutMeshSolver(pos, tris, h) as s:
+        r = s.solve(t, mode="harmonic", precision="fp64", tol=1e-13)
+    assert rel_err(r.x, xo) <= FP64_TOL
+
+
+def test_rhs_matches_oracle_and_handles_overlaid(oracle):
+    pos, tris, h, t = workload("c1")
+    with CutMeshSolver(pos, tris, h) as s:
+        r = s.solve(t, mode="deform", precision="fp64", tol=1e-12)
+    assert np.array_equal(r.x[h], t)  # DeformSolve.lean:108-109 overlay
+
+
+def test_identity_pose_reproduces_rest():
+    pos, tris, h, _ = workload("torus_small")
+    with CutMeshSolver(pos, tris, h) as s:
+        r = s.solve(pos[h], mode="deform", precision="fp64", tol=1e-12)
+    assert np.abs(r.x - pos).max() < 1e-9
+
+
+def test_plain_fp64_path_matches(oracle):
+    pos, tris, h, t = workload("c1")
+    ref = oracle.System(pos, tris, h)
+    st, xo, _, _ = ref.solve(t, mode=1, tol=1e-13)
+    with CutMeshSolver(pos, tris, h) as s:
+        r = s.solve(t, mode="deform", precision="fp64", algo="plain", tol=1e-11, max_iter=100000)
+    assert r.status == 0
+    assert rel_err(r.x, xo) <= 1e-7
+
+
+def test_warm_start_converges_faster_to_same_answer():
+    pos, tris, h, t = workload("torus_small")
+    with CutMeshSolver(pos, tris, h) as s:
+        a = s.solve(t, mode="deform", precision="fp64", tol=1e-10)
+        b = s.solve(t * 1.0, mode="deform", precision="fp64", tol=1e-10, warm_start=True)
+    assert b.iterations < a.iterations
+    assert rel_err(b.x, a.x) < 1e-8
+
+
+def test_x0_initial_guess():
+    pos, tris, h, t = workload("c1")
+    with CutMeshSolver(pos, tris, h) as s:
+        a = s.solve(t, mode="deform", precision="fp64", tol=1e-12)
+        b = s.solve(t, x0=a.x, mode="deform", precision="fp64", tol=1e-10)
+    assert b.iterations == 0
+    assert rel_err(b.x, a.x) < 1e-12
+
+
+@pytest.mark.parametrize("k", [1, 9])
+def test_other_rhs_counts(k, oracle):
+    pos, tris, h, _ = workload("torus_small")
+    rng = np.random.default_rng(5)
+    t = rng.normal(size=(h.size, k))
+    ref = oracle.System(pos, tris, h)
+    st, xo, _, _ = ref.solve(t, mode=0, tol=1e-13)
+    with CutMeshSolver(pos, tris, h, max_rhs=k) as s:
+        r = s.solve(t, mode="harmonic", precision="fp64", tol=1e-13)
+        rm = s.solve(t, mode="harmonic", precision="mixed", tol=1e-8)
+    assert rel_err(r.x, xo) <= FP64_TOL
+    assert rel_err(rm.x, xo) <= MIXED_TOL
+
+
+@pytest.mark.parametrize("grid,block,lanes", [(1, 256, 1), (1, 1024, 8), (8, 256, 2), (148, 512, 4), (296, 256, 16)])
+def test_launch_shapes_agree(grid, block, lanes, oracle):
+    pos, tris, h, t = workload("torus_small")
+    ref = oracle.System(pos, tris, h)
+    st, xo, _, _ = ref.solve(t, mode=1, tol=1e-13)
+    with CutMeshSolver(pos, tris, h, grid=grid, block=block, lanes=lanes) as s:
+        r = s.solve(t, mode="deform", precision="fp64", tol=1e-13)
+        rm = s.solve(t, mode="deform", precision="mixed", tol=1e-8)
+    assert rel_err(r.x, xo) <= FP64_TOL
+    assert rel_err(rm.x, xo) <= MIXED_TOL
+
+
+# ----------------------------------------------------------------- errors
+def test_singular_component_reported():
+    pos, tris, h, _ = workload("c1")
+    top_only = h[h >= 64]  # the bottom band keeps no handle
+    with pytest.raises(CnError) as e:
+        CutMeshSolver(pos, tris, top_only)
+    assert e.value.status == L.CN_SINGULAR_COMPONENT
+
+
+def test_nan_positions_reported():
+    pos, tris, h, _ = workload("cyl_tiny")
+    pos = pos.copy()
+    pos[5, 1] = np.nan
+    with pytest.raises(CnError) as e:
+        CutMeshSolver(pos, tris, h)
+    assert e.value.status == L.CN_NAN
+
+
+def test_bad_triangles_reported():
+    pos, tris, h, _ = workload("cyl_tiny")
+    bad = tris.copy()
+    bad[3, 1] = pos.shape[0] + 5
+    with pytest.raises(CnError) as e:
+        CutMeshSolver(pos, bad, h)
+    assert e.value.status == L.CN_BAD_INPUT
+    dup = np.concatenate([h, h[:1]])
+    with pytest.raises(CnError) as e:
+        CutMeshSolver(pos, tris, dup)
+    assert e.value.status == L.CN_BAD_INPUT
+
+
+def test_nan_targets_reported():
+    pos, tris, h, t = workload("cyl_tiny")
+    t = t.copy()
+    t[0, 0] = np.inf
+    with CutMeshSolver(pos, tris, h) as s:
+        with pytest.raises(CnError) as e:
+            s.solve(t)
+    assert e.value.status == L.CN_NAN
+
+
+def test_max_iter_reported():
+    pos, tris, h, t = workload("c1")
+    with CutMeshSolver(pos, tris, h) as s:
+        r = s.solve(t, precision="fp64", tol=1e-12, max_iter=3, max_refine=1, check=False)
+    assert r.status == L.CN_MAX_ITER

@@ -1,0 +1,228 @@
+"""Pins the CPU FP64 oracle to the reference's own known answers: every
+`native_decide` example of the Lean specification on the sparse-solve path
+(tests/golden/known_answers.json, written by make_known_answers.py)."""
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+FIX = json.load(open(os.path.join(HERE, "golden", "known_answers.json")))
+
+HE_BASE = {}
+
+
+def _bases():
+    from tests.golden.make_known_answers import HE_QUAD, HE_STRIP, HE_TRIANGLE
+    return {"triangle": ([3, 1, 6], HE_TRIANGLE), "quad": ([4, 1, 8], HE_QUAD), "strip": ([4, 2, 10], HE_STRIP)}
+
+
+def csr(A):
+    return np.array(A["rowPtr"], np.int32), np.array(A["colIdx"], np.int32), np.array(A["values"])
+
+
+def dense_of(A):
+    p, c, v = csr(A)
+    n = p.size - 1
+    D = np.zeros((n, n))
+    for i in range(n):
+        D[i, c[p[i]:p[i + 1]]] = v[p[i]:p[i + 1]]
+    return D
+
+
+def fid(f):
+    return f"{f['src']}:{f['kind']}"
+
+
+@pytest.mark.parametrize("f", FIX, ids=[fid(f) for f in FIX])
+def test_known_answer(f, oracle):
+    O = oracle
+    k = f["kind"]
+    eps = f.get("eps", 0.0)
+    if k in ("tri_rowsum", "tri_symmetric", "tri_offdiag01"):
+        Lm = O.triangle_cot_laplacian(*f["pts"])
+        if k == "tri_rowsum":
+            assert np.all(np.abs(Lm.sum(1)) < eps)
+        elif k == "tri_symmetric":
+            assert np.all(np.abs(Lm - Lm.T) < eps)
+        else:
+            assert abs(Lm[0, 1] - f["expected"]) < eps
+    elif k in ("poly_rowsum", "poly_symmetric"):
+        Lm = O.polygon_cot_laplacian(f["pts"])
+        if k == "poly_rowsum":
+            assert np.all(np.abs(Lm.sum(1)) < eps)
+        else:
+            assert np.all(np.abs(Lm - Lm.T) < eps)
+    elif k == "mollify_zero":
+        assert abs(O.mollify_triangle(f["delta"], f["e"])) < eps
+    elif k == "mollify_positive":
+        assert O.mollify_triangle(f["delta"], f["e"]) > 0.0
+    elif k == "mollify_margin":
+        d = f["delta"]
+        e = np.array(f["e"]) + O.mollify_triangle(d, f["e"])
+        t = f["tol"]
+        assert e[1] + e[2] > e[0] + d - t and e[0] + e[2] > e[1] + d - t and e[0] + e[1] > e[2] + d - t
+    elif k == "cot_from_lengths":
+        assert abs(O.cot_from_lengths(*f["e"]) - f["expected"]) < eps
+    elif k == "robust_equals_embedded":
+        a = O.robust_triangle_cot_laplacian(f["delta"], *f["pts"])
+        b = O.triangle_cot_laplacian(*f["pts"])
+        assert np.all(np.abs(a - b) < eps)
+    elif k == "robust_rowsum":
+        a = O.robust_triangle_cot_laplacian(f["delta"], *f["pts"])
+        assert np.all(np.abs(a.sum(1)) < eps)
+    elif k == "robust_symmetric":
+        a = O.robust_triangle_cot_laplacian(f["delta"], *f["pts"])
+        assert np.all(np.abs(a - a.T) < eps)
+    elif k == "robust_finite":
+        a = O.robust_triangle_cot_laplacian(f["delta"], *f["pts"])
+        assert np.all(np.isfinite(a))
+    elif k == "manifold":
+        assert O.manifold(f["nv"], f["nf"], np.array(f["he"], np.int32))
+    elif k == "builder":
+        he = O.halfedges_from_triangles(f["nv"], f["tris"])
+        assert he.shape[0] == f["n_he"]
+        assert O.manifold(f["nv"], f["nf"], he)
+        if f.get("all_twins"):
+            assert np.all(he[:, 1] >= 0) and np.all(he[he[:, 1], 1] == np.arange(he.shape[0]))
+    elif k == "surgery":
+        counts, he = _bases()[f["base"]]
+        he = np.array(he, np.int32)
+        counts = np.array(counts, np.int32)
+        for op in f["ops"]:
+            if op[0] == "subdivide":
+                counts, he = O.subdivide_edge(counts, he, op[1])
+            elif op[0] == "split":
+                counts, he = O.split_face(counts, he, op[1], op[2])
+            else:
+                counts, he = O.insert_crack(counts, he, op[1])
+        assert (counts[0], counts[2], counts[1]) == (f["nv"], f["n_he"], f["nf"])
+        assert O.manifold(int(counts[0]), int(counts[1]), he)
+        for h, length in f.get("loops", []):
+            assert O.loop_length(he, h) == length
+        if "crack" in f:
+            a, b = f["crack"]
+            assert he[a, 3] == 0 and he[b, 3] == 0 and he[a, 1] == b and he[b, 1] == a
+    elif k == "partition":
+        assert O.partition_of_unity(np.array(f["he"], np.int32), f["vkind"]) == f["expected"]
+    elif k == "vtlhv":
+        M = O.assemble_vtlhv_dense(f["nv"], f["nf"], np.array(f["he"], np.int32), f["vkind"], f["pos"])
+        assert M.shape == (f["nv"], f["nv"])
+        if "eps_rowsum" in f:
+            assert np.all(np.abs(M.sum(1)) < f["eps_rowsum"])
+        assert np.all(np.abs(M - M.T) < f["eps_sym"])
+    elif k == "dense_solve":
+        n = len(f["b"])
+        x = O.dense_solve(np.array(f["A"], float).reshape(n, n), f["b"])
+        assert np.all(np.abs(x - f["x"]) < eps)
+    elif k == "dense_residual":
+        n = len(f["b"])
+        A = np.array(f["A"], float).reshape(n, n)
+        x = O.dense_solve(A, f["b"])
+        assert np.all(np.abs(A @ x - f["b"]) < eps)
+    elif k == "lu_solve":
+        n = len(f["b"])
+        x = O.lu_solve(np.array(f["A"], float).reshape(n, n), f["b"])
+        assert np.all(np.abs(x - f["x"]) < eps)
+    elif k == "lu_vs_ge":
+        n = len(f["b"])
+        A = np.array(f["A"], float).reshape(n, n)
+        assert np.all(np.abs(O.lu_solve(A, f["b"]) - O.dense_solve(A, f["b"])) < eps)
+    elif k == "cholesky":
+        n = int(math.isqrt(len(f["A"])))
+        Lm = O.cholesky_factor(np.array(f["A"], float).reshape(n, n))
+        assert np.all(np.abs(Lm - np.array(f["L"]).reshape(n, n)) < eps)
+        assert np.all(np.abs(Lm @ Lm.T - np.array(f["A"]).reshape(n, n)) < eps)
+    elif k == "cholesky_solve":
+        n = len(f["b"])
+        Lm = O.cholesky_factor(np.array(f["A"], float).reshape(n, n))
+        assert np.all(np.abs(O.cholesky_solve(Lm, f["b"]) - f["x"]) < eps)
+    elif k == "cholesky_vs_ge":
+        n = len(f["b"])
+        A = np.array(f["A"], float).reshape(n, n)
+        Lm = O.cholesky_factor(A)
+        assert np.all(np.abs(O.cholesky_solve(Lm, f["b"]) - O.dense_solve(A, f["b"])) < eps)
+    elif k == "spmv":
+        assert np.all(np.abs(dense_of(f["A"]) @ np.array(f["x"]) - f["y"]) < eps)
+    elif k == "cg":
+        x, _ = O.cg_ref(*csr(f["A"]), f["b"], f["max_iter"], f["tol"])
+        assert np.all(np.abs(x - f["x"]) < eps)
+    elif k == "cg_vs_dense":
+        x, _ = O.cg_ref(*csr(f["A"]), f["b"], f["max_iter"], f["tol"])
+        xd = O.dense_solve(np.array(f["A_dense"]).reshape(len(f["b"]), -1), f["b"])
+        assert np.all(np.abs(x - xd) < eps)
+    elif k == "cg_warm_vs_cold":
+        xc, _ = O.cg_ref(*csr(f["A"]), f["b"], f["max_iter"], f["tol"])
+        xw, _ = O.cg_ref(*csr(f["A"]), f["b"], f["max_iter"], f["tol"], x0=f["x0"])
+        assert np.all(np.abs(xc - xw) < eps)
+    elif k == "cg_warm_exact":
+        xw, it = O.cg_ref(*csr(f["A"]), f["b"], f["max_iter"], f["tol"], x0=f["x0"])
+        assert it == 0 and np.all(np.abs(xw - f["x0"]) < eps)
+    elif k == "cg_residual":
+        x, _ = O.cg_ref(*csr(f["A"]), f["b"], f["max_iter"], f["tol"])
+        r = np.array(f["b"]) - dense_of(f["A"]) @ x
+        assert float(r @ r) < f["rr_max"]
+    elif k in ("ic0_llt", "ic0_solve"):
+        st, Lp, Lc, Lv = O.ic0_factor(*csr(f["A"]))
+        assert st == 0
+        n = Lp.size - 1
+        Lm = np.zeros((n, n))
+        for i in range(n):
+            Lm[i, Lc[Lp[i]:Lp[i + 1]]] = Lv[Lp[i]:Lp[i + 1]]
+        assert np.all(np.triu(Lm, 1) == 0.0)
+        A = dense_of(f["A"])
+        if k == "ic0_llt":
+            assert np.all(np.abs(Lm @ Lm.T - A) < eps)
+        else:
+            y = np.linalg.solve(Lm, f["b"])
+            x = np.linalg.solve(Lm.T, y)
+            assert np.all(np.abs(A @ x - f["b"]) < eps)
+    elif k == "hsc":
+        g = [tuple(e) for e in f["edges"]]
+        for v in f["elim"]:
+            g = O.hsc_eliminate(g, v)
+        if "n_edges" in f:
+            assert len(g) == f["n_edges"]
+        for a, b, w in f.get("weights", []):
+            got = [e[2] for e in g if (e[0], e[1]) == (a, b)]
+            assert got and abs(got[0] - w) < eps
+        if "degree" in f:
+            v, d = f["degree"]
+            assert abs(sum(e[2] for e in g if v in (e[0], e[1])) - d) < eps
+    elif k == "color":
+        c = O.greedy_color(f["adj"])
+        assert all(c[i] != c[j] for i, a in enumerate(f["adj"]) for j in a)
+        assert int(c.max()) + 1 == f["n_colors"]
+    elif k == "harmonic":
+        X = O.harmonic_solve_multi(f["nv"], f["nf"], np.array(f["he"], np.int32), f["sample_col"], f["pos"],
+                                   f["Fc"], f["k"])
+        for r, want in f["rows"].items():
+            assert np.all(np.abs(X[int(r)] - want) < eps)
+    elif k == "deform":
+        X = O.solve_deformation(f["nv"], f["nf"], np.array(f["he"], np.int32), f["sample_col"], f["pos"],
+                                f["Fc"], f["Xc"])
+        for r, want in f["rows"].items():
+            assert np.all(np.abs(X[int(r)] - want) < eps)
+    elif k == "bezier":
+        out = np.empty(3)
+        O.lib().orc_bezier3(O.dp(O.f64(f["P"])), f["t"], O.dp(out))
+        assert np.all(np.abs(out - f["expected"]) < eps)
+    elif k in ("segment_gradient", "curve_deform"):
+        def bez(P, t):
+            out = np.empty(3)
+            O.lib().orc_bezier3(O.dp(O.f64(P)), t, O.dp(out))
+            return out
+        rp, rq = bez(f["P_rest"], f["t"]), bez(f["P_rest"], f["t_fwd"])
+        pp, pq = bez(f["P_posed"], f["t"]), bez(f["P_posed"], f["t_fwd"])
+        F = np.empty(9)
+        O.lib().orc_isolated_segment_gradient(O.dp(rp), O.dp(rq), O.dp(pp), O.dp(pq), O.dp(F))
+        if k == "segment_gradient":
+            assert np.all(np.abs(F - f["F"]) < eps)
+        else:
+            X = O.solve_deformation(f["nv"], f["nf"], np.array(f["he"], np.int32), f["sample_col"], f["pos"], F, pp)
+            for r, want in f["rows"].items():
+                assert np.all(np.abs(X[int(r)] - want) < eps)
+    else:
+        pytest.fail(f"unknown fixture kind {k}")

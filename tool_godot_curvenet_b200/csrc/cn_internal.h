@@ -1,0 +1,153 @@
+// cn_internal.h -- shared between the host orchestration (cn_host.cpp) and the
+// sm_100a kernels (cn_*.cu).  Not part of the public ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/curvenet_b200.h"
+
+namespace cn {
+
+// Persistent-solve control block (reset by the host before every launch).
+struct Control {
+  unsigned bar_count;
+  unsigned bar_gen;
+  int abort;
+  int status;
+};
+
+// Device-side statistics written by the persistent solve.
+struct DevStats {
+  int status;
+  int iterations;
+  int refinements;
+  int pad;
+  double rel_residual[32];
+};
+
+// Everything the persistent PCG kernel reads.  Arrays are device pointers;
+// vectors are row-interleaved [rows][K].  T-typed arrays are passed as void*
+// and cast inside the kernel (float for mixed precision, double for FP64).
+struct SolveArgs {
+  int n;        // free unknowns (rows of A)
+  int nlev;     // level sets of the triangular solves
+  const int* lev_ptr;
+  // reduced matrix A in solve order
+  const int* A_ptr;
+  const int* A_col;
+  const void* A_val;       // T
+  const double* A_val64;
+  // IC(0): strictly-lower L and its transpose U, and 1/L_ii
+  const int* L_ptr;
+  const int* L_col;
+  const void* L_val;       // T
+  const int* U_ptr;
+  const int* U_col;
+  const void* U_val;       // T
+  const void* dinv;        // T
+  // right-hand side assembly and output over all vertices
+  int nv;
+  int nh;
+  const int* K_ptr;
+  const int* K_col;
+  const double* K_val;
+  const int* free_of;      // row -> vertex
+  const int* hidx;         // vertex -> handle index or -1
+  const int* handles;      // handle -> vertex
+  const double* pos;       // rest positions (deform mode)
+  int mode;                // CN_MODE_*
+  const double* targets;   // nh x K (or n x K for CN_MODE_RHS, solve order)
+  double* x_out;           // nv x K (nullable)
+  const double* x0;        // nv x K initial guess (nullable)
+  int warm;                // keep x64 from the previous solve
+  // vectors
+  double* b64;
+  double* x64;
+  void* r;    // T
+  void* y;    // T
+  void* z;    // T
+  void* p0;   // T
+  void* p1;   // T
+  void* Ap;   // T
+  void* xin;  // T
+  double* partials;        // [kSlots][grid][K]
+  // control
+  double tol;
+  double inner_tol;
+  int max_iter;
+  int max_refine;
+  Control* ctl;
+  DevStats* stats;
+  long long timeout_ns;
+};
+
+constexpr int kSlots = 6;
+
+// Launch the persistent solve; returns a cudaError_t.  precision: CN_PREC_*.
+cudaError_t launch_persistent_solve(const SolveArgs& a, int precision, int K, int lanes,
+                                    int block, int grid, cudaStream_t s);
+// Largest co-resident grid of the persistent solve for this configuration.
+int persistent_max_grid(int precision, int K, int lanes, int block);
+
+// Build-time kernels (cn_assemble.cu).
+struct BuildArgs {
+  int nv, nt, nnzK, n, nnzA, nnzL, nlev;
+  const double* pos;
+  const int* tris;
+  int lap_kind;
+  double delta;
+  double* face_m;           // nt x 6
+  const int* K_cptr;        // nnzK + 1
+  const int* K_contrib;     // face*6 + slot, ascending face per entry
+  double* K_val;
+  const int* A_src;         // nnzA -> K entry
+  double* A_val64;
+  float* A_val32;
+  const int* A_diag;        // n -> A entry of the diagonal
+  const int* lev_ptr;
+  const int* h_lev_ptr;     // host copy of lev_ptr (launch bounds)
+  const int* L_ptr;         // strictly lower, n + 1
+  const int* L_src;         // nnzL -> A entry
+  const int* L_col;
+  const int* T_ptr;         // nnzL + 1 task pointers
+  const int* T_a;           // L entry of L_ik
+  const int* T_b;           // L entry of L_jk
+  double* L_val64;
+  float* L_val32;
+  double* Ld64;             // n
+  double* dinv64;
+  float* dinv32;
+  const int* U_src;         // nnzL -> L entry
+  double* U_val64;
+  float* U_val32;
+  int* status;              // -1 ok, else first failing row
+  double shift;             // diagonal shift factor (Manteuffel): A_ii * (1 + shift)
+  int precond;
+};
+cudaError_t launch_assemble(const BuildArgs& b, cudaStream_t s);
+cudaError_t launch_factor(const BuildArgs& b, cudaStream_t s);
+
+// Plain FP64 Jacobi-PCG with one kernel per primitive and the scalars folded
+// on the host each iteration (the reference's GPU orchestration).
+struct PlainArgs {
+  int n, K;
+  const int* A_ptr;
+  const int* A_col;
+  const double* A_val;
+  const int* A_diag;
+  double *b, *x, *r, *z, *p, *Ap;
+  double* partials;  // [blocks][K]
+  int blocks;
+};
+cudaError_t plain_spmv(const PlainArgs& a, const double* x, double* y, cudaStream_t s);
+cudaError_t plain_dot(const PlainArgs& a, const double* u, const double* v, cudaStream_t s);
+cudaError_t plain_axpy2(const PlainArgs& a, const double* alpha, cudaStream_t s);
+cudaError_t plain_jacobi(const PlainArgs& a, cudaStream_t s);
+cudaError_t plain_saxpby(const PlainArgs& a, const double* beta, cudaStream_t s);
+cudaError_t plain_rhs_and_init(const SolveArgs& sa, const PlainArgs& a, cudaStream_t s);
+cudaError_t plain_residual(const PlainArgs& a, cudaStream_t s);
+cudaError_t plain_output(const SolveArgs& sa, const PlainArgs& a, cudaStream_t s);
+cudaError_t plain_set_scalars(double* d_dst, const double* h_src, int K, cudaStream_t s);
+
+}  // namespace cn

@@ -1,0 +1,219 @@
+"""Host-side mirror of the reference runtime's build / solve / deform entry
+points for the sparse solve, over the C ABI (include/curvenet_b200.h).
+
+Names follow the reference: `cut_mesh` is the seam cut of CutAlgorithm.lean /
+CutMesh.lean, `CutMeshSolver` holds the assembled V^T L_h V
+(CutMeshLaplacian.lean:86-93) with its factor, `solve_multi` is
+HarmonicSolve.lean:51-66 and `solve_deformation` is the Stage-2 solve of
+DeformSolve.lean:110-135 with F_f = I.  Failures raise CnError carrying the
+status code (the reference's silent "degenerate -> 0" results are reported as
+statuses instead).
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _lib as L
+
+
+class CnError(RuntimeError):
+    def __init__(self, status, where):
+        self.status = int(status)
+        super().__init__(f"{where}: {L.status_string(status)} ({self.status}): {L.last_error()}")
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _ip(a):
+    return a.ctypes.data_as(C.POINTER(C.c_int32))
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+_PRECOND = {"jacobi": L.PRECOND_JACOBI, "ic0": L.PRECOND_IC0, "hsc": L.PRECOND_HSC}
+_ORDER = {"natural": L.ORDER_NATURAL, "color": L.ORDER_COLOR}
+_LAP = {"cot": L.LAPLACIAN_COT, "robust": L.LAPLACIAN_ROBUST}
+_PREC = {"fp64": L.PREC_FP64, "mixed": L.PREC_MIXED}
+_MODE = {"harmonic": L.MODE_HARMONIC, "deform": L.MODE_DEFORM, "rhs": L.MODE_RHS}
+_ALGO = {"fused": L.ALGO_FUSED, "plain": L.ALGO_PLAIN}
+
+
+def cut_mesh(n_verts, tris, loops):
+    """Duplicate the vertices of each closed loop; faces on the loop's left move
+    to the copies.  Returns (tris_cut, parent) with parent[v] the uncut vertex."""
+    tris = _i32(tris).reshape(-1, 3)
+    ptr = np.zeros(len(loops) + 1, np.int32)
+    for i, l in enumerate(loops):
+        ptr[i + 1] = ptr[i] + len(l)
+    verts = _i32(np.concatenate(loops)) if loops else np.zeros(0, np.int32)
+    out = np.empty_like(tris)
+    parent = np.empty(n_verts + verts.size, np.int32)
+    nv_out = C.c_int32(0)
+    st = L.lib().cn_cut_mesh(n_verts, tris.shape[0], _ip(tris), len(loops), _ip(ptr), _ip(verts),
+                             _ip(out), _ip(parent), C.byref(nv_out))
+    if st != L.CN_OK:
+        raise CnError(st, "cn_cut_mesh")
+    return out, parent[: nv_out.value]
+
+
+class SolveResult:
+    def __init__(self, x, stats):
+        self.x = x
+        self.status = stats.status
+        self.iterations = stats.iterations
+        self.refinements = stats.refinements
+        self.rel_residual = np.array(stats.rel_residual[: max(1, min(stats.k, 32))])
+        self.device_ms = stats.device_ms
+
+
+class CutMeshSolver:
+    """Assembled and factored system of one cut mesh on one GPU."""
+
+    def __init__(self, positions, tris, handles, precond="ic0", ordering="color",
+                 laplacian="cot", mollify_delta=1e-4, max_rhs=3, device=0, lanes=0,
+                 block=0, grid=0):
+        self.positions = _f64(positions).reshape(-1, 3)
+        self.tris = _i32(tris).reshape(-1, 3)
+        self.handles = _i32(handles).reshape(-1)
+        self.n_verts = self.positions.shape[0]
+        desc = L.MeshDesc(self.n_verts, self.tris.shape[0], _dp(self.positions), _ip(self.tris),
+                          self.handles.size, _ip(self.handles))
+        opts = L.BuildOpts()
+        L.lib().cn_default_build_opts(C.byref(opts))
+        opts.precond = _PRECOND[precond]
+        opts.ordering = _ORDER[ordering]
+        opts.laplacian = _LAP[laplacian]
+        opts.mollify_delta = mollify_delta
+        opts.max_rhs = max_rhs
+        opts.device = device
+        opts.lanes, opts.block, opts.grid = lanes, block, grid
+        h = C.c_void_p()
+        st = L.lib().cn_build(C.byref(desc), C.byref(opts), C.byref(h))
+        if st != L.CN_OK:
+            raise CnError(st, "cn_build")
+        self._h = h
+        self.max_rhs = max_rhs
+
+    # -- lifetime
+    def close(self):
+        if getattr(self, "_h", None):
+            L.lib().cn_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- introspection
+    def info(self):
+        v = (C.c_int64 * 12)()
+        L.lib().cn_system_info(self._h, v)
+        keys = ["n_free", "nnz_A", "nnz_L", "n_levels", "nnz_K", "n_verts", "n_handles", "grid",
+                "block", "lanes", "n_colors", "device_bytes"]
+        return dict(zip(keys, list(v)))
+
+    def stream(self):
+        return L.lib().cn_stream(self._h)
+
+    def export_csr(self):
+        i = self.info()
+        n, nnz = i["n_free"], i["nnz_A"]
+        free_of = np.empty(n, np.int32)
+        ptr = np.empty(n + 1, np.int32)
+        col = np.empty(max(nnz, 1), np.int32)
+        val = np.empty(max(nnz, 1), np.float64)
+        st = L.lib().cn_export_csr(self._h, _ip(free_of), _ip(ptr), _ip(col), _dp(val))
+        if st != L.CN_OK:
+            raise CnError(st, "cn_export_csr")
+        return free_of, ptr, col[:nnz], val[:nnz]
+
+    def export_factor(self):
+        i = self.info()
+        n, nnz = i["n_free"], i["nnz_L"] + i["n_free"]
+        ptr = np.empty(n + 1, np.int32)
+        col = np.empty(max(nnz, 1), np.int32)
+        val = np.empty(max(nnz, 1), np.float64)
+        st = L.lib().cn_export_factor(self._h, _ip(ptr), _ip(col), _dp(val))
+        if st != L.CN_OK:
+            raise CnError(st, "cn_export_factor")
+        return ptr, col[:nnz], val[:nnz]
+
+    def export_k(self):
+        i = self.info()
+        nv, nnz = i["n_verts"], i["nnz_K"]
+        ptr = np.empty(nv + 1, np.int32)
+        col = np.empty(max(nnz, 1), np.int32)
+        val = np.empty(max(nnz, 1), np.float64)
+        st = L.lib().cn_export_k(self._h, _ip(ptr), _ip(col), _dp(val))
+        if st != L.CN_OK:
+            raise CnError(st, "cn_export_k")
+        return ptr, col[:nnz], val[:nnz]
+
+    # -- solves
+    @staticmethod
+    def make_opts(mode="deform", precision="mixed", tol=1e-8, max_iter=2000, max_refine=8,
+                  inner_tol=1e-5, warm_start=False, algo="fused"):
+        o = L.SolveOpts()
+        L.lib().cn_default_solve_opts(C.byref(o))
+        o.mode, o.precision, o.algo = _MODE[mode], _PREC[precision], _ALGO[algo]
+        o.tol, o.max_iter, o.max_refine, o.inner_tol = tol, max_iter, max_refine, inner_tol
+        o.warm_start = int(bool(warm_start))
+        return o
+
+    def solve(self, targets, x0=None, check=True, **kw):
+        """targets: (n_handles, k) for harmonic/deform, (n_free, k) in solve
+        order for mode='rhs'.  Returns SolveResult with x (n_verts, k)."""
+        t = _f64(targets)
+        t = t.reshape(t.shape[0], -1)
+        k = t.shape[1]
+        o = self.make_opts(**kw)
+        x = np.empty((self.n_verts, k), np.float64)
+        stats = L.SolveStats()
+        x0p = _dp(_f64(x0).reshape(self.n_verts, k)) if x0 is not None else None
+        st = L.lib().cn_solve(self._h, k, _dp(t), x0p, _dp(x), C.byref(o), C.byref(stats))
+        if check and st not in (L.CN_OK,):
+            raise CnError(st, "cn_solve")
+        return SolveResult(x, stats)
+
+    def solve_device(self, k, d_targets, d_x_out, stats=True, **kw):
+        """Device-pointer solve on the handle's stream (ints are device addresses)."""
+        o = self.make_opts(**kw)
+        s = L.SolveStats()
+        st = L.lib().cn_solve_device(self._h, k, C.c_void_p(d_targets), C.c_void_p(d_x_out),
+                                     C.byref(o), C.byref(s) if stats else None)
+        if st != L.CN_OK:
+            raise CnError(st, "cn_solve_device")
+        return s if stats else None
+
+
+def solve_multi(positions, tris, handles, Fc, **kw):
+    """HarmonicSolve.lean:51-66: (V^T L_h V) X_v = -V^T L_h (C F_c); the handle
+    rows carry F_c (the reference returns 0 there and the caller overlays)."""
+    Fc = _f64(Fc)
+    Fc = Fc.reshape(Fc.shape[0], -1)
+    k = Fc.shape[1]
+    with CutMeshSolver(positions, tris, handles, max_rhs=k if k in (1, 3, 9) else 9) as s:
+        return s.solve(Fc, mode="harmonic", **kw).x
+
+
+def solve_deformation(positions, tris, handles, Xc, **kw):
+    """DeformSolve.lean:123-135 Stage 2 with F_f = I: the displacement-harmonic
+    solve that reproduces the rest pose when X_c is the rest handle position."""
+    with CutMeshSolver(positions, tris, handles, max_rhs=3) as s:
+        return s.solve(_f64(Xc).reshape(-1, 3), mode="deform", **kw).x
