@@ -410,7 +410,7 @@ cn_status alloc_solve_state(cn_system* S) {
 void choose_launch(cn_system* S) {
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, S->device);
-  S->lanes = S->opts.lanes > 0 ? S->opts.lanes : 4;
+  S->lanes = S->opts.lanes > 0 ? S->opts.lanes : 2;
   if (S->n <= 12288) {
     S->block = S->opts.block > 0 ? S->opts.block : 1024;
     S->grid = S->opts.grid > 0 ? S->opts.grid : 1;

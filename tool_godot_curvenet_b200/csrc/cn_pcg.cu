@@ -37,19 +37,21 @@ __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
   asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
   return v;
 }
-__device__ __forceinline__ void st_release_u32(unsigned* p, unsigned v) {
-  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
 __device__ __forceinline__ unsigned long long global_ns() {
   unsigned long long t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
 }
 
-// All blocks of a cooperative grid.
+// All blocks of a cooperative grid.  A monotonic arrival counter: barrier
+// number e completes when the counter reaches e * gridDim.x (the host zeroes
+// it before the launch).  Each block's thread 0 adds 1 with a fire-and-forget
+// reduction after a fence, then polls with acquire loads; the wait is bounded
+// by timeout_ns and by the shared abort flag.
 struct GridTeam {
   Control* ctl;
   long long timeout_ns;
+  mutable unsigned epoch;
   __device__ __forceinline__ int rank() const { return blockIdx.x; }
   __device__ __forceinline__ int size() const { return gridDim.x; }
   __device__ bool sync() const {
@@ -57,18 +59,15 @@ struct GridTeam {
     __syncthreads();
     if (threadIdx.x == 0) {
       int ok = 1;
-      unsigned gen = ld_acquire_u32(&ctl->bar_gen);
+      ++epoch;
+      const unsigned target = epoch * gridDim.x;
       __threadfence();
-      unsigned prev = atomicAdd(&ctl->bar_count, 1u);
-      if (prev == gridDim.x - 1) {
-        atomicExch(&ctl->bar_count, 0u);
-        __threadfence();
-        st_release_u32(&ctl->bar_gen, gen + 1);
-      } else {
-        unsigned long long t0 = global_ns();
+      asm volatile("red.relaxed.gpu.global.add.u32 [%0], 1;" ::"l"(&ctl->bar_count) : "memory");
+      if (ld_acquire_u32(&ctl->bar_count) < target) {
+        const unsigned long long t0 = global_ns();
         unsigned spins = 0;
-        while (ld_acquire_u32(&ctl->bar_gen) == gen) {
-          if ((++spins & 255u) == 0) {
+        while (ld_acquire_u32(&ctl->bar_count) < target) {
+          if ((++spins & 63u) == 0) {
             if (*(volatile int*)&ctl->abort) { ok = 0; break; }
             if ((long long)(global_ns() - t0) > timeout_ns) {
               atomicExch(&ctl->abort, 1);
@@ -78,8 +77,6 @@ struct GridTeam {
           }
         }
       }
-      if (ok && *(volatile int*)&ctl->abort) ok = 0;
-      __threadfence();
       s_ok = ok;
     }
     __syncthreads();
@@ -135,22 +132,23 @@ __device__ void block_reduce_store(double (&v)[K], double* red, double* out) {
   __syncthreads();
 }
 
-// After a barrier: every block adds the team's partials of one slot in the
-// same order; the result lands in s->sum.
+// After a barrier: every block adds the team's partials of one slot; every
+// thread loads at most a few partials (independent loads, one L2 latency),
+// then a fixed-order block reduction lands the K sums in s->sum.
 template <int K>
 __device__ void team_sum(const double* part, int size, Smem<K>* s) {
-  const int lane = threadIdx.x & 31;
-  if (threadIdx.x < 32) {
+  double v[K];
 #pragma unroll
-    for (int c = 0; c < K; ++c) {
-      double t = 0.0;
-      for (int r = lane; r < size; r += 32) t += __ldcg(part + (size_t)r * K + c);
+  for (int c = 0; c < K; ++c) v[c] = 0.0;
+  const int tot = size * K;
+  for (int i = threadIdx.x; i < tot; i += blockDim.x) {
+    const double x = __ldcg(part + i);
+    const int ci = i % K;
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
-      if (lane == 0) s->sum[c] = t;
-    }
+    for (int c = 0; c < K; ++c)
+      if (c == ci) v[c] += x;
   }
-  __syncthreads();
+  block_reduce_store<K>(v, s->red, s->sum);
 }
 
 template <int G>
@@ -500,7 +498,7 @@ done:
 template <typename T, int K, int G>
 __global__ void __launch_bounds__(1024) k_solve_grid(SolveArgs a) {
   __shared__ Smem<K> s;
-  GridTeam team{a.ctl, a.timeout_ns};
+  GridTeam team{a.ctl, a.timeout_ns, 0u};
   solve_body<T, K, G>(a, team, &s);
 }
 
