@@ -145,6 +145,32 @@ cn_status cn_export_csr(cn_handle h, int32_t* free_of, int32_t* rowptr, int32_t*
 cn_status cn_export_factor(cn_handle h, int32_t* rowptr, int32_t* colidx, double* vals);
 cn_status cn_export_k(cn_handle h, int32_t* rowptr, int32_t* colidx, double* vals);
 
+/* FP64 Jacobi-preconditioned CG on a caller-owned device CSR matrix
+ * (n rows, sorted columns, FP64 values) for k = 1, 3 or 9 right-hand sides,
+ * that allocates no GPU memory.  No counterpart in the reference.
+ *
+ * For callers that cannot call cudaMalloc while they run: a real-time frame
+ * loop with a fixed memory budget (an engine that pre-allocates at start-up
+ * and forbids allocation per frame), code that records work into a CUDA
+ * stream, or a host that owns all device memory itself.  The caller passes
+ * the matrix (d_rowptr n+1, d_colidx, d_vals), the right-hand sides d_b
+ * (n x k, row-major) and the solution d_x (n x k: initial guess in, solution
+ * out); every temporary lives in one fixed device array inside the library
+ * (about 14 MB per GPU, kept until the process exits).
+ *
+ * Limits: n <= 65,536 and n * k <= 196,608; larger systems return
+ * CN_BAD_INPUT with the reason in cn_last_error().  The stopping test is the
+ * relative residual ||b - A x|| <= tol ||b|| per column.  The work is
+ * enqueued on `stream` (a cudaStream_t; NULL = the default stream) of the
+ * current device; with stats == NULL the call does not synchronise.  Every
+ * call shares the same scratch array, so calls that overlap on the GPU (two
+ * streams or two threads at once) race and must be serialised by the caller.
+ * The first call on a device looks up the array's device address; make that
+ * first call before any stream capture. */
+cn_status cn_pcg_csr_noalloc(int32_t n, const int32_t* d_rowptr, const int32_t* d_colidx,
+                             const double* d_vals, int32_t k, const double* d_b, double* d_x,
+                             double tol, int32_t max_iter, void* stream, cn_solve_stats* stats);
+
 #ifdef __cplusplus
 }
 #endif

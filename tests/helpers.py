@@ -21,6 +21,10 @@ def workload(name):
         m = synth.torus(96, 48, cut_u=(0, 24, 48, 72), seed=11)
         h = synth.pick_handles(m, 0.02, 12)
         t = synth.uniform_targets(m.positions, h, 0.2, 13)
+    elif name == "torus_mid":
+        m = synth.torus(160, 112, cut_u=(0, 40, 80, 120), seed=31)
+        h = synth.pick_handles(m, 0.02, 32)
+        t = synth.uniform_targets(m.positions, h, 0.2, 33)
     elif name == "cyl_tiny":
         m = synth.cylinder(12, 8, cut_rows=(4,), seed=21)
         h = np.concatenate([np.arange(12), np.arange(12) + 7 * 12]).astype(np.int32)

@@ -64,6 +64,8 @@ SIGNATURES = {
     "cn_export_csr": (C.c_int, [_P, _I32P, _I32P, _I32P, _DP]),
     "cn_export_factor": (C.c_int, [_P, _I32P, _I32P, _DP]),
     "cn_export_k": (C.c_int, [_P, _I32P, _I32P, _DP]),
+    "cn_pcg_csr_noalloc": (C.c_int, [C.c_int32, _P, _P, _P, C.c_int32, _P, _P, C.c_double, C.c_int32, _P,
+                                     C.POINTER(SolveStats)]),
 }
 
 _lib = None

@@ -81,6 +81,8 @@ struct Dsu {
 
 }  // namespace
 
+void cn::set_last_error_text(const char* msg) { g_err = msg; }
+
 // ---------------------------------------------------------------------------
 struct cn_system {
   int device = 0;

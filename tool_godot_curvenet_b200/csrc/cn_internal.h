@@ -84,6 +84,9 @@ struct SolveArgs {
 
 constexpr int kSlots = 6;
 
+// Sets the text cn_last_error() returns on this thread (cn_host.cpp).
+void set_last_error_text(const char* msg);
+
 // Launch the persistent solve; returns a cudaError_t.  precision: CN_PREC_*.
 cudaError_t launch_persistent_solve(const SolveArgs& a, int precision, int K, int lanes,
                                     int block, int grid, cudaStream_t s);
