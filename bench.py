@@ -307,7 +307,8 @@ def main():
             "speedup_mixed_vs_fp64_fused": ms_fp64 / ms_mixed,
             "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
                          "peak_kind": peak_kind, "traffic": traffic,
-                         "kernel": "k_solve_grid<float,3,4> (persistent solve)",
+                         "kernel": f"k_solve_grid<float,3,{info['lanes']}> (persistent solve, grid {info['grid']} x {info['block']})",
+                         "note": "L2-resident working set: DRAM traffic per launch is ~1% of the algorithmic bytes; latency-bound (barriers, dependent L2 loads)",
                          "algorithmic_bytes_per_launch": bytes_mixed,
                          "fp64_fused_achieved": bytes_fp64 / (ms_fp64 * 1e-3) / 1e9},
             "e2e": {"value": world * 1e3 / ms_e2e, "unit": "solves/s", "h2d_bytes_per_step": int(h_t.numel() * 8),
