@@ -154,6 +154,91 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def batch_section(torch, dist, world, rank, local, steps, warmup):
+    """The batched workload (512 meshes, cylinder or torus, n_v log-uniform in
+    [2k, 60k], 1-4 seams, 8 poses x 3 RHS, mixed precision to 1e-8) in one
+    persistent CUDA-graph launch per batch; with N ranks the meshes are
+    sharded (longest-processing-time partition) and each rank launches its
+    share."""
+    from tool_godot_curvenet_b200 import BatchSolver, cut_mesh, synth
+    from tool_godot_curvenet_b200.shard import lpt_partition, mesh_cost
+    n_meshes = 512
+    specs = [synth.config3_mesh(i) for i in range(n_meshes)]
+    costs = [mesh_cost(m.positions.shape[0] + sum(len(l) for l in m.loops), m.tris.shape[0]) for m, _, _ in specs]
+    mine = lpt_partition(costs, world)[rank]
+    meshes, targets = [], []
+    for i in mine:
+        m, h, t = specs[i]
+        tris, parent = cut_mesh(m.positions.shape[0], m.tris, m.loops)
+        meshes.append((np.ascontiguousarray(m.positions[parent]), tris, h))
+        targets.append(t)
+    t0 = time.perf_counter()
+    B = BatchSolver(meshes, k=24, device=local)
+    build_s = time.perf_counter() - t0
+    info = B.info()
+    flat = np.concatenate([t.reshape(-1) for t in targets])
+    d_t = torch.from_numpy(flat).to(f"cuda:{local}")
+    d_x = torch.empty(int(B.out_off[-1]), dtype=torch.float64, device=f"cuda:{local}")
+    stream = torch.cuda.ExternalStream(B.stream(), device=local)
+    st_mixed = B.solve_device(d_t.data_ptr(), d_x.data_ptr(), precision="mixed", tol=1e-8)
+    sts, its, rel = B.mesh_stats()
+    st_fp64 = B.solve_device(d_t.data_ptr(), d_x.data_ptr(), precision="fp64", tol=1e-8)
+
+    def timed(precision, k_steps):
+        with torch.cuda.stream(stream):
+            for _ in range(warmup):
+                B.solve_device(d_t.data_ptr(), d_x.data_ptr(), stats=False, precision=precision, tol=1e-8)
+            evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(k_steps)]
+            torch.cuda.synchronize()
+            if world > 1:
+                dist.barrier()
+            for a, b in evs:
+                a.record(stream)
+                B.solve_device(d_t.data_ptr(), d_x.data_ptr(), stats=False, precision=precision, tol=1e-8)
+                b.record(stream)
+            torch.cuda.synchronize()
+            if world > 1:
+                dist.barrier()
+        return [a.elapsed_time(b) for a, b in evs]
+
+    tm = timed("mixed", steps)
+    chk_m = B.solve_device(d_t.data_ptr(), d_x.data_ptr(), precision="mixed", tol=1e-8)
+    tf = timed("fp64", max(2, steps // 2))
+    chk_f = B.solve_device(d_t.data_ptr(), d_x.data_ptr(), precision="fp64", tol=1e-8)
+    if chk_m.n_failed or chk_f.n_failed or chk_m.max_rel_residual > 1e-8 or chk_f.max_rel_residual > 1e-8:
+        raise SystemExit(f"batch solve did not converge: mixed {chk_m.n_failed} failed, fp64 {chk_f.n_failed} failed")
+
+    def red(v, op):
+        if world == 1:
+            return v
+        tt = torch.tensor([v], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(tt, op=op)
+        return float(tt.item())
+    mx = dist.ReduceOp.MAX if world > 1 else None
+    p50 = red(float(np.percentile(tm, 50)), mx)
+    p99 = red(float(np.percentile(tm, 99)), mx)
+    ms_m = red(sum(tm) / len(tm), mx)
+    ms_f = red(sum(tf) / len(tf), mx)
+    solves = n_meshes * 8  # (mesh, pose) solves of 3 RHS each, over all ranks
+    # algorithmic bytes of the batch (mixed): per mesh iterations x B_iter + residuals
+    nnz = info["nnz_A"]
+    n = info["n_free"]
+    return {
+        "workload": "512 meshes (cylinder|torus, n_v log-uniform [2k,60k], 1-4 seams, 2% handles) x 8 poses x 3 RHS",
+        "n_meshes": n_meshes, "meshes_this_rank": len(mine), "n_verts_rank0": info["n_verts"],
+        "nnz_A_rank0": nnz, "n_free_rank0": n,
+        "cluster_size": info["cluster_size"], "n_clusters": info["n_clusters"], "block": info["block"],
+        "mixed": {"solves_per_s": solves / (ms_m * 1e-3), "ms_per_batch": ms_m, "p50_ms": p50, "p99_ms": p99,
+                  "max_iterations": st_mixed.max_iterations, "total_iterations": st_mixed.total_iterations,
+                  "max_rel_residual": st_mixed.max_rel_residual, "failed": st_mixed.n_failed},
+        "fp64_fused": {"solves_per_s": solves / (ms_f * 1e-3), "ms_per_batch": ms_f,
+                       "max_rel_residual": st_fp64.max_rel_residual, "failed": st_fp64.n_failed},
+        "speedup_mixed_vs_fp64_fused": ms_f / ms_m,
+        "build_s": build_s,
+        "graph": "one cudaGraphLaunch (memset of the work counter + the persistent cluster kernel) per batch",
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -161,6 +246,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batch", action="store_true")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -278,6 +364,10 @@ def main():
         traffic = tj.get("cn_persistent_solve_mixed", {}).get("dram_bytes_per_launch")
     except Exception:
         pass
+    batch = None
+    if not args.no_batch:
+        solver.close()
+        batch = batch_section(torch, dist, world, rank, local, max(3, args.steps // 6), 2)
     if rank == 0:
         x = d_x.cpu().numpy()
         line = {
@@ -317,6 +407,8 @@ def main():
             "clocks": clk,
             "checksum": float(np.abs(x).sum()),
         }
+        if batch is not None:
+            line["batch"] = batch
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(pos, tris, h, t)
         print(json.dumps(line), flush=True)

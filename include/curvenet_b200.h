@@ -145,6 +145,72 @@ cn_status cn_export_csr(cn_handle h, int32_t* free_of, int32_t* rowptr, int32_t*
 cn_status cn_export_factor(cn_handle h, int32_t* rowptr, int32_t* colidx, double* vals);
 cn_status cn_export_k(cn_handle h, int32_t* rowptr, int32_t* colidx, double* vals);
 
+/* ---------------------------------------------------------------------------
+ * Profile curves and the adjoint.  A curve is a composite cubic Bezier of
+ * n_segments segments (3 n_segments + 1 control points, the cubic of
+ * EndToEndExample.lean:52-60 per segment).  Handle h is bound at rest to curve
+ * curve_of[h] (-1: none) at parameter tau[h] in [0, n_segments]; with per-curve
+ * weight w_c its target is rest(h) + w_c (B_posed(tau_h) - B_rest(tau_h)).
+ * The reference binds samples to curves by nearest-vertex projection
+ * (SurfaceProjection.lean:46-64) and has no per-curve weights; this map is
+ * the library's definition. */
+cn_status cn_bind_curves(cn_handle h, int32_t n_curves, int32_t n_segments, const double* rest_cp,
+                         const int32_t* curve_of, const double* tau);
+/* Handle targets from the posed control points (n_curves x (3S+1) x 3) and
+ * weights, then the deform solve (CN_MODE_DEFORM, k = 3); x_out: n_verts x 3. */
+cn_status cn_deform(cn_handle h, const double* posed_cp, const double* weights, double* x_out,
+                    const cn_solve_opts* opts, cn_solve_stats* stats);
+/* Vector-Jacobian product of the last cn_deform: given dL/dx (n_verts x 3),
+ * solves A lambda = (dL/dx)_free with the same factor (A = A^T), then
+ * dL/dX_c(h) = -(K_{h,free} lambda) + dL/dx_h, chained to the control points
+ * (dL_dcp, like posed_cp) and the weights (dL_dw, n_curves). */
+cn_status cn_adjoint(cn_handle h, const double* dL_dx, double* dL_dcp, double* dL_dw,
+                     const cn_solve_opts* opts, cn_solve_stats* stats);
+
+/* ---------------------------------------------------------------------------
+ * Batched solves: many meshes of uneven size, each with k right-hand sides
+ * (k = 24: 8 poses x 3 coordinates, or k = 3), in ONE persistent,
+ * CUDA-graph-captured launch.  Each thread-block cluster takes the next mesh
+ * (largest first) and solves it with the algorithm of cn_solve; the hardware
+ * cluster barrier synchronises the cluster.  The runtime's per-frame loop
+ * over bound meshes and poses (HarmonicSolve.lean:51-66 per mesh;
+ * SlangCodegen/SpmvMulti.lean:8-14 for the multi-RHS layout) becomes one
+ * launch.  Targets are concatenated mesh by mesh (n_handles_m x k each),
+ * positions likewise (n_verts_m x k each); cn_batch_offsets gives the
+ * offsets. */
+typedef struct {
+  int32_t status;            /* worst mesh status */
+  int32_t n_meshes;
+  int32_t n_failed;          /* meshes not at CN_OK */
+  int32_t max_iterations;    /* largest inner-iteration count of one mesh */
+  int64_t total_iterations;
+  double max_rel_residual;   /* over all meshes and columns */
+  double device_ms;          /* device time of the launch (CUDA events) */
+} cn_batch_stats;
+
+/* cluster_size: blocks per cluster (0 = 4; up to 16); n_clusters: clusters of
+ * the persistent grid (0 = all co-resident).  opts->block: threads per block
+ * (0 = 512). */
+cn_status cn_build_batch(const cn_mesh_desc* meshes, int32_t n_meshes, const cn_build_opts* opts,
+                         int32_t k, int32_t cluster_size, int32_t n_clusters, cn_batch_handle* out);
+void cn_destroy_batch(cn_batch_handle b);
+cn_status cn_solve_batch(cn_batch_handle b, const double* targets, double* x_out,
+                         const cn_solve_opts* opts, cn_batch_stats* stats);
+/* Device buffers, enqueued on the batch's stream as one graph launch; with
+ * stats == NULL the call does not synchronise. */
+cn_status cn_solve_batch_device(cn_batch_handle b, const double* d_targets, double* d_x_out,
+                                const cn_solve_opts* opts, cn_batch_stats* stats);
+void* cn_batch_stream(cn_batch_handle b);
+/* info[0..11] = n_meshes, k, total vertices, total handles, total free rows,
+ * total nnz(A), total nnz(L strict), cluster size, clusters, block, max free
+ * rows of one mesh, device bytes held. */
+cn_status cn_batch_info(cn_batch_handle b, int64_t* info);
+/* n_meshes + 1 offsets (in doubles) of each mesh's targets and positions. */
+cn_status cn_batch_offsets(cn_batch_handle b, int64_t* tgt_off, int64_t* out_off);
+/* Per-mesh results of the last solve with stats. */
+cn_status cn_batch_mesh_stats(cn_batch_handle b, int32_t* status, int32_t* iterations,
+                              double* max_rel_residual);
+
 /* FP64 Jacobi-preconditioned CG on a caller-owned device CSR matrix
  * (n rows, sorted columns, FP64 values) for k = 1, 3 or 9 right-hand sides,
  * that allocates no GPU memory.  No counterpart in the reference.

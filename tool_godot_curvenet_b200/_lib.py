@@ -38,6 +38,12 @@ class SolveOpts(C.Structure):
                 ("inner_tol", C.c_double), ("warm_start", C.c_int32)]
 
 
+class BatchStats(C.Structure):
+    _fields_ = [("status", C.c_int32), ("n_meshes", C.c_int32), ("n_failed", C.c_int32),
+                ("max_iterations", C.c_int32), ("total_iterations", C.c_int64),
+                ("max_rel_residual", C.c_double), ("device_ms", C.c_double)]
+
+
 class SolveStats(C.Structure):
     _fields_ = [("status", C.c_int32), ("iterations", C.c_int32), ("refinements", C.c_int32),
                 ("k", C.c_int32), ("rel_residual", C.c_double * 32),
@@ -64,6 +70,18 @@ SIGNATURES = {
     "cn_export_csr": (C.c_int, [_P, _I32P, _I32P, _I32P, _DP]),
     "cn_export_factor": (C.c_int, [_P, _I32P, _I32P, _DP]),
     "cn_export_k": (C.c_int, [_P, _I32P, _I32P, _DP]),
+    "cn_bind_curves": (C.c_int, [_P, C.c_int32, C.c_int32, _DP, _I32P, _DP]),
+    "cn_deform": (C.c_int, [_P, _DP, _DP, _DP, C.POINTER(SolveOpts), C.POINTER(SolveStats)]),
+    "cn_adjoint": (C.c_int, [_P, _DP, _DP, _DP, C.POINTER(SolveOpts), C.POINTER(SolveStats)]),
+    "cn_build_batch": (C.c_int, [C.POINTER(MeshDesc), C.c_int32, C.POINTER(BuildOpts), C.c_int32, C.c_int32,
+                                 C.c_int32, C.POINTER(_P)]),
+    "cn_destroy_batch": (None, [_P]),
+    "cn_solve_batch": (C.c_int, [_P, _DP, _DP, C.POINTER(SolveOpts), C.POINTER(BatchStats)]),
+    "cn_solve_batch_device": (C.c_int, [_P, _P, _P, C.POINTER(SolveOpts), C.POINTER(BatchStats)]),
+    "cn_batch_stream": (_P, [_P]),
+    "cn_batch_info": (C.c_int, [_P, C.POINTER(C.c_int64)]),
+    "cn_batch_offsets": (C.c_int, [_P, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    "cn_batch_mesh_stats": (C.c_int, [_P, _I32P, _I32P, _DP]),
     "cn_pcg_csr_noalloc": (C.c_int, [C.c_int32, _P, _P, _P, C.c_int32, _P, _P, C.c_double, C.c_int32, _P,
                                      C.POINTER(SolveStats)]),
 }

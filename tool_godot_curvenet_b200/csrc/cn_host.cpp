@@ -1,36 +1,21 @@
-// cn_host.cpp -- host side of the C ABI: input checks, the seam cut, the CSR
-// pattern of K and of the reduced system, the elimination order (greedy
-// colouring + level sets), the IC(0) task lists, device buffers, and the
-// solve dispatch.  All floating-point work runs on the GPU; the host builds
-// integer structure only.
+// cn_host.cpp -- the single-mesh handle of the C ABI: build (host structure,
+// one device allocation, GPU assembly + IC(0)), solve dispatch (persistent
+// fused solve or the plain per-primitive baseline), and the exports.  All
+// floating-point work runs on the GPU; the host builds integer structure only.
 #include <algorithm>
 #include <cmath>
-#include <cstdarg>
-#include <cstdio>
 #include <cstring>
 #include <numeric>
-#include <string>
 #include <vector>
 
-#include "cn_internal.h"
+#include "cn_mesh.h"
 
-using cn::BuildArgs;
 using cn::Control;
 using cn::DevStats;
+using cn::MeshDev;
+using cn::MeshHost;
 using cn::SolveArgs;
-
-namespace {
-
-thread_local std::string g_err;
-
-void set_err(const char* fmt, ...) {
-  char buf[512];
-  va_list ap;
-  va_start(ap, fmt);
-  vsnprintf(buf, sizeof buf, fmt, ap);
-  va_end(ap);
-  g_err = buf;
-}
+using cn::set_err;
 
 #define CN_CUDA(call)                                                          \
   do {                                                                         \
@@ -42,84 +27,34 @@ void set_err(const char* fmt, ...) {
     }                                                                          \
   } while (0)
 
-// Device allocation list owned by a handle.
-struct DevArena {
-  std::vector<void*> ptrs;
-  size_t bytes = 0;
-  template <class T>
-  cudaError_t alloc(T** p, size_t count) {
-    *p = nullptr;
-    if (count == 0) count = 1;
-    cudaError_t e = cudaMalloc((void**)p, sizeof(T) * count);
-    if (e == cudaSuccess) { ptrs.push_back(*p); bytes += sizeof(T) * count; }
-    return e;
-  }
-  template <class T>
-  cudaError_t upload(T** p, const std::vector<T>& h) {
-    cudaError_t e = alloc(p, h.size());
-    if (e != cudaSuccess) return e;
-    if (!h.empty()) e = cudaMemcpy(*p, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice);
-    return e;
-  }
-  void release() {
-    for (void* p : ptrs) cudaFree(p);
-    ptrs.clear();
-    bytes = 0;
-  }
-};
-
-// Union-find over vertices.
-struct Dsu {
-  std::vector<int> p;
-  explicit Dsu(int n) : p(n) { std::iota(p.begin(), p.end(), 0); }
-  int find(int a) {
-    while (p[a] != a) { p[a] = p[p[a]]; a = p[a]; }
-    return a;
-  }
-  void unite(int a, int b) { p[find(a)] = find(b); }
-};
-
-}  // namespace
-
-void cn::set_last_error_text(const char* msg) { g_err = msg; }
-
-// ---------------------------------------------------------------------------
 struct cn_system {
   int device = 0;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   cn_build_opts opts{};
-  int nv = 0, nt = 0, nh = 0, n = 0, nlev = 0, ncolors = 0, kmax = 3;
-  int nnzK = 0, nnzA = 0, nnzL = 0;
-  int lanes = 4, block = 512, grid = 0;
+  MeshHost H;
+  MeshDev D;
+  int kmax = 3;
+  int lanes = 2, block = 512, grid = 0;
   double shift_used = 0.0;
-  // host structure (exports)
-  std::vector<int> K_ptr, K_col, free_of, A_ptr, A_col, L_ptr, L_col, lev_ptr, handles;
-  // device
-  DevArena mem;
-  double *d_pos = nullptr, *d_face_m = nullptr, *d_K_val = nullptr;
-  int *d_tris = nullptr, *d_K_ptr = nullptr, *d_K_col = nullptr, *d_K_cptr = nullptr,
-      *d_K_contrib = nullptr;
-  int *d_hidx = nullptr, *d_free_of = nullptr, *d_handles = nullptr;
-  int *d_A_ptr = nullptr, *d_A_col = nullptr, *d_A_src = nullptr, *d_A_diag = nullptr,
-      *d_lev_ptr = nullptr;
-  double* d_A64 = nullptr;
-  float* d_A32 = nullptr;
-  int *d_L_ptr = nullptr, *d_L_col = nullptr, *d_L_src = nullptr, *d_T_ptr = nullptr,
-      *d_T_a = nullptr, *d_T_b = nullptr;
-  int *d_U_ptr = nullptr, *d_U_col = nullptr, *d_U_src = nullptr;
-  double *d_L64 = nullptr, *d_U64 = nullptr, *d_Ld64 = nullptr, *d_dinv64 = nullptr;
-  float *d_L32 = nullptr, *d_U32 = nullptr, *d_dinv32 = nullptr;
-  int* d_status = nullptr;
-  // solve state
+  char* buf = nullptr;   // the one device allocation
+  size_t bytes = 0;
+  // solve state (inside buf)
   double *d_b64 = nullptr, *d_x64 = nullptr, *d_partials = nullptr;
   double* d_w64[7] = {};
   float* d_w32[7] = {};
   Control* d_ctl = nullptr;
   DevStats* d_stats = nullptr;
-  double *d_targets = nullptr, *d_x0 = nullptr, *d_xout = nullptr, *d_scal = nullptr;
+  double *d_targets = nullptr, *d_xout = nullptr, *d_scal = nullptr;
+  int* d_status = nullptr;
   int max_grid_alloc = 0;
   bool have_solution = false;
+  // profile-curve binding (cn_bind_curves), own allocations
+  int ncurves = 0, nseg = 0;
+  bool have_forward = false;
+  int *d_curve_of = nullptr, *d_row_of = nullptr;
+  double *d_tau = nullptr, *d_rest_cp = nullptr, *d_posed_cp = nullptr, *d_weights = nullptr;
+  double *d_dLdx = nullptr, *d_dP = nullptr, *d_dw = nullptr;
 };
 
 namespace {
@@ -128,292 +63,30 @@ const char* kStatusText[] = {"ok", "max_iter", "singular_component", "nonpositiv
                              "nan", "breakdown", "timeout", "bad_input", "cuda_error",
                              "no_device"};
 
-int local_of(int corner) { return (corner + 2) % 3; }  // t0,t1,t2 -> faceLoop slots 2,0,1
-int off_slot(int a, int b) {
-  if (a > b) std::swap(a, b);
-  return a == 0 ? (b == 1 ? 3 : 4) : 5;
-}
-
-// Vertex -> incident faces (ascending face id), with the corner of the vertex.
-void vertex_faces(int nv, int nt, const int* tris, std::vector<int>& ptr, std::vector<int>& face,
-                  std::vector<int>& corner) {
-  ptr.assign(nv + 1, 0);
-  for (int i = 0; i < 3 * nt; ++i) ptr[tris[i] + 1]++;
-  for (int v = 0; v < nv; ++v) ptr[v + 1] += ptr[v];
-  face.resize(3 * (size_t)nt);
-  corner.resize(3 * (size_t)nt);
-  std::vector<int> fill(ptr.begin(), ptr.end() - 1);
-  for (int f = 0; f < nt; ++f)
-    for (int c = 0; c < 3; ++c) {
-      int v = tris[3 * f + c];
-      face[fill[v]] = f;
-      corner[fill[v]] = c;
-      fill[v]++;
-    }
-}
-
-cn_status build_structure(cn_system* S, const cn_mesh_desc* m, std::vector<int>& K_cptr,
-                          std::vector<int>& K_contrib, std::vector<int>& hidx,
-                          std::vector<int>& A_src, std::vector<int>& A_diag,
-                          std::vector<int>& L_src, std::vector<int>& T_ptr, std::vector<int>& T_a,
-                          std::vector<int>& T_b, std::vector<int>& U_ptr, std::vector<int>& U_col,
-                          std::vector<int>& U_src) {
-  const int nv = m->n_verts, nt = m->n_tris;
-  const int* tris = m->tris;
-  // --- K pattern and the face contributions of every entry
-  std::vector<int> vf_ptr, vf_face, vf_corner;
-  vertex_faces(nv, nt, tris, vf_ptr, vf_face, vf_corner);
-  S->K_ptr.assign(nv + 1, 0);
-  S->K_col.clear();
-  S->K_col.reserve((size_t)nv * 8);
-  std::vector<int> nb;
-  for (int u = 0; u < nv; ++u) {
-    nb.clear();
-    nb.push_back(u);
-    for (int q = vf_ptr[u]; q < vf_ptr[u + 1]; ++q) {
-      int f = vf_face[q];
-      for (int c = 0; c < 3; ++c) nb.push_back(tris[3 * f + c]);
-    }
-    std::sort(nb.begin(), nb.end());
-    nb.erase(std::unique(nb.begin(), nb.end()), nb.end());
-    S->K_col.insert(S->K_col.end(), nb.begin(), nb.end());
-    S->K_ptr[u + 1] = (int)S->K_col.size();
-  }
-  S->nnzK = (int)S->K_col.size();
-  K_cptr.assign(S->nnzK + 1, 0);
-  auto entry = [&](int u, int v) {
-    int lo = S->K_ptr[u], hi = S->K_ptr[u + 1];
-    return (int)(std::lower_bound(S->K_col.begin() + lo, S->K_col.begin() + hi, v) - S->K_col.begin());
-  };
-  for (int pass = 0; pass < 2; ++pass) {
-    std::vector<int> fill;
-    if (pass == 1) {
-      for (int e = 0; e < S->nnzK; ++e) K_cptr[e + 1] += K_cptr[e];
-      K_contrib.assign(K_cptr[S->nnzK], 0);
-      fill.assign(K_cptr.begin(), K_cptr.end() - 1);
-    }
-    for (int u = 0; u < nv; ++u)
-      for (int q = vf_ptr[u]; q < vf_ptr[u + 1]; ++q) {  // ascending face
-        const int f = vf_face[q], cu = vf_corner[q], a = local_of(cu);
-        for (int c = 0; c < 3; ++c) {
-          const int v = tris[3 * f + c], b = local_of(c);
-          const int e = entry(u, v);
-          const int slot = c == cu ? a : off_slot(a, b);
-          if (pass == 0) K_cptr[e + 1]++;
-          else K_contrib[fill[e]++] = 6 * f + slot;
-        }
-      }
-  }
-  // --- handles, components (every component needs a handle)
-  hidx.assign(nv, -1);
-  for (int h = 0; h < m->n_handles; ++h) {
-    const int v = m->handles[h];
-    if (v < 0 || v >= nv || hidx[v] >= 0) {
-      set_err("handle %d: vertex %d out of range or repeated", h, v);
-      return CN_BAD_INPUT;
-    }
-    hidx[v] = h;
-  }
-  {
-    Dsu dsu(nv);
-    for (int f = 0; f < nt; ++f) {
-      dsu.unite(tris[3 * f], tris[3 * f + 1]);
-      dsu.unite(tris[3 * f], tris[3 * f + 2]);
-    }
-    std::vector<char> has(nv, 0);
-    for (int h = 0; h < m->n_handles; ++h) has[dsu.find(m->handles[h])] = 1;
-    for (int v = 0; v < nv; ++v)
-      if (!has[dsu.find(v)]) {
-        set_err("vertex %d lies in a connected component without a handle", v);
-        return CN_SINGULAR_COMPONENT;
-      }
-  }
-  // --- free unknowns in vertex order; A_nat = K[free, free]
-  std::vector<int> fidx(nv, -1), fverts;
-  for (int v = 0; v < nv; ++v)
-    if (hidx[v] < 0) { fidx[v] = (int)fverts.size(); fverts.push_back(v); }
-  const int n = (int)fverts.size();
-  S->n = n;
-  std::vector<int> Nptr(n + 1, 0), Ncol, Nsrc;
-  Ncol.reserve(S->nnzK);
-  Nsrc.reserve(S->nnzK);
-  for (int i = 0; i < n; ++i) {
-    const int v = fverts[i];
-    for (int e = S->K_ptr[v]; e < S->K_ptr[v + 1]; ++e)
-      if (fidx[S->K_col[e]] >= 0) { Ncol.push_back(fidx[S->K_col[e]]); Nsrc.push_back(e); }
-    Nptr[i + 1] = (int)Ncol.size();
-  }
-  // --- elimination order: natural, or greedy colour (GraphColoring.lean:41-56)
-  std::vector<int> ord(n);
-  std::iota(ord.begin(), ord.end(), 0);
-  std::vector<int> color(n, 0);
-  {
-    std::vector<int> mark;
-    int nc = n ? 1 : 0;
-    for (int i = 0; i < n; ++i) {
-      mark.assign(Nptr[i + 1] - Nptr[i] + 2, 0);
-      for (int p = Nptr[i]; p < Nptr[i + 1]; ++p) {
-        const int j = Ncol[p];
-        if (j < i && color[j] < (int)mark.size()) mark[color[j]] = 1;
-      }
-      int c = 0;
-      while (c < (int)mark.size() && mark[c]) ++c;
-      color[i] = c;
-      nc = std::max(nc, c + 1);
-    }
-    S->ncolors = nc;
-  }
-  if (S->opts.ordering == CN_ORDER_COLOR)
-    std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return color[a] < color[b]; });
-  // level of every unknown in that order; rows sorted by level
-  std::vector<int> posn(n), level(n, 0);
-  for (int i = 0; i < n; ++i) posn[ord[i]] = i;
-  int nlev = n ? 1 : 0;
-  if (S->opts.precond == CN_PRECOND_IC0) {
-    for (int i = 0; i < n; ++i) {
-      const int v = ord[i];
-      int l = 0;
-      for (int p = Nptr[v]; p < Nptr[v + 1]; ++p) {
-        const int u = Ncol[p];
-        if (posn[u] < i) l = std::max(l, level[u] + 1);
-      }
-      level[v] = l;
-      nlev = std::max(nlev, l + 1);
-    }
-  }
-  std::vector<int> perm = ord;
-  std::stable_sort(perm.begin(), perm.end(), [&](int a, int b) { return level[a] < level[b]; });
-  std::vector<int> inv(n);
-  for (int i = 0; i < n; ++i) inv[perm[i]] = i;
-  S->nlev = nlev;
-  S->lev_ptr.assign(nlev + 1, 0);
-  for (int i = 0; i < n; ++i) S->lev_ptr[level[perm[i]] + 1]++;
-  for (int l = 0; l < nlev; ++l) S->lev_ptr[l + 1] += S->lev_ptr[l];
-  S->free_of.resize(n);
-  for (int i = 0; i < n; ++i) S->free_of[i] = fverts[perm[i]];
-  // --- permuted A with its source entries in K
-  S->A_ptr.assign(n + 1, 0);
-  S->A_col.resize(Ncol.size());
-  A_src.resize(Ncol.size());
-  A_diag.assign(n, -1);
-  std::vector<std::pair<int, int>> row;
-  for (int i = 0; i < n; ++i) {
-    const int o = perm[i];
-    row.clear();
-    for (int p = Nptr[o]; p < Nptr[o + 1]; ++p) row.push_back({inv[Ncol[p]], Nsrc[p]});
-    std::sort(row.begin(), row.end());
-    const int base = S->A_ptr[i];
-    for (size_t q = 0; q < row.size(); ++q) {
-      S->A_col[base + q] = row[q].first;
-      A_src[base + q] = row[q].second;
-      if (row[q].first == i) A_diag[i] = base + (int)q;
-    }
-    S->A_ptr[i + 1] = base + (int)row.size();
-    if (A_diag[i] < 0) {
-      set_err("row %d has no diagonal entry", i);
-      return CN_BAD_INPUT;
-    }
-  }
-  S->nnzA = (int)S->A_col.size();
-  // --- strictly-lower L pattern (IC(0): no fill), its tasks, and U = L^T
-  S->L_ptr.assign(n + 1, 0);
-  S->L_col.clear();
-  L_src.clear();
-  if (S->opts.precond == CN_PRECOND_IC0) {
-    for (int i = 0; i < n; ++i) {
-      for (int e = S->A_ptr[i]; e < S->A_ptr[i + 1]; ++e)
-        if (S->A_col[e] < i) { S->L_col.push_back(S->A_col[e]); L_src.push_back(e); }
-      S->L_ptr[i + 1] = (int)S->L_col.size();
-    }
-  }
-  S->nnzL = (int)S->L_col.size();
-  T_ptr.assign(S->nnzL + 1, 0);
-  T_a.clear();
-  T_b.clear();
-  for (int i = 0; i < n; ++i)
-    for (int e = S->L_ptr[i]; e < S->L_ptr[i + 1]; ++e) {
-      const int j = S->L_col[e];
-      int a = S->L_ptr[i], b = S->L_ptr[j];
-      const int bhi = S->L_ptr[j + 1];
-      while (a < e && b < bhi) {  // common k < j, ascending
-        if (S->L_col[a] == S->L_col[b]) { T_a.push_back(a); T_b.push_back(b); ++a; ++b; }
-        else if (S->L_col[a] < S->L_col[b]) ++a;
-        else ++b;
-      }
-      T_ptr[e + 1] = (int)T_a.size();
-    }
-  U_ptr.assign(n + 1, 0);
-  for (int e = 0; e < S->nnzL; ++e) U_ptr[S->L_col[e] + 1]++;
-  for (int i = 0; i < n; ++i) U_ptr[i + 1] += U_ptr[i];
-  U_col.resize(S->nnzL);
-  U_src.resize(S->nnzL);
-  {
-    std::vector<int> fill(U_ptr.begin(), U_ptr.end() - 1);
-    for (int i = 0; i < n; ++i)
-      for (int e = S->L_ptr[i]; e < S->L_ptr[i + 1]; ++e) {
-        const int j = S->L_col[e];
-        U_col[fill[j]] = i;
-        U_src[fill[j]] = e;
-        fill[j]++;
-      }
-  }
-  return CN_OK;
-}
-
-cn_status check_mesh(const cn_mesh_desc* m) {
-  if (!m || m->n_verts < 0 || m->n_tris < 0 || m->n_handles < 0) {
-    set_err("negative sizes");
-    return CN_BAD_INPUT;
-  }
-  if ((m->n_verts && !m->positions) || (m->n_tris && !m->tris) || (m->n_handles && !m->handles)) {
-    set_err("null array");
-    return CN_BAD_INPUT;
-  }
-  for (long long i = 0; i < 3LL * m->n_verts; ++i)
-    if (!std::isfinite(m->positions[i])) {
-      set_err("position %lld is not finite", i / 3);
-      return CN_NAN;
-    }
-  for (int f = 0; f < m->n_tris; ++f) {
-    const int a = m->tris[3 * f], b = m->tris[3 * f + 1], c = m->tris[3 * f + 2];
-    if (a < 0 || b < 0 || c < 0 || a >= m->n_verts || b >= m->n_verts || c >= m->n_verts ||
-        a == b || b == c || a == c) {
-      set_err("triangle %d has an out-of-range or repeated vertex", f);
-      return CN_BAD_INPUT;
-    }
-  }
-  return CN_OK;
-}
-
-cn_status alloc_solve_state(cn_system* S) {
-  const size_t nk = (size_t)std::max(S->n, 1) * S->kmax;
-  CN_CUDA(S->mem.alloc(&S->d_b64, nk));
-  CN_CUDA(S->mem.alloc(&S->d_x64, nk));
-  CN_CUDA(cudaMemset(S->d_x64, 0, sizeof(double) * nk));
+// Lay out the mesh tables and the solve state in one buffer.
+void layout_all(cn::Bump& b, cn_system* S) {
+  cn::layout(b, S->H, S->D);
+  const size_t nk = (size_t)std::max(S->H.n, 1) * S->kmax;
+  S->d_b64 = b.take<double>(nk);
+  S->d_x64 = b.take<double>(nk);
   for (int i = 0; i < 7; ++i) {
-    CN_CUDA(S->mem.alloc(&S->d_w64[i], nk));
-    CN_CUDA(S->mem.alloc(&S->d_w32[i], nk));
-    CN_CUDA(cudaMemset(S->d_w64[i], 0, sizeof(double) * nk));
-    CN_CUDA(cudaMemset(S->d_w32[i], 0, sizeof(float) * nk));
+    S->d_w64[i] = b.take<double>(nk);
+    S->d_w32[i] = b.take<float>(nk);
   }
-  int sms = 0;
-  CN_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, S->device));
-  S->max_grid_alloc = std::max(sms * 8, 1024);
-  CN_CUDA(S->mem.alloc(&S->d_partials, (size_t)cn::kSlots * S->max_grid_alloc * S->kmax));
-  CN_CUDA(S->mem.alloc(&S->d_scal, 64));
-  CN_CUDA(S->mem.alloc(&S->d_ctl, 1));
-  CN_CUDA(S->mem.alloc(&S->d_stats, 1));
-  CN_CUDA(S->mem.alloc(&S->d_targets, (size_t)std::max(S->nh, S->n) * S->kmax + 1));
-  CN_CUDA(S->mem.alloc(&S->d_x0, (size_t)S->nv * S->kmax + 1));
-  CN_CUDA(S->mem.alloc(&S->d_xout, (size_t)S->nv * S->kmax + 1));
-  return CN_OK;
+  S->d_partials = b.take<double>((size_t)cn::kSlots * S->max_grid_alloc * S->kmax);
+  S->d_scal = b.take<double>(64);
+  S->d_ctl = b.take<Control>(1);
+  S->d_stats = b.take<DevStats>(1);
+  S->d_targets = b.take<double>((size_t)std::max(S->H.nh, S->H.n) * S->kmax + 1);
+  S->d_xout = b.take<double>((size_t)S->H.nv * S->kmax + 1);
+  S->d_status = b.take<int>(1);
 }
 
 void choose_launch(cn_system* S) {
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, S->device);
   S->lanes = S->opts.lanes > 0 ? S->opts.lanes : 2;
-  if (S->n <= 12288) {
+  if (S->H.n <= 12288) {
     S->block = S->opts.block > 0 ? S->opts.block : 1024;
     S->grid = S->opts.grid > 0 ? S->opts.grid : 1;
   } else {
@@ -454,7 +127,7 @@ const char* cn_status_string(int32_t s) {
   return kStatusText[s];
 }
 
-const char* cn_last_error(void) { return g_err.c_str(); }
+const char* cn_last_error(void) { return cn::last_err(); }
 
 cn_status cn_cut_mesh(int32_t nv, int32_t nt, const int32_t* tris, int32_t nloops,
                       const int32_t* loop_ptr, const int32_t* loop_verts, int32_t* tris_out,
@@ -469,7 +142,7 @@ cn_status cn_cut_mesh(int32_t nv, int32_t nt, const int32_t* tris, int32_t nloop
       return CN_BAD_INPUT;
     }
   std::vector<int> vf_ptr, vf_face, vf_corner;
-  vertex_faces(nv, nt, tris, vf_ptr, vf_face, vf_corner);
+  cn::vertex_faces(nv, nt, tris, vf_ptr, vf_face, vf_corner);
   std::memcpy(tris_out, tris, sizeof(int32_t) * 3 * (size_t)nt);
   for (int v = 0; v < nv; ++v) parent_out[v] = v;
   std::vector<char> seen(nv, 0);
@@ -516,13 +189,13 @@ cn_status cn_cut_mesh(int32_t nv, int32_t nt, const int32_t* tris, int32_t nloop
 }
 
 cn_status cn_build(const cn_mesh_desc* mesh, const cn_build_opts* opts, cn_handle* out) {
-  g_err.clear();
+  cn::set_last_error_text("");
   if (!out) {
     set_err("out is NULL");
     return CN_BAD_INPUT;
   }
   *out = nullptr;
-  cn_status st = check_mesh(mesh);
+  cn_status st = cn::check_mesh(mesh);
   if (st != CN_OK) return st;
   cn_build_opts o;
   if (opts) o = *opts;
@@ -552,114 +225,38 @@ cn_status cn_build(const cn_mesh_desc* mesh, const cn_build_opts* opts, cn_handl
   S->opts = o;
   S->device = o.device;
   S->kmax = o.max_rhs;
-  S->nv = mesh->n_verts;
-  S->nt = mesh->n_tris;
-  S->nh = mesh->n_handles;
-  S->handles.assign(mesh->handles, mesh->handles + mesh->n_handles);
   auto fail = [&](cn_status s) {
     cn_destroy(S);
     return s;
   };
-  std::vector<int> K_cptr, K_contrib, hidx, A_src, A_diag, L_src, T_ptr, T_a, T_b, U_ptr, U_col,
-      U_src;
-  st = build_structure(S, mesh, K_cptr, K_contrib, hidx, A_src, A_diag, L_src, T_ptr, T_a, T_b,
-                       U_ptr, U_col, U_src);
+  st = cn::build_host(mesh, o, S->H);
   if (st != CN_OK) return fail(st);
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, S->device);
+  S->max_grid_alloc = std::max(sms * 8, 1024);
   if (cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreate(&S->ev0) != cudaSuccess || cudaEventCreate(&S->ev1) != cudaSuccess) {
     set_err("stream/event creation failed");
     return fail(CN_CUDA_ERROR);
   }
-  DevArena& M = S->mem;
-  std::vector<double> pos(mesh->positions, mesh->positions + 3 * (size_t)S->nv);
-  std::vector<int> tris(mesh->tris, mesh->tris + 3 * (size_t)S->nt);
-#define UP(dst, vec)                                     \
-  if (M.upload(&(dst), (vec)) != cudaSuccess) {          \
-    set_err("device allocation/upload of " #vec " failed"); \
-    return fail(CN_CUDA_ERROR);                          \
-  }
-  UP(S->d_pos, pos);
-  UP(S->d_tris, tris);
-  UP(S->d_K_ptr, S->K_ptr);
-  UP(S->d_K_col, S->K_col);
-  UP(S->d_K_cptr, K_cptr);
-  UP(S->d_K_contrib, K_contrib);
-  UP(S->d_hidx, hidx);
-  UP(S->d_free_of, S->free_of);
-  UP(S->d_handles, S->handles);
-  UP(S->d_A_ptr, S->A_ptr);
-  UP(S->d_A_col, S->A_col);
-  UP(S->d_A_src, A_src);
-  UP(S->d_A_diag, A_diag);
-  UP(S->d_lev_ptr, S->lev_ptr);
-  UP(S->d_L_ptr, S->L_ptr);
-  UP(S->d_L_col, S->L_col);
-  UP(S->d_L_src, L_src);
-  UP(S->d_T_ptr, T_ptr);
-  UP(S->d_T_a, T_a);
-  UP(S->d_T_b, T_b);
-  UP(S->d_U_ptr, U_ptr);
-  UP(S->d_U_col, U_col);
-  UP(S->d_U_src, U_src);
-#undef UP
-  if (M.alloc(&S->d_face_m, 6 * (size_t)S->nt) || M.alloc(&S->d_K_val, S->nnzK) ||
-      M.alloc(&S->d_A64, S->nnzA) || M.alloc(&S->d_A32, S->nnzA) ||
-      M.alloc(&S->d_L64, S->nnzL) || M.alloc(&S->d_L32, S->nnzL) ||
-      M.alloc(&S->d_U64, S->nnzL) || M.alloc(&S->d_U32, S->nnzL) ||
-      M.alloc(&S->d_Ld64, S->n) || M.alloc(&S->d_dinv64, S->n) || M.alloc(&S->d_dinv32, S->n) ||
-      M.alloc(&S->d_status, 1)) {
-    set_err("device allocation failed");
+  cn::Bump sizing;
+  layout_all(sizing, S);
+  if (cudaMalloc((void**)&S->buf, sizing.off) != cudaSuccess) {
+    set_err("device allocation of %zu bytes failed", sizing.off);
     return fail(CN_CUDA_ERROR);
   }
-  st = alloc_solve_state(S);
+  S->bytes = sizing.off;
+  cn::Bump real;
+  real.base = S->buf;
+  layout_all(real, S);
+  if (cudaMemsetAsync(S->buf, 0, S->bytes, S->stream) != cudaSuccess) {
+    set_err("device memset failed");
+    return fail(CN_CUDA_ERROR);
+  }
+  st = cn::upload(S->H, S->D, S->stream);
   if (st != CN_OK) return fail(st);
-
-  BuildArgs b{};
-  b.nv = S->nv; b.nt = S->nt; b.nnzK = S->nnzK; b.n = S->n; b.nnzA = S->nnzA;
-  b.nnzL = S->nnzL; b.nlev = S->nlev;
-  b.pos = S->d_pos; b.tris = S->d_tris; b.lap_kind = o.laplacian; b.delta = o.mollify_delta;
-  b.face_m = S->d_face_m; b.K_cptr = S->d_K_cptr; b.K_contrib = S->d_K_contrib; b.K_val = S->d_K_val;
-  b.A_src = S->d_A_src; b.A_val64 = S->d_A64; b.A_val32 = S->d_A32; b.A_diag = S->d_A_diag;
-  b.lev_ptr = S->d_lev_ptr; b.h_lev_ptr = S->lev_ptr.data();
-  b.L_ptr = S->d_L_ptr; b.L_src = S->d_L_src; b.L_col = S->d_L_col;
-  b.T_ptr = S->d_T_ptr; b.T_a = S->d_T_a; b.T_b = S->d_T_b;
-  b.L_val64 = S->d_L64; b.L_val32 = S->d_L32; b.Ld64 = S->d_Ld64;
-  b.dinv64 = S->d_dinv64; b.dinv32 = S->d_dinv32;
-  b.U_src = S->d_U_src; b.U_val64 = S->d_U64; b.U_val32 = S->d_U32;
-  b.status = S->d_status; b.precond = o.precond;
-  if (cn::launch_assemble(b, S->stream) != cudaSuccess) {
-    set_err("assembly launch failed: %s", cudaGetErrorString(cudaGetLastError()));
-    return fail(CN_CUDA_ERROR);
-  }
-  // IC(0) with Manteuffel diagonal-shift retries on a non-positive pivot.
-  const double shifts[] = {0.0, 1e-3, 1e-2, 1e-1};
-  int bad = -1;
-  for (double sh : shifts) {
-    const int ok = 0x7fffffff;
-    if (cudaMemcpyAsync(S->d_status, &ok, sizeof ok, cudaMemcpyHostToDevice, S->stream) != cudaSuccess) {
-      set_err("status reset failed");
-      return fail(CN_CUDA_ERROR);
-    }
-    b.shift = sh;
-    if (cn::launch_factor(b, S->stream) != cudaSuccess) {
-      set_err("factor launch failed");
-      return fail(CN_CUDA_ERROR);
-    }
-    int h_status = 0;
-    if (cudaMemcpyAsync(&h_status, S->d_status, sizeof h_status, cudaMemcpyDeviceToHost, S->stream) !=
-            cudaSuccess ||
-        cudaStreamSynchronize(S->stream) != cudaSuccess) {
-      set_err("factor failed: %s", cudaGetErrorString(cudaGetLastError()));
-      return fail(CN_CUDA_ERROR);
-    }
-    bad = h_status == ok ? -1 : h_status;
-    S->shift_used = sh;
-    if (bad < 0) break;
-  }
-  if (bad >= 0) {
-    set_err("IC(0) pivot of row %d is not positive", bad);
-    return fail(CN_NONPOS_PIVOT);
-  }
+  st = cn::assemble_factor(S->H, S->D, o, S->d_status, S->stream, &S->shift_used);
+  if (st != CN_OK) return fail(st);
   choose_launch(S);
   *out = S;
   return CN_OK;
@@ -669,7 +266,10 @@ void cn_destroy(cn_handle S) {
   if (!S) return;
   cudaSetDevice(S->device);
   if (S->stream) cudaStreamSynchronize(S->stream);
-  S->mem.release();
+  if (S->buf) cudaFree(S->buf);
+  for (void* p : {(void*)S->d_curve_of, (void*)S->d_row_of, (void*)S->d_tau, (void*)S->d_rest_cp,
+                  (void*)S->d_posed_cp, (void*)S->d_weights, (void*)S->d_dLdx, (void*)S->d_dP, (void*)S->d_dw})
+    if (p) cudaFree(p);
   if (S->ev0) cudaEventDestroy(S->ev0);
   if (S->ev1) cudaEventDestroy(S->ev1);
   if (S->stream) cudaStreamDestroy(S->stream);
@@ -680,8 +280,9 @@ void* cn_stream(cn_handle S) { return S ? (void*)S->stream : nullptr; }
 
 cn_status cn_system_info(cn_handle S, int64_t* info) {
   if (!S || !info) return CN_BAD_INPUT;
-  int64_t v[12] = {S->n, S->nnzA, S->nnzL, S->nlev, S->nnzK, S->nv, S->nh,
-                   S->grid, S->block, S->lanes, S->ncolors, (int64_t)S->mem.bytes};
+  const MeshHost& H = S->H;
+  int64_t v[12] = {H.n, H.nnzA, H.nnzL, H.nlev, H.nnzK, H.nv, H.nh,
+                   S->grid, S->block, S->lanes, H.ncolors, (int64_t)S->bytes};
   std::memcpy(info, v, sizeof v);
   return CN_OK;
 }
@@ -735,19 +336,7 @@ cn_status cn_solve_device(cn_handle S, int32_t k, const double* d_targets, doubl
   CN_CUDA(cudaSetDevice(S->device));
   if (o.algo == CN_ALGO_PLAIN) return solve_plain(S, k, d_targets, d_xout, &o, stats);
   const bool mixed = o.precision == CN_PREC_MIXED;
-  SolveArgs a{};
-  a.n = S->n; a.nlev = S->nlev; a.lev_ptr = S->d_lev_ptr;
-  a.A_ptr = S->d_A_ptr; a.A_col = S->d_A_col;
-  a.A_val = mixed ? (const void*)S->d_A32 : (const void*)S->d_A64;
-  a.A_val64 = S->d_A64;
-  a.L_ptr = S->d_L_ptr; a.L_col = S->d_L_col;
-  a.L_val = mixed ? (const void*)S->d_L32 : (const void*)S->d_L64;
-  a.U_ptr = S->d_U_ptr; a.U_col = S->d_U_col;
-  a.U_val = mixed ? (const void*)S->d_U32 : (const void*)S->d_U64;
-  a.dinv = mixed ? (const void*)S->d_dinv32 : (const void*)S->d_dinv64;
-  a.nv = S->nv; a.nh = S->nh;
-  a.K_ptr = S->d_K_ptr; a.K_col = S->d_K_col; a.K_val = S->d_K_val;
-  a.free_of = S->d_free_of; a.hidx = S->d_hidx; a.handles = S->d_handles; a.pos = S->d_pos;
+  SolveArgs a = cn::solve_args(S->H, S->D, mixed);
   a.mode = o.mode; a.targets = d_targets; a.x_out = d_xout; a.x0 = nullptr;
   a.warm = o.warm_start && S->have_solution ? 1 : 0;
   a.b64 = S->d_b64; a.x64 = S->d_x64;
@@ -792,7 +381,8 @@ cn_status cn_solve(cn_handle S, int32_t k, const double* targets, const double* 
   if (opts) o = *opts;
   else cn_default_solve_opts(&o);
   CN_CUDA(cudaSetDevice(S->device));
-  const size_t nt = (size_t)(o.mode == CN_MODE_RHS ? S->n : S->nh) * k;
+  const MeshHost& H = S->H;
+  const size_t nt = (size_t)(o.mode == CN_MODE_RHS ? H.n : H.nh) * k;
   for (size_t i = 0; i < nt; ++i)
     if (!std::isfinite(targets[i])) {
       set_err("target %zu is not finite", i);
@@ -801,9 +391,9 @@ cn_status cn_solve(cn_handle S, int32_t k, const double* targets, const double* 
   if (nt) CN_CUDA(cudaMemcpyAsync(S->d_targets, targets, sizeof(double) * nt, cudaMemcpyHostToDevice, S->stream));
   if (x0) {
     // the initial guess enters as the warm-start state, gathered to solve order
-    std::vector<double> xs((size_t)S->n * k);
-    for (int i = 0; i < S->n; ++i)
-      for (int c = 0; c < k; ++c) xs[(size_t)i * k + c] = x0[(size_t)S->free_of[i] * k + c];
+    std::vector<double> xs((size_t)H.n * k);
+    for (int i = 0; i < H.n; ++i)
+      for (int c = 0; c < k; ++c) xs[(size_t)i * k + c] = x0[(size_t)H.free_of[i] * k + c];
     CN_CUDA(cudaMemcpyAsync(S->d_x64, xs.data(), sizeof(double) * xs.size(), cudaMemcpyHostToDevice,
                             S->stream));
     CN_CUDA(cudaStreamSynchronize(S->stream));
@@ -813,7 +403,7 @@ cn_status cn_solve(cn_handle S, int32_t k, const double* targets, const double* 
   cn_solve_stats local;
   cn_status st = cn_solve_device(S, k, S->d_targets, S->d_xout, &o, stats ? stats : &local);
   if (st != CN_OK && st != CN_MAX_ITER) return st;
-  CN_CUDA(cudaMemcpyAsync(x_out, S->d_xout, sizeof(double) * (size_t)S->nv * k, cudaMemcpyDeviceToHost,
+  CN_CUDA(cudaMemcpyAsync(x_out, S->d_xout, sizeof(double) * (size_t)H.nv * k, cudaMemcpyDeviceToHost,
                           S->stream));
   CN_CUDA(cudaStreamSynchronize(S->stream));
   return st;
@@ -825,16 +415,16 @@ cn_status cn_solve(cn_handle S, int32_t k, const double* targets, const double* 
 static cn_status solve_plain(cn_handle S, int k, const double* d_targets, double* d_xout,
                              const cn_solve_opts* o, cn_solve_stats* stats) {
   cn::PlainArgs p{};
-  p.n = S->n; p.K = k;
-  p.A_ptr = S->d_A_ptr; p.A_col = S->d_A_col; p.A_val = S->d_A64; p.A_diag = S->d_A_diag;
+  p.n = S->H.n; p.K = k;
+  p.A_ptr = S->D.A_ptr; p.A_col = S->D.A_col; p.A_val = S->D.A64; p.A_diag = S->D.A_diag;
   p.b = S->d_b64; p.x = S->d_x64;
   p.r = S->d_w64[0]; p.z = S->d_w64[1]; p.p = S->d_w64[2]; p.Ap = S->d_w64[3];
   p.blocks = 120;
   p.partials = S->d_partials;
   double* d_scal = S->d_scal;
   SolveArgs sa{};
-  sa.nv = S->nv; sa.nh = S->nh; sa.K_ptr = S->d_K_ptr; sa.K_col = S->d_K_col; sa.K_val = S->d_K_val;
-  sa.free_of = S->d_free_of; sa.hidx = S->d_hidx; sa.handles = S->d_handles; sa.pos = S->d_pos;
+  sa.nv = S->H.nv; sa.nh = S->H.nh; sa.K_ptr = S->D.K_ptr; sa.K_col = S->D.K_col; sa.K_val = S->D.K_val;
+  sa.free_of = S->D.free_of; sa.hidx = S->D.hidx; sa.handles = S->D.handles; sa.pos = S->D.pos;
   sa.mode = o->mode; sa.targets = d_targets; sa.x_out = d_xout; sa.x0 = nullptr;
   std::vector<double> part((size_t)p.blocks * k), alpha(k), beta(k), rz(k), bb(k), rr(k);
   std::vector<int> active(k, 1);
@@ -892,7 +482,7 @@ static cn_status solve_plain(cn_handle S, int k, const double* d_targets, double
   CN_CUDA(cudaEventRecord(S->ev1, S->stream));
   CN_CUDA(cudaStreamSynchronize(S->stream));
   S->have_solution = false;  // the plain path does not keep the warm-start layout
-  CN_CUDA(cudaMemsetAsync(S->d_x64, 0, sizeof(double) * (size_t)S->n * S->kmax, S->stream));
+  CN_CUDA(cudaMemsetAsync(S->d_x64, 0, sizeof(double) * (size_t)S->H.n * S->kmax, S->stream));
   double mx = 0.0;
   cn_status res = CN_OK;
   cn_solve_stats local{};
@@ -915,28 +505,162 @@ static cn_status solve_plain(cn_handle S, int k, const double* d_targets, double
   return res;
 }
 
+// ---------------------------------------------------------------------------
+// Profile curves -> handle targets, deform, adjoint (cn_adjoint.cu).
+static cn::CurveArgs curve_args(cn_handle S) {
+  cn::CurveArgs c{};
+  c.nh = S->H.nh; c.ncurves = S->ncurves; c.nseg = S->nseg;
+  c.handles = S->D.handles; c.curve_of = S->d_curve_of; c.tau = S->d_tau;
+  c.rest_cp = S->d_rest_cp; c.posed_cp = S->d_posed_cp; c.weights = S->d_weights; c.pos = S->D.pos;
+  return c;
+}
+
+cn_status cn_bind_curves(cn_handle S, int32_t n_curves, int32_t n_segments, const double* rest_cp,
+                         const int32_t* curve_of, const double* tau) {
+  if (!S || n_curves < 1 || n_segments < 1 || !rest_cp || !curve_of || !tau) {
+    set_err("bad curve binding arguments");
+    return CN_BAD_INPUT;
+  }
+  const MeshHost& H = S->H;
+  for (int h = 0; h < H.nh; ++h)
+    if (curve_of[h] >= n_curves || !std::isfinite(tau[h]) || tau[h] < 0.0 || tau[h] > n_segments) {
+      set_err("handle %d: curve %d / parameter out of range", h, curve_of[h]);
+      return CN_BAD_INPUT;
+    }
+  const size_t ncp = (size_t)n_curves * (3 * n_segments + 1) * 3;
+  for (size_t i = 0; i < ncp; ++i)
+    if (!std::isfinite(rest_cp[i])) {
+      set_err("rest control point %zu is not finite", i);
+      return CN_NAN;
+    }
+  CN_CUDA(cudaSetDevice(S->device));
+  for (void* p : {(void*)S->d_curve_of, (void*)S->d_row_of, (void*)S->d_tau, (void*)S->d_rest_cp,
+                  (void*)S->d_posed_cp, (void*)S->d_weights, (void*)S->d_dLdx, (void*)S->d_dP, (void*)S->d_dw})
+    if (p) cudaFree(p);
+  S->ncurves = n_curves;
+  S->nseg = n_segments;
+  S->have_forward = false;
+  std::vector<int> row_of(H.nv, -1);
+  for (int i = 0; i < H.n; ++i) row_of[H.free_of[i]] = i;
+  CN_CUDA(cudaMalloc((void**)&S->d_curve_of, sizeof(int) * std::max(H.nh, 1)));
+  CN_CUDA(cudaMalloc((void**)&S->d_row_of, sizeof(int) * std::max(H.nv, 1)));
+  CN_CUDA(cudaMalloc((void**)&S->d_tau, sizeof(double) * std::max(H.nh, 1)));
+  CN_CUDA(cudaMalloc((void**)&S->d_rest_cp, sizeof(double) * ncp));
+  CN_CUDA(cudaMalloc((void**)&S->d_posed_cp, sizeof(double) * ncp));
+  CN_CUDA(cudaMalloc((void**)&S->d_weights, sizeof(double) * n_curves));
+  CN_CUDA(cudaMalloc((void**)&S->d_dLdx, sizeof(double) * 3 * std::max(H.nv, 1)));
+  CN_CUDA(cudaMalloc((void**)&S->d_dP, sizeof(double) * ncp));
+  CN_CUDA(cudaMalloc((void**)&S->d_dw, sizeof(double) * n_curves));
+  if (H.nh) {
+    CN_CUDA(cudaMemcpy(S->d_curve_of, curve_of, sizeof(int) * H.nh, cudaMemcpyHostToDevice));
+    CN_CUDA(cudaMemcpy(S->d_tau, tau, sizeof(double) * H.nh, cudaMemcpyHostToDevice));
+  }
+  CN_CUDA(cudaMemcpy(S->d_row_of, row_of.data(), sizeof(int) * H.nv, cudaMemcpyHostToDevice));
+  CN_CUDA(cudaMemcpy(S->d_rest_cp, rest_cp, sizeof(double) * ncp, cudaMemcpyHostToDevice));
+  return CN_OK;
+}
+
+cn_status cn_deform(cn_handle S, const double* posed_cp, const double* weights, double* x_out,
+                    const cn_solve_opts* opts, cn_solve_stats* stats) {
+  if (!S || !posed_cp || !weights || !x_out) {
+    set_err("null argument");
+    return CN_BAD_INPUT;
+  }
+  if (!S->ncurves) {
+    set_err("no curves bound (cn_bind_curves)");
+    return CN_BAD_INPUT;
+  }
+  const size_t ncp = (size_t)S->ncurves * (3 * S->nseg + 1) * 3;
+  for (size_t i = 0; i < ncp; ++i)
+    if (!std::isfinite(posed_cp[i])) {
+      set_err("posed control point %zu is not finite", i);
+      return CN_NAN;
+    }
+  for (int c = 0; c < S->ncurves; ++c)
+    if (!std::isfinite(weights[c])) {
+      set_err("weight %d is not finite", c);
+      return CN_NAN;
+    }
+  cn_solve_opts o;
+  if (opts) o = *opts;
+  else cn_default_solve_opts(&o);
+  o.mode = CN_MODE_DEFORM;
+  CN_CUDA(cudaSetDevice(S->device));
+  CN_CUDA(cudaMemcpyAsync(S->d_posed_cp, posed_cp, sizeof(double) * ncp, cudaMemcpyHostToDevice, S->stream));
+  CN_CUDA(cudaMemcpyAsync(S->d_weights, weights, sizeof(double) * S->ncurves, cudaMemcpyHostToDevice, S->stream));
+  CN_CUDA(cn::launch_curve_targets(curve_args(S), S->d_targets, S->stream));
+  cn_solve_stats local;
+  cn_status st = cn_solve_device(S, 3, S->d_targets, S->d_xout, &o, stats ? stats : &local);
+  if (st != CN_OK && st != CN_MAX_ITER) return st;
+  CN_CUDA(cudaMemcpyAsync(x_out, S->d_xout, sizeof(double) * 3 * (size_t)S->H.nv, cudaMemcpyDeviceToHost,
+                          S->stream));
+  CN_CUDA(cudaStreamSynchronize(S->stream));
+  S->have_forward = true;
+  return st;
+}
+
+cn_status cn_adjoint(cn_handle S, const double* dL_dx, double* dL_dcp, double* dL_dw, const cn_solve_opts* opts,
+                     cn_solve_stats* stats) {
+  if (!S || !dL_dx || !dL_dcp || !dL_dw) {
+    set_err("null argument");
+    return CN_BAD_INPUT;
+  }
+  if (!S->have_forward) {
+    set_err("cn_adjoint needs a preceding cn_deform on this handle");
+    return CN_BAD_INPUT;
+  }
+  const MeshHost& H = S->H;
+  for (size_t i = 0; i < 3 * (size_t)H.nv; ++i)
+    if (!std::isfinite(dL_dx[i])) {
+      set_err("dL/dx %zu is not finite", i);
+      return CN_NAN;
+    }
+  cn_solve_opts o;
+  if (opts) o = *opts;
+  else cn_default_solve_opts(&o);
+  o.mode = CN_MODE_RHS;
+  o.warm_start = 0;
+  CN_CUDA(cudaSetDevice(S->device));
+  CN_CUDA(cudaMemcpyAsync(S->d_dLdx, dL_dx, sizeof(double) * 3 * H.nv, cudaMemcpyHostToDevice, S->stream));
+  CN_CUDA(cn::launch_adjoint_rhs(H.n, S->D.free_of, S->d_dLdx, S->d_targets, S->stream));
+  // A lambda = g_f with the same factor (A is symmetric); lambda lands in x64.
+  cn_solve_stats local;
+  cn_status st = cn_solve_device(S, 3, S->d_targets, nullptr, &o, stats ? stats : &local);
+  S->have_solution = false;  // x64 now holds lambda, not a warm start
+  if (st != CN_OK && st != CN_MAX_ITER) return st;
+  CN_CUDA(cn::launch_adjoint_grad(curve_args(S), S->D.K_ptr, S->D.K_col, S->D.K_val, S->d_row_of, S->d_x64,
+                                  S->d_dLdx, S->d_dP, S->d_dw, S->stream));
+  const size_t ncp = (size_t)S->ncurves * (3 * S->nseg + 1) * 3;
+  CN_CUDA(cudaMemcpyAsync(dL_dcp, S->d_dP, sizeof(double) * ncp, cudaMemcpyDeviceToHost, S->stream));
+  CN_CUDA(cudaMemcpyAsync(dL_dw, S->d_dw, sizeof(double) * S->ncurves, cudaMemcpyDeviceToHost, S->stream));
+  CN_CUDA(cudaStreamSynchronize(S->stream));
+  return st;
+}
+
 cn_status cn_export_csr(cn_handle S, int32_t* free_of, int32_t* rowptr, int32_t* colidx,
                         double* vals) {
   if (!S) return CN_BAD_INPUT;
   CN_CUDA(cudaSetDevice(S->device));
-  if (free_of) std::memcpy(free_of, S->free_of.data(), sizeof(int) * S->n);
-  if (rowptr) std::memcpy(rowptr, S->A_ptr.data(), sizeof(int) * (S->n + 1));
-  if (colidx) std::memcpy(colidx, S->A_col.data(), sizeof(int) * S->nnzA);
-  if (vals) CN_CUDA(cudaMemcpy(vals, S->d_A64, sizeof(double) * S->nnzA, cudaMemcpyDeviceToHost));
+  const MeshHost& H = S->H;
+  if (free_of) std::memcpy(free_of, H.free_of.data(), sizeof(int) * H.n);
+  if (rowptr) std::memcpy(rowptr, H.A_ptr.data(), sizeof(int) * (H.n + 1));
+  if (colidx) std::memcpy(colidx, H.A_col.data(), sizeof(int) * H.nnzA);
+  if (vals) CN_CUDA(cudaMemcpy(vals, S->D.A64, sizeof(double) * H.nnzA, cudaMemcpyDeviceToHost));
   return CN_OK;
 }
 
 cn_status cn_export_factor(cn_handle S, int32_t* rowptr, int32_t* colidx, double* vals) {
   if (!S) return CN_BAD_INPUT;
   CN_CUDA(cudaSetDevice(S->device));
-  std::vector<double> L(S->nnzL), d(S->n);
-  if (S->nnzL) CN_CUDA(cudaMemcpy(L.data(), S->d_L64, sizeof(double) * S->nnzL, cudaMemcpyDeviceToHost));
-  if (S->n) CN_CUDA(cudaMemcpy(d.data(), S->d_Ld64, sizeof(double) * S->n, cudaMemcpyDeviceToHost));
+  const MeshHost& H = S->H;
+  std::vector<double> L(H.nnzL), d(H.n);
+  if (H.nnzL) CN_CUDA(cudaMemcpy(L.data(), S->D.L64, sizeof(double) * H.nnzL, cudaMemcpyDeviceToHost));
+  if (H.n) CN_CUDA(cudaMemcpy(d.data(), S->D.Ld64, sizeof(double) * H.n, cudaMemcpyDeviceToHost));
   int q = 0;
   if (rowptr) rowptr[0] = 0;
-  for (int i = 0; i < S->n; ++i) {
-    for (int e = S->L_ptr[i]; e < S->L_ptr[i + 1]; ++e, ++q) {
-      if (colidx) colidx[q] = S->L_col[e];
+  for (int i = 0; i < H.n; ++i) {
+    for (int e = H.L_ptr[i]; e < H.L_ptr[i + 1]; ++e, ++q) {
+      if (colidx) colidx[q] = H.L_col[e];
       if (vals) vals[q] = L[e];
     }
     if (colidx) colidx[q] = i;
@@ -950,9 +674,10 @@ cn_status cn_export_factor(cn_handle S, int32_t* rowptr, int32_t* colidx, double
 cn_status cn_export_k(cn_handle S, int32_t* rowptr, int32_t* colidx, double* vals) {
   if (!S) return CN_BAD_INPUT;
   CN_CUDA(cudaSetDevice(S->device));
-  if (rowptr) std::memcpy(rowptr, S->K_ptr.data(), sizeof(int) * (S->nv + 1));
-  if (colidx) std::memcpy(colidx, S->K_col.data(), sizeof(int) * S->nnzK);
-  if (vals) CN_CUDA(cudaMemcpy(vals, S->d_K_val, sizeof(double) * S->nnzK, cudaMemcpyDeviceToHost));
+  const MeshHost& H = S->H;
+  if (rowptr) std::memcpy(rowptr, H.K_ptr.data(), sizeof(int) * (H.nv + 1));
+  if (colidx) std::memcpy(colidx, H.K_col.data(), sizeof(int) * H.nnzK);
+  if (vals) CN_CUDA(cudaMemcpy(vals, S->D.K_val, sizeof(double) * H.nnzK, cudaMemcpyDeviceToHost));
   return CN_OK;
 }
 

@@ -131,6 +131,23 @@ struct BuildArgs {
 cudaError_t launch_assemble(const BuildArgs& b, cudaStream_t s);
 cudaError_t launch_factor(const BuildArgs& b, cudaStream_t s);
 
+// Profile-curve binding of the handles (cn_adjoint.cu).
+struct CurveArgs {
+  int nh, ncurves, nseg;
+  const int* handles;     // handle -> vertex
+  const int* curve_of;    // handle -> curve or -1
+  const double* tau;      // handle -> curve parameter in [0, nseg]
+  const double* rest_cp;  // ncurves x (3 nseg + 1) x 3
+  const double* posed_cp;
+  const double* weights;  // ncurves
+  const double* pos;      // rest positions
+};
+cudaError_t launch_curve_targets(const CurveArgs& c, double* targets, cudaStream_t s);
+cudaError_t launch_adjoint_rhs(int n, const int* free_of, const double* dLdx, double* b, cudaStream_t s);
+cudaError_t launch_adjoint_grad(const CurveArgs& c, const int* K_ptr, const int* K_col, const double* K_val,
+                                const int* row_of, const double* lambda, const double* dLdx, double* dP,
+                                double* dw, cudaStream_t s);
+
 // Plain FP64 Jacobi-PCG with one kernel per primitive and the scalars folded
 // on the host each iteration (the reference's GPU orchestration).
 struct PlainArgs {

@@ -217,3 +217,102 @@ def solve_deformation(positions, tris, handles, Xc, **kw):
     solve that reproduces the rest pose when X_c is the rest handle position."""
     with CutMeshSolver(positions, tris, handles, max_rhs=3) as s:
         return s.solve(_f64(Xc).reshape(-1, 3), mode="deform", **kw).x
+
+
+class BatchSolver:
+    """Many cut meshes solved together: one persistent, CUDA-graph-captured
+    launch per solve of all meshes x k right-hand sides (cn_build_batch /
+    cn_solve_batch).  meshes: list of (positions, tris, handles)."""
+
+    def __init__(self, meshes, k=24, precond="ic0", ordering="color", laplacian="cot",
+                 mollify_delta=1e-4, device=0, cluster_size=0, n_clusters=0, block=0):
+        self.k = k
+        self._keep = []
+        descs = (L.MeshDesc * len(meshes))()
+        self.n_verts = []
+        self.n_handles = []
+        for i, (pos, tris, h) in enumerate(meshes):
+            pos = _f64(pos).reshape(-1, 3)
+            tris = _i32(tris).reshape(-1, 3)
+            h = _i32(h).reshape(-1)
+            self._keep += [pos, tris, h]
+            descs[i] = L.MeshDesc(pos.shape[0], tris.shape[0], _dp(pos), _ip(tris), h.size, _ip(h))
+            self.n_verts.append(pos.shape[0])
+            self.n_handles.append(h.size)
+        opts = L.BuildOpts()
+        L.lib().cn_default_build_opts(C.byref(opts))
+        opts.precond = _PRECOND[precond]
+        opts.ordering = _ORDER[ordering]
+        opts.laplacian = _LAP[laplacian]
+        opts.mollify_delta = mollify_delta
+        opts.device = device
+        opts.block = block
+        h = C.c_void_p()
+        st = L.lib().cn_build_batch(descs, len(meshes), C.byref(opts), k, cluster_size, n_clusters, C.byref(h))
+        self._keep = []
+        if st != L.CN_OK:
+            raise CnError(st, "cn_build_batch")
+        self._h = h
+        self.n_meshes = len(meshes)
+        t = (C.c_int64 * (self.n_meshes + 1))()
+        o = (C.c_int64 * (self.n_meshes + 1))()
+        L.lib().cn_batch_offsets(self._h, t, o)
+        self.tgt_off = np.array(list(t), np.int64)
+        self.out_off = np.array(list(o), np.int64)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            L.lib().cn_destroy_batch(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def info(self):
+        v = (C.c_int64 * 12)()
+        L.lib().cn_batch_info(self._h, v)
+        keys = ["n_meshes", "k", "n_verts", "n_handles", "n_free", "nnz_A", "nnz_L", "cluster_size",
+                "n_clusters", "block", "max_free", "device_bytes"]
+        return dict(zip(keys, list(v)))
+
+    def stream(self):
+        return L.lib().cn_batch_stream(self._h)
+
+    def mesh_stats(self):
+        st = np.zeros(self.n_meshes, np.int32)
+        it = np.zeros(self.n_meshes, np.int32)
+        rel = np.zeros(self.n_meshes)
+        L.lib().cn_batch_mesh_stats(self._h, _ip(st), _ip(it), _dp(rel))
+        return st, it, rel
+
+    def solve(self, targets, check=True, **kw):
+        """targets: list of (n_handles_m, k) arrays.  Returns (list of
+        (n_verts_m, k) arrays, BatchStats)."""
+        flat = np.concatenate([_f64(t).reshape(-1) for t in targets])
+        assert flat.size == self.tgt_off[-1]
+        x = np.empty(int(self.out_off[-1]), np.float64)
+        o = CutMeshSolver.make_opts(**kw)
+        stats = L.BatchStats()
+        st = L.lib().cn_solve_batch(self._h, _dp(flat), _dp(x), C.byref(o), C.byref(stats))
+        if check and st != L.CN_OK:
+            raise CnError(st, "cn_solve_batch")
+        xs = [x[self.out_off[m]:self.out_off[m + 1]].reshape(-1, self.k) for m in range(self.n_meshes)]
+        return xs, stats
+
+    def solve_device(self, d_targets, d_x_out, stats=True, **kw):
+        o = CutMeshSolver.make_opts(**kw)
+        s = L.BatchStats()
+        st = L.lib().cn_solve_batch_device(self._h, C.c_void_p(d_targets), C.c_void_p(d_x_out), C.byref(o),
+                                           C.byref(s) if stats else None)
+        if st != L.CN_OK:
+            raise CnError(st, "cn_solve_batch_device")
+        return s if stats else None

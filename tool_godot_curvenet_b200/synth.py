@@ -198,3 +198,62 @@ def config3_mesh(idx, seed=3):
         m = cylinder(short, long_, 1.0, 4.0, 0.005, cut_rows=cuts, seed=s)
     h = pick_handles(m, 0.02, s + 1)
     return m, h, normal_targets(m.positions, h, 0.1, s + 2, poses=8)
+
+
+def circle_bezier(center, e1, e2, radius, nseg):
+    """Composite cubic Bezier (nseg segments, 3 nseg + 1 points) of the circle
+    center + radius (cos phi e1 + sin phi e2); each arc uses the standard
+    4/3 tan(dphi/4) tangent length."""
+    dphi = 2.0 * np.pi / nseg
+    k = 4.0 / 3.0 * np.tan(dphi / 4.0)
+    pts = []
+    for s in range(nseg):
+        p0, p1 = s * dphi, (s + 1) * dphi
+        c0 = center + radius * (np.cos(p0) * e1 + np.sin(p0) * e2)
+        c1 = center + radius * (np.cos(p1) * e1 + np.sin(p1) * e2)
+        t0 = -np.sin(p0) * e1 + np.cos(p0) * e2
+        t1 = -np.sin(p1) * e1 + np.cos(p1) * e2
+        if s == 0:
+            pts.append(c0)
+        pts += [c0 + k * radius * t0, c1 - k * radius * t1, c1]
+    return np.array(pts)
+
+
+def config4(seed=4, nseg=5):
+    """Torus 128 (major) x 64 (minor) = 8,192 vertices with 4 seams (profile
+    curves) at u = 0, 32, 64, 96.  Handles: every loop vertex and its seam copy,
+    bound to its loop's curve at tau = nseg * v / 64.  Curves: the meridian
+    circles as composite cubic Beziers (nseg = 5 -> 16 control points);
+    posed = rest + N(0, 0.05), weights 1 + U(-0.1, 0.1); the target is the
+    deformed mesh under parameters perturbed by N(0, 0.02).
+    Returns (positions, tris, handles, curve_of, tau, rest_cp, posed_cp,
+    weights, target_cp, target_w) on the cut mesh."""
+    from .solver import cut_mesh
+    U, V, R, r = 128, 64, 3.0, 1.0
+    cuts = (0, 32, 64, 96)
+    m = torus(U, V, R, r, 0.005, cut_u=cuts, seed=seed)
+    tris, parent = cut_mesh(m.positions.shape[0], m.tris, m.loops)
+    pos = np.ascontiguousarray(m.positions[parent])
+    nv0 = m.positions.shape[0]
+    handles, curve_of, tau = [], [], []
+    copy = nv0
+    for c, cu in enumerate(cuts):
+        for v in range(V):
+            for vid in (cu * V + v, copy):
+                handles.append(vid)
+                curve_of.append(c)
+                tau.append(nseg * v / V)
+            copy += 1
+    rng = np.random.Generator(np.random.PCG64(seed + 7))
+    rest_cp = []
+    for cu in cuts:
+        th = 2.0 * np.pi * cu / U
+        er = np.array([np.cos(th), np.sin(th), 0.0])
+        rest_cp.append(circle_bezier(R * er, er, np.array([0.0, 0.0, 1.0]), r, nseg))
+    rest_cp = np.array(rest_cp)
+    posed_cp = rest_cp + rng.normal(0.0, 0.05, rest_cp.shape)
+    weights = 1.0 + rng.uniform(-0.1, 0.1, len(cuts))
+    target_cp = posed_cp + rng.normal(0.0, 0.02, rest_cp.shape)
+    target_w = weights + rng.normal(0.0, 0.02, len(cuts))
+    return (pos, tris, np.array(handles, np.int32), np.array(curve_of, np.int32), np.array(tau),
+            rest_cp, posed_cp, weights, target_cp, target_w)
