@@ -27,6 +27,7 @@ namespace cg = cooperative_groups;
 namespace cn {
 namespace {
 
+using pcg::gather_row;
 using pcg::kBB;
 using pcg::kPAP;
 using pcg::kRR;
@@ -116,6 +117,7 @@ __device__ void solve_body_wide(const SolveArgs& a, const ClusterTeam& team, Sme
   const int row0 = team.rank() * gpb + grp, rstride = team.size() * gpb;
   const int csize = team.size();
   int status = CN_OK, total_iters = 0, refinements = 0;
+  constexpr int UW = 4;  // entries of a row gathered together
 
   // ---- right-hand side (HarmonicSolve.lean:51-66 / DeformSolve.lean:123-135)
   {
@@ -128,18 +130,18 @@ __device__ void solve_body_wide(const SolveArgs& a, const ClusterTeam& team, Sme
       for (int c = 0; c < CPL; ++c) acc[c] = 0.0;
       const int v = a.free_of[row];
       if (a.mode != CN_MODE_RHS) {
-        for (int e = a.K_ptr[v]; e < a.K_ptr[v + 1]; ++e) {
-          const int u = a.K_col[e];
-          const double kv = a.K_val[e];
-          const int h = a.hidx[u];
+        const bool deform = a.mode == CN_MODE_DEFORM;
+        gather_row<CPL, 1, UW>(a.K_ptr[v], a.K_ptr[v + 1], 0, a.K_col, a.K_val,
+                               [&](int u, double* d) {
+                                 const int h = a.hidx[u];
 #pragma unroll
-          for (int c = 0; c < CPL; ++c) {
-            const int cc = c0 + c;
-            const double rest = a.mode == CN_MODE_DEFORM ? a.pos[3 * u + cc % 3] : 0.0;
-            const double d = h >= 0 ? a.targets[(size_t)h * K + cc] - rest : -rest;
-            acc[c] += kv * d;
-          }
-        }
+                                 for (int c = 0; c < CPL; ++c) {
+                                   const int cc = c0 + c;
+                                   const double rest = deform ? a.pos[3 * u + cc % 3] : 0.0;
+                                   d[c] = h >= 0 ? a.targets[(size_t)h * K + cc] - rest : -rest;
+                                 }
+                               },
+                               acc);
       }
 #pragma unroll
       for (int c = 0; c < CPL; ++c) {
@@ -167,12 +169,13 @@ __device__ void solve_body_wide(const SolveArgs& a, const ClusterTeam& team, Sme
         double acc[CPL];
 #pragma unroll
         for (int c = 0; c < CPL; ++c) acc[c] = 0.0;
-        for (int e = a.A_ptr[row]; e < a.A_ptr[row + 1]; ++e) {
-          const double av = a.A_val64[e];
-          const double* xj = a.x64 + (size_t)a.A_col[e] * K + c0;
+        gather_row<CPL, 1, UW>(a.A_ptr[row], a.A_ptr[row + 1], 0, a.A_col, a.A_val64,
+                               [&](int j, double* x) {
+                                 const double* xj = a.x64 + (size_t)j * K + c0;
 #pragma unroll
-          for (int c = 0; c < CPL; ++c) acc[c] += av * xj[c];
-        }
+                                 for (int c = 0; c < CPL; ++c) x[c] = xj[c];
+                               },
+                               acc);
 #pragma unroll
         for (int c = 0; c < CPL; ++c) {
           const size_t ix = (size_t)row * K + c0 + c;
@@ -229,16 +232,22 @@ __device__ void solve_body_wide(const SolveArgs& a, const ClusterTeam& team, Sme
           T acc[CPL];
 #pragma unroll
           for (int c = 0; c < CPL; ++c) acc[c] = (T)0;
-          for (int e = a.A_ptr[row]; e < a.A_ptr[row + 1]; ++e) {
-            const size_t jb = (size_t)a.A_col[e] * K + c0;
-            const T av = Aval[e];
-            if (b0) {
+          if (b0) {
+            gather_row<CPL, 1, UW>(a.A_ptr[row], a.A_ptr[row + 1], 0, a.A_col, Aval,
+                                   [&](int j, T* x) {
+                                     const size_t jb = (size_t)j * K + c0;
 #pragma unroll
-              for (int c = 0; c < CPL; ++c) acc[c] += av * z[jb + c];
-            } else {
+                                     for (int c = 0; c < CPL; ++c) x[c] = z[jb + c];
+                                   },
+                                   acc);
+          } else {
+            gather_row<CPL, 1, UW>(a.A_ptr[row], a.A_ptr[row + 1], 0, a.A_col, Aval,
+                                   [&](int j, T* x) {
+                                     const size_t jb = (size_t)j * K + c0;
 #pragma unroll
-              for (int c = 0; c < CPL; ++c) acc[c] += av * (z[jb + c] + beta[c] * pold[jb + c]);
-            }
+                                     for (int c = 0; c < CPL; ++c) x[c] = z[jb + c] + beta[c] * pold[jb + c];
+                                   },
+                                   acc);
           }
 #pragma unroll
           for (int c = 0; c < CPL; ++c) {
@@ -275,12 +284,13 @@ __device__ void solve_body_wide(const SolveArgs& a, const ClusterTeam& team, Sme
           T acc[CPL];
 #pragma unroll
           for (int c = 0; c < CPL; ++c) acc[c] = (T)0;
-          for (int e = a.L_ptr[row]; e < a.L_ptr[row + 1]; ++e) {
-            const size_t jb = (size_t)a.L_col[e] * K + c0;
-            const T lv = Lval[e];
+          gather_row<CPL, 1, UW>(a.L_ptr[row], a.L_ptr[row + 1], 0, a.L_col, Lval,
+                                 [&](int j, T* x) {
+                                   const size_t jb = (size_t)j * K + c0;
 #pragma unroll
-            for (int c = 0; c < CPL; ++c) acc[c] += lv * y[jb + c];
-          }
+                                   for (int c = 0; c < CPL; ++c) x[c] = y[jb + c];
+                                 },
+                                 acc);
           const T di = dinv[row];
 #pragma unroll
           for (int c = 0; c < CPL; ++c) {
@@ -310,12 +320,13 @@ __device__ void solve_body_wide(const SolveArgs& a, const ClusterTeam& team, Sme
           T acc[CPL];
 #pragma unroll
           for (int c = 0; c < CPL; ++c) acc[c] = (T)0;
-          for (int e = a.U_ptr[row]; e < a.U_ptr[row + 1]; ++e) {
-            const size_t jb = (size_t)a.U_col[e] * K + c0;
-            const T uv = Uval[e];
+          gather_row<CPL, 1, UW>(a.U_ptr[row], a.U_ptr[row + 1], 0, a.U_col, Uval,
+                                 [&](int j, T* x) {
+                                   const size_t jb = (size_t)j * K + c0;
 #pragma unroll
-            for (int c = 0; c < CPL; ++c) acc[c] += uv * z[jb + c];
-          }
+                                   for (int c = 0; c < CPL; ++c) x[c] = z[jb + c];
+                                 },
+                                 acc);
           const T di = dinv[row];
 #pragma unroll
           for (int c = 0; c < CPL; ++c) {
@@ -394,7 +405,7 @@ done:
 }
 
 template <typename T, int K, int C>
-__global__ void __launch_bounds__(512, 1) k_batch(BatchArgs ba) {
+__global__ void __launch_bounds__(512, 2) k_batch(BatchArgs ba) {
   __shared__ SmemW<K> s;
   __shared__ int s_mesh;
   cg::cluster_group cl = cg::this_cluster();

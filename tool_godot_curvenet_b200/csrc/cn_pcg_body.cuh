@@ -143,6 +143,43 @@ __device__ __forceinline__ V group_sum(V v, unsigned mask) {
   return v;
 }
 
+// acc[c] += sum of val[e] * X(col[e], c) over this lane's entries of a row
+// (e = e0 + sub, e0 + sub + G, ... < e1).  Up to U entries at a time: their
+// column indices and values are loaded first, then all U gathers are issued
+// before any of them is used, so one row costs about two dependent memory
+// latencies instead of two per entry.  Entries past e1 contribute zero and
+// read nothing.
+template <int K, int G, int U, typename V, typename A, typename F>
+__device__ __forceinline__ void gather_row(int e0, int e1, int sub, const int* __restrict__ col,
+                                           const V* __restrict__ val, F&& load, A (&acc)[K]) {
+  for (int e = e0 + sub; e < e1; e += G * U) {
+    int j[U];
+    A w[U];
+    bool ok[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int ee = e + u * G;
+      ok[u] = ee < e1;
+      j[u] = ok[u] ? col[ee] : 0;
+      w[u] = ok[u] ? (A)val[ee] : (A)0;
+    }
+    A x[U][K];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (ok[u]) {
+        load(j[u], x[u]);
+      } else {
+#pragma unroll
+        for (int c = 0; c < K; ++c) x[u][c] = (A)0;
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+#pragma unroll
+      for (int c = 0; c < K; ++c) acc[c] += w[u] * x[u][c];
+  }
+}
+
 template <typename T, int K, int G, class Team>
 __device__ void solve_body(const SolveArgs& a, const Team& team, Smem<K>* s) {
   const T* Aval = (const T*)a.A_val;
@@ -168,6 +205,8 @@ __device__ void solve_body(const SolveArgs& a, const Team& team, Smem<K>* s) {
     block_reduce_store<K>(v, s->red, slot_ptr(slot) + (size_t)team.rank() * K);
   };
   int status = CN_OK, total_iters = 0, refinements = 0;
+  // entries gathered together per lane: a row of ~7 entries in one or two passes
+  constexpr int UR = K <= 3 ? (G >= 8 ? 1 : 8 / G) : 2;
 
   // ---- phase A: right-hand side (HarmonicSolve.lean:51-66 / DeformSolve.lean:123-135)
   {
@@ -180,17 +219,17 @@ __device__ void solve_body(const SolveArgs& a, const Team& team, Smem<K>* s) {
       for (int c = 0; c < K; ++c) acc[c] = 0.0;
       const int v = a.free_of[row];
       if (a.mode != CN_MODE_RHS) {
-        for (int e = a.K_ptr[v] + sub; e < a.K_ptr[v + 1]; e += G) {
-          const int u = a.K_col[e];
-          const double kv = a.K_val[e];
-          const int h = a.hidx[u];
+        const bool deform = a.mode == CN_MODE_DEFORM;
+        gather_row<K, G, UR>(a.K_ptr[v], a.K_ptr[v + 1], sub, a.K_col, a.K_val,
+                             [&](int u, double* d) {
+                               const int h = a.hidx[u];
 #pragma unroll
-          for (int c = 0; c < K; ++c) {
-            const double rest = a.mode == CN_MODE_DEFORM ? a.pos[3 * u + c % 3] : 0.0;
-            const double d = h >= 0 ? a.targets[(size_t)h * K + c] - rest : -rest;
-            acc[c] += kv * d;
-          }
-        }
+                               for (int c = 0; c < K; ++c) {
+                                 const double rest = deform ? a.pos[3 * u + c % 3] : 0.0;
+                                 d[c] = h >= 0 ? a.targets[(size_t)h * K + c] - rest : -rest;
+                               }
+                             },
+                             acc);
       }
 #pragma unroll
       for (int c = 0; c < K; ++c) acc[c] = group_sum<G>(acc[c], gmask);
@@ -221,12 +260,12 @@ __device__ void solve_body(const SolveArgs& a, const Team& team, Smem<K>* s) {
         double acc[K];
 #pragma unroll
         for (int c = 0; c < K; ++c) acc[c] = 0.0;
-        for (int e = a.A_ptr[row] + sub; e < a.A_ptr[row + 1]; e += G) {
-          const int j = a.A_col[e];
-          const double av = a.A_val64[e];
+        gather_row<K, G, UR>(a.A_ptr[row], a.A_ptr[row + 1], sub, a.A_col, a.A_val64,
+                             [&](int j, double* x) {
 #pragma unroll
-          for (int c = 0; c < K; ++c) acc[c] += av * a.x64[(size_t)j * K + c];
-        }
+                               for (int c = 0; c < K; ++c) x[c] = a.x64[(size_t)j * K + c];
+                             },
+                             acc);
 #pragma unroll
         for (int c = 0; c < K; ++c) acc[c] = group_sum<G>(acc[c], gmask);
         if (sub == 0) {
@@ -289,15 +328,21 @@ __device__ void solve_body(const SolveArgs& a, const Team& team, Smem<K>* s) {
           T acc[K];
 #pragma unroll
           for (int c = 0; c < K; ++c) acc[c] = (T)0;
-          for (int e = a.A_ptr[row] + sub; e < a.A_ptr[row + 1]; e += G) {
-            const int j = a.A_col[e];
-            const T av = Aval[e];
+          if (b0) {
+            gather_row<K, G, UR>(a.A_ptr[row], a.A_ptr[row + 1], sub, a.A_col, Aval,
+                                 [&](int j, T* x) {
 #pragma unroll
-            for (int c = 0; c < K; ++c) {
-              T pj = z[(size_t)j * K + c];
-              if (!b0) pj += beta[c] * pold[(size_t)j * K + c];
-              acc[c] += av * pj;
-            }
+                                   for (int c = 0; c < K; ++c) x[c] = z[(size_t)j * K + c];
+                                 },
+                                 acc);
+          } else {
+            gather_row<K, G, UR>(a.A_ptr[row], a.A_ptr[row + 1], sub, a.A_col, Aval,
+                                 [&](int j, T* x) {
+#pragma unroll
+                                   for (int c = 0; c < K; ++c)
+                                     x[c] = z[(size_t)j * K + c] + beta[c] * pold[(size_t)j * K + c];
+                                 },
+                                 acc);
           }
 #pragma unroll
           for (int c = 0; c < K; ++c) acc[c] = group_sum<G>(acc[c], gmask);
@@ -343,12 +388,12 @@ __device__ void solve_body(const SolveArgs& a, const Team& team, Smem<K>* s) {
           T acc[K];
 #pragma unroll
           for (int c = 0; c < K; ++c) acc[c] = (T)0;
-          for (int e = a.L_ptr[row] + sub; e < a.L_ptr[row + 1]; e += G) {
-            const int j = a.L_col[e];
-            const T lv = Lval[e];
+          gather_row<K, G, UR>(a.L_ptr[row], a.L_ptr[row + 1], sub, a.L_col, Lval,
+                               [&](int j, T* x) {
 #pragma unroll
-            for (int c = 0; c < K; ++c) acc[c] += lv * y[(size_t)j * K + c];
-          }
+                                 for (int c = 0; c < K; ++c) x[c] = y[(size_t)j * K + c];
+                               },
+                               acc);
 #pragma unroll
           for (int c = 0; c < K; ++c) acc[c] = group_sum<G>(acc[c], gmask);
           if (sub == 0) {
@@ -385,12 +430,12 @@ __device__ void solve_body(const SolveArgs& a, const Team& team, Smem<K>* s) {
           T acc[K];
 #pragma unroll
           for (int c = 0; c < K; ++c) acc[c] = (T)0;
-          for (int e = a.U_ptr[row] + sub; e < a.U_ptr[row + 1]; e += G) {
-            const int j = a.U_col[e];
-            const T uv = Uval[e];
+          gather_row<K, G, UR>(a.U_ptr[row], a.U_ptr[row + 1], sub, a.U_col, Uval,
+                               [&](int j, T* x) {
 #pragma unroll
-            for (int c = 0; c < K; ++c) acc[c] += uv * z[(size_t)j * K + c];
-          }
+                                 for (int c = 0; c < K; ++c) x[c] = z[(size_t)j * K + c];
+                               },
+                               acc);
 #pragma unroll
           for (int c = 0; c < K; ++c) acc[c] = group_sum<G>(acc[c], gmask);
           if (sub == 0) {
