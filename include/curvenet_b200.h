@@ -71,6 +71,8 @@ typedef struct {
   int32_t lanes;         /* 0: default/tuned; else lanes per row (1,2,4,8,16) */
   int32_t block;         /* 0: default/tuned; else threads per block */
   int32_t grid;          /* 0: default/tuned; else blocks of the persistent solve */
+  int32_t hsc_tail_rows; /* HSC: levels with at most this many unknowns left run in one block (0 = 1024) */
+  double hsc_theta;      /* HSC: fill kept when |S_ij| >= theta sqrt(S_ii S_jj) (0 = 0.01) */
 } cn_build_opts;
 
 typedef struct {
@@ -144,6 +146,27 @@ cn_status cn_export_csr(cn_handle h, int32_t* free_of, int32_t* rowptr, int32_t*
                         double* vals);
 cn_status cn_export_factor(cn_handle h, int32_t* rowptr, int32_t* colidx, double* vals);
 cn_status cn_export_k(cn_handle h, int32_t* rowptr, int32_t* colidx, double* vals);
+
+/* Launch shape of the persistent solve: lanes per row (1, 2, 4, 8, 16),
+ * threads per block, blocks (1 = one block, __syncthreads barriers; more =
+ * cooperative grid, clamped to the co-resident maximum). */
+cn_status cn_set_launch(cn_handle h, int32_t lanes, int32_t block, int32_t grid);
+
+/* The launch-shape autotuner: times every candidate shape (lanes per row x
+ * threads per block x blocks) on k device right-hand sides with `reps`
+ * timed solves each and keeps the fastest median.  results (nullable):
+ * 5 doubles per candidate (lanes, block, grid, median ms, iterations);
+ * capacity 120 candidates. */
+cn_status cn_autotune(cn_handle h, int32_t k, const double* d_targets, const cn_solve_opts* opts,
+                      int32_t reps, double* results, int32_t* n_results);
+
+/* Structure of an HSC handle (CN_PRECOND_HSC; hierarchy built from the
+ * elimination primitive of HierarchicalSparsifyCompensate.lean:97-125):
+ * level count, first level solved by one block, coarse size, the n_levels+1
+ * level offsets in HSC positions, and order[p] = row (natural free order,
+ * i.e. free vertices by ascending id) at position p. */
+cn_status cn_hsc_info(cn_handle h, int32_t* n_levels, int32_t* tail, int32_t* n_coarse,
+                      int32_t* level_off, int32_t* order);
 
 /* ---------------------------------------------------------------------------
  * Profile curves and the adjoint.  A curve is a composite cubic Bezier of

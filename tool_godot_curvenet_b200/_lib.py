@@ -29,7 +29,7 @@ class BuildOpts(C.Structure):
     _fields_ = [("precond", C.c_int32), ("ordering", C.c_int32), ("laplacian", C.c_int32),
                 ("mollify_delta", C.c_double), ("device", C.c_int32), ("max_rhs", C.c_int32),
                 ("tune", C.c_int32), ("lanes", C.c_int32), ("block", C.c_int32),
-                ("grid", C.c_int32)]
+                ("grid", C.c_int32), ("hsc_tail_rows", C.c_int32), ("hsc_theta", C.c_double)]
 
 
 class SolveOpts(C.Structure):
@@ -70,6 +70,9 @@ SIGNATURES = {
     "cn_export_csr": (C.c_int, [_P, _I32P, _I32P, _I32P, _DP]),
     "cn_export_factor": (C.c_int, [_P, _I32P, _I32P, _DP]),
     "cn_export_k": (C.c_int, [_P, _I32P, _I32P, _DP]),
+    "cn_set_launch": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32]),
+    "cn_autotune": (C.c_int, [_P, C.c_int32, _P, C.POINTER(SolveOpts), C.c_int32, _DP, _I32P]),
+    "cn_hsc_info": (C.c_int, [_P, _I32P, _I32P, _I32P, _I32P, _I32P]),
     "cn_bind_curves": (C.c_int, [_P, C.c_int32, C.c_int32, _DP, _I32P, _DP]),
     "cn_deform": (C.c_int, [_P, _DP, _DP, _DP, C.POINTER(SolveOpts), C.POINTER(SolveStats)]),
     "cn_adjoint": (C.c_int, [_P, _DP, _DP, _DP, C.POINTER(SolveOpts), C.POINTER(SolveStats)]),

@@ -8,6 +8,7 @@
 #include <numeric>
 #include <vector>
 
+#include "cn_hsc.h"
 #include "cn_mesh.h"
 
 using cn::Control;
@@ -49,6 +50,15 @@ struct cn_system {
   int* d_status = nullptr;
   int max_grid_alloc = 0;
   bool have_solution = false;
+  // HSC preconditioner tables (own allocations)
+  bool hsc = false;
+  int hsc_L = 0, hsc_tail = 0, hsc_nc = 0;
+  std::vector<int> hsc_order, hsc_off_h;
+  std::vector<void*> hsc_mem;
+  int *d_hoff = nullptr, *d_hrlev = nullptr, *d_hrrow = nullptr, *d_hrptr = nullptr, *d_hrcol = nullptr,
+      *d_hpptr = nullptr, *d_hpcol = nullptr;
+  double *d_hrval64 = nullptr, *d_hpval64 = nullptr, *d_hdinv64 = nullptr, *d_hsinv64 = nullptr;
+  float *d_hrval32 = nullptr, *d_hpval32 = nullptr, *d_hdinv32 = nullptr, *d_hsinv32 = nullptr;
   // profile-curve binding (cn_bind_curves), own allocations
   int ncurves = 0, nseg = 0;
   bool have_forward = false;
@@ -93,6 +103,92 @@ void choose_launch(cn_system* S) {
     S->block = S->opts.block > 0 ? S->opts.block : 512;
     S->grid = S->opts.grid > 0 ? S->opts.grid : sms;
   }
+}
+
+template <class Tp>
+cn_status up_new(cn_system* S, Tp** dst, const std::vector<Tp>& h) {
+  const size_t bytes = sizeof(Tp) * std::max<size_t>(h.size(), 1);
+  if (cudaMalloc((void**)dst, bytes) != cudaSuccess) {
+    set_err("device allocation of %zu bytes failed", bytes);
+    return CN_CUDA_ERROR;
+  }
+  S->hsc_mem.push_back(*dst);
+  if (!h.empty() && cudaMemcpy(*dst, h.data(), sizeof(Tp) * h.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+    set_err("upload failed");
+    return CN_CUDA_ERROR;
+  }
+  return CN_OK;
+}
+
+std::vector<float> to_f32(const std::vector<double>& v) { return std::vector<float>(v.begin(), v.end()); }
+
+// HSC: read A back, build the hierarchy on the host, move the rows into HSC
+// order, reassemble A in that order and upload the level tables.
+cn_status setup_hsc(cn_system* S, const cn_build_opts& ob) {
+  MeshHost& H = S->H;
+  std::vector<double> A(H.nnzA);
+  if (H.nnzA && cudaMemcpy(A.data(), S->D.A64, sizeof(double) * H.nnzA, cudaMemcpyDeviceToHost) != cudaSuccess) {
+    set_err("read-back of A failed");
+    return CN_CUDA_ERROR;
+  }
+  cn::HscHost h;
+  cn::HscParams prm;
+  if (S->opts.hsc_theta > 0.0) prm.theta = S->opts.hsc_theta;
+  cn_status st = cn::hsc_build(H.n, H.A_ptr.data(), H.A_col.data(), A.data(), prm, h);
+  if (st != CN_OK) {
+    set_err("HSC coarse matrix is not positive definite");
+    return st;
+  }
+  cn::permute_solve_order(H, h.order);
+  st = cn::upload(H, S->D, S->stream);
+  if (st != CN_OK) return st;
+  st = cn::assemble_factor(H, S->D, ob, S->d_status, S->stream, nullptr);
+  if (st != CN_OK) return st;
+  const int L = (int)h.levels.size();
+  S->hsc_L = L;
+  S->hsc_nc = h.nc;
+  S->hsc_order = h.order;
+  std::vector<int> off(L + 1), rlev(L + 1, 0), rrow, rptr(1, 0), rcol, pptr(1, 0), pcol;
+  std::vector<double> rval, pval, dinv;
+  for (int l = 0; l < L; ++l) {
+    const auto& V = h.levels[l];
+    off[l] = V.off;
+    for (size_t k = 0; k < V.R_rows.size(); ++k) {
+      rrow.push_back(V.R_rows[k]);
+      for (int e = V.R_ptr[k]; e < V.R_ptr[k + 1]; ++e) {
+        rcol.push_back(V.R_col[e]);
+        rval.push_back(V.R_val[e]);
+      }
+      rptr.push_back((int)rcol.size());
+    }
+    rlev[l + 1] = (int)rrow.size();
+    for (int k = 0; k < V.nf; ++k) {
+      for (int e = V.P_ptr[k]; e < V.P_ptr[k + 1]; ++e) {
+        pcol.push_back(V.P_col[e]);
+        pval.push_back(V.P_val[e]);
+      }
+      pptr.push_back((int)pcol.size());
+      dinv.push_back(V.dinv[k]);
+    }
+  }
+  off[L] = h.coarse_off;
+  S->hsc_off_h = off;
+  // levels with at most this many remaining unknowns run in one block
+  const int kTailRows = S->opts.hsc_tail_rows > 0 ? S->opts.hsc_tail_rows : 1024;
+  int tail = L;
+  for (int l = 0; l < L; ++l)
+    if (H.n - off[l] <= kTailRows) { tail = l; break; }
+  S->hsc_tail = tail;
+  if ((st = up_new(S, &S->d_hoff, off)) || (st = up_new(S, &S->d_hrlev, rlev)) ||
+      (st = up_new(S, &S->d_hrrow, rrow)) || (st = up_new(S, &S->d_hrptr, rptr)) ||
+      (st = up_new(S, &S->d_hrcol, rcol)) || (st = up_new(S, &S->d_hpptr, pptr)) ||
+      (st = up_new(S, &S->d_hpcol, pcol)) || (st = up_new(S, &S->d_hrval64, rval)) ||
+      (st = up_new(S, &S->d_hpval64, pval)) || (st = up_new(S, &S->d_hdinv64, dinv)) ||
+      (st = up_new(S, &S->d_hsinv64, h.Sinv)) || (st = up_new(S, &S->d_hrval32, to_f32(rval))) ||
+      (st = up_new(S, &S->d_hpval32, to_f32(pval))) || (st = up_new(S, &S->d_hdinv32, to_f32(dinv))) ||
+      (st = up_new(S, &S->d_hsinv32, to_f32(h.Sinv))))
+    return st;
+  return CN_OK;
 }
 
 }  // namespace
@@ -204,7 +300,7 @@ cn_status cn_build(const cn_mesh_desc* mesh, const cn_build_opts* opts, cn_handl
     set_err("max_rhs must be 1, 3 or 9");
     return CN_BAD_INPUT;
   }
-  if (o.precond != CN_PRECOND_IC0 && o.precond != CN_PRECOND_JACOBI) {
+  if (o.precond != CN_PRECOND_IC0 && o.precond != CN_PRECOND_JACOBI && o.precond != CN_PRECOND_HSC) {
     set_err("unsupported preconditioner %d", o.precond);
     return CN_BAD_INPUT;
   }
@@ -229,7 +325,13 @@ cn_status cn_build(const cn_mesh_desc* mesh, const cn_build_opts* opts, cn_handl
     cn_destroy(S);
     return s;
   };
-  st = cn::build_host(mesh, o, S->H);
+  S->hsc = o.precond == CN_PRECOND_HSC;
+  cn_build_opts ob = o;
+  if (S->hsc) {  // the structure pass builds A in natural order without an IC(0) pattern
+    ob.precond = CN_PRECOND_JACOBI;
+    ob.ordering = CN_ORDER_NATURAL;
+  }
+  st = cn::build_host(mesh, ob, S->H);
   if (st != CN_OK) return fail(st);
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, S->device);
@@ -255,8 +357,12 @@ cn_status cn_build(const cn_mesh_desc* mesh, const cn_build_opts* opts, cn_handl
   }
   st = cn::upload(S->H, S->D, S->stream);
   if (st != CN_OK) return fail(st);
-  st = cn::assemble_factor(S->H, S->D, o, S->d_status, S->stream, &S->shift_used);
+  st = cn::assemble_factor(S->H, S->D, ob, S->d_status, S->stream, &S->shift_used);
   if (st != CN_OK) return fail(st);
+  if (S->hsc) {
+    st = setup_hsc(S, ob);
+    if (st != CN_OK) return fail(st);
+  }
   choose_launch(S);
   *out = S;
   return CN_OK;
@@ -267,6 +373,7 @@ void cn_destroy(cn_handle S) {
   cudaSetDevice(S->device);
   if (S->stream) cudaStreamSynchronize(S->stream);
   if (S->buf) cudaFree(S->buf);
+  for (void* p : S->hsc_mem) cudaFree(p);
   for (void* p : {(void*)S->d_curve_of, (void*)S->d_row_of, (void*)S->d_tau, (void*)S->d_rest_cp,
                   (void*)S->d_posed_cp, (void*)S->d_weights, (void*)S->d_dLdx, (void*)S->d_dP, (void*)S->d_dw})
     if (p) cudaFree(p);
@@ -281,7 +388,7 @@ void* cn_stream(cn_handle S) { return S ? (void*)S->stream : nullptr; }
 cn_status cn_system_info(cn_handle S, int64_t* info) {
   if (!S || !info) return CN_BAD_INPUT;
   const MeshHost& H = S->H;
-  int64_t v[12] = {H.n, H.nnzA, H.nnzL, H.nlev, H.nnzK, H.nv, H.nh,
+  int64_t v[12] = {H.n, H.nnzA, H.nnzL, S->hsc ? S->hsc_L : H.nlev, H.nnzK, H.nv, H.nh,
                    S->grid, S->block, S->lanes, H.ncolors, (int64_t)S->bytes};
   std::memcpy(info, v, sizeof v);
   return CN_OK;
@@ -343,6 +450,23 @@ cn_status cn_solve_device(cn_handle S, int32_t k, const double* d_targets, doubl
   void** w = mixed ? (void**)S->d_w32 : (void**)S->d_w64;
   a.r = w[0]; a.y = w[1]; a.z = w[2]; a.p0 = w[3]; a.p1 = w[4]; a.Ap = w[5]; a.xin = w[6];
   a.partials = S->d_partials;
+  if (S->hsc) {
+    a.hsc = 1;
+    a.hsc_L = S->hsc_L;
+    a.hsc_tail = S->hsc_tail;
+    a.hsc_nc = S->hsc_nc;
+    a.hsc_off = S->d_hoff;
+    a.hsc_rlev = S->d_hrlev;
+    a.hsc_rrow = S->d_hrrow;
+    a.hsc_rptr = S->d_hrptr;
+    a.hsc_rcol = S->d_hrcol;
+    a.hsc_rval = mixed ? (const void*)S->d_hrval32 : (const void*)S->d_hrval64;
+    a.hsc_pptr = S->d_hpptr;
+    a.hsc_pcol = S->d_hpcol;
+    a.hsc_pval = mixed ? (const void*)S->d_hpval32 : (const void*)S->d_hpval64;
+    a.hsc_dinv = mixed ? (const void*)S->d_hdinv32 : (const void*)S->d_hdinv64;
+    a.hsc_sinv = mixed ? (const void*)S->d_hsinv32 : (const void*)S->d_hsinv64;
+  }
   a.tol = o.tol;
   a.inner_tol = mixed ? o.inner_tol : 0.0;
   a.max_iter = o.max_iter;
@@ -635,6 +759,103 @@ cn_status cn_adjoint(cn_handle S, const double* dL_dx, double* dL_dcp, double* d
   CN_CUDA(cudaMemcpyAsync(dL_dw, S->d_dw, sizeof(double) * S->ncurves, cudaMemcpyDeviceToHost, S->stream));
   CN_CUDA(cudaStreamSynchronize(S->stream));
   return st;
+}
+
+cn_status cn_set_launch(cn_handle S, int32_t lanes, int32_t block, int32_t grid) {
+  if (!S || (lanes != 1 && lanes != 2 && lanes != 4 && lanes != 8 && lanes != 16) || block < 64 ||
+      block > 1024 || block % 32 != 0 || grid < 1) {
+    set_err("bad launch shape (lanes %d, block %d, grid %d)", lanes, block, grid);
+    return CN_BAD_INPUT;
+  }
+  if (grid > 1) {
+    const int mg = std::min(cn::persistent_max_grid(CN_PREC_MIXED, S->kmax, lanes, block),
+                            cn::persistent_max_grid(CN_PREC_FP64, S->kmax, lanes, block));
+    if (mg < 1) {
+      set_err("shape (lanes %d, block %d) does not fit as a cooperative grid", lanes, block);
+      return CN_BAD_INPUT;
+    }
+    grid = std::min(grid, std::min(mg, S->max_grid_alloc));
+  }
+  S->lanes = lanes;
+  S->block = block;
+  S->grid = grid;
+  return CN_OK;
+}
+
+// The project's launch-shape autotuner: every candidate (lanes per row,
+// threads per block, blocks) solves the caller's right-hand sides a few times
+// on the device; the fastest median keeps.  results (nullable, 5 doubles per
+// candidate): lanes, block, grid, median ms, iterations.
+cn_status cn_autotune(cn_handle S, int32_t k, const double* d_targets, const cn_solve_opts* opts, int32_t reps,
+                      double* results, int32_t* n_results) {
+  if (!S || !d_targets) {
+    set_err("null argument");
+    return CN_BAD_INPUT;
+  }
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, S->device);
+  struct Cand { int lanes, block, grid; };
+  std::vector<Cand> cands;
+  const int lane_set[] = {1, 2, 4, 8};
+  if (S->H.n <= 65536)
+    for (int l : lane_set)
+      for (int b : {256, 512, 1024}) cands.push_back({l, b, 1});
+  if (S->H.n > 4096)
+    for (int l : lane_set)
+      for (int b : {256, 512, 1024})
+        for (int g : {sms / 2, sms, 2 * sms}) cands.push_back({l, b, g});
+  const int old_l = S->lanes, old_b = S->block, old_g = S->grid;
+  cn_solve_opts o;
+  if (opts) o = *opts;
+  else cn_default_solve_opts(&o);
+  double best = 1e30;
+  Cand pick{old_l, old_b, old_g};
+  int nr = 0;
+  reps = std::max(1, reps);
+  for (const Cand& c : cands) {
+    if (cn_set_launch(S, c.lanes, c.block, c.grid) != CN_OK) continue;
+    std::vector<double> ms;
+    int iters = 0;
+    bool ok = true;
+    for (int r = 0; r <= reps; ++r) {  // the first run warms up
+      cn_solve_stats st;
+      if (cn_solve_device(S, k, d_targets, S->d_xout, &o, &st) != CN_OK) { ok = false; break; }
+      if (r) ms.push_back(st.device_ms);
+      iters = st.iterations;
+    }
+    if (!ok) continue;
+    std::sort(ms.begin(), ms.end());
+    const double med = ms[ms.size() / 2];
+    if (results) {
+      double* R = results + 5 * nr;
+      R[0] = c.lanes; R[1] = c.block; R[2] = S->grid; R[3] = med; R[4] = iters;
+    }
+    ++nr;
+    if (med < best) { best = med; pick = {c.lanes, c.block, S->grid}; }
+  }
+  if (n_results) *n_results = nr;
+  cn_set_launch(S, pick.lanes, pick.block, pick.grid);
+  S->have_solution = false;
+  if (nr == 0) {
+    set_err("no launch shape ran");
+    cn_set_launch(S, old_l, old_b, old_g);
+    return CN_CUDA_ERROR;
+  }
+  return CN_OK;
+}
+
+cn_status cn_hsc_info(cn_handle S, int32_t* n_levels, int32_t* tail, int32_t* n_coarse, int32_t* level_off,
+                      int32_t* order) {
+  if (!S || !S->hsc) {
+    set_err("not an HSC handle");
+    return CN_BAD_INPUT;
+  }
+  if (n_levels) *n_levels = S->hsc_L;
+  if (tail) *tail = S->hsc_tail;
+  if (n_coarse) *n_coarse = S->hsc_nc;
+  if (level_off) std::memcpy(level_off, S->hsc_off_h.data(), sizeof(int) * S->hsc_off_h.size());
+  if (order) std::memcpy(order, S->hsc_order.data(), sizeof(int) * S->hsc_order.size());
+  return CN_OK;
 }
 
 cn_status cn_export_csr(cn_handle S, int32_t* free_of, int32_t* rowptr, int32_t* colidx,

@@ -72,6 +72,21 @@ struct SolveArgs {
   void* Ap;   // T
   void* xin;  // T
   double* partials;        // [kSlots][grid][K]
+  // HSC preconditioner (hsc != 0): rows are in HSC order; F_l = positions
+  // [hsc_off[l], hsc_off[l + 1]); the coarse set starts at hsc_off[hsc_L];
+  // levels >= hsc_tail (and the coarse solve) run in block 0 alone.
+  int hsc, hsc_L, hsc_tail, hsc_nc;
+  const int* hsc_off;
+  const int* hsc_rlev;   // hsc_L + 1: R rows of level l
+  const int* hsc_rrow;   // R row -> position of the C row
+  const int* hsc_rptr;
+  const int* hsc_rcol;
+  const void* hsc_rval;  // T
+  const int* hsc_pptr;   // over F positions [0, hsc_off[hsc_L])
+  const int* hsc_pcol;
+  const void* hsc_pval;  // T
+  const void* hsc_dinv;  // T, over F positions
+  const void* hsc_sinv;  // T, hsc_nc x hsc_nc
   // control
   double tol;
   double inner_tol;

@@ -415,6 +415,32 @@ cn_status assemble_factor(const MeshHost& H, const MeshDev& D, const cn_build_op
   return CN_OK;
 }
 
+void permute_solve_order(MeshHost& H, const std::vector<int>& order) {
+  const int n = H.n;
+  std::vector<int> pos_of(n);
+  for (int p = 0; p < n; ++p) pos_of[order[p]] = p;
+  std::vector<int> ptr(n + 1, 0), col(H.nnzA), src(H.nnzA), diag(n, -1), free_of(n);
+  std::vector<std::pair<int, int>> row;
+  for (int p = 0; p < n; ++p) {
+    const int o = order[p];
+    free_of[p] = H.free_of[o];
+    row.clear();
+    for (int e = H.A_ptr[o]; e < H.A_ptr[o + 1]; ++e) row.push_back({pos_of[H.A_col[e]], H.A_src[e]});
+    std::sort(row.begin(), row.end());
+    for (size_t q = 0; q < row.size(); ++q) {
+      col[ptr[p] + q] = row[q].first;
+      src[ptr[p] + q] = row[q].second;
+      if (row[q].first == p) diag[p] = ptr[p] + (int)q;
+    }
+    ptr[p + 1] = ptr[p] + (int)row.size();
+  }
+  H.A_ptr.swap(ptr);
+  H.A_col.swap(col);
+  H.A_src.swap(src);
+  H.A_diag.swap(diag);
+  H.free_of.swap(free_of);
+}
+
 SolveArgs solve_args(const MeshHost& H, const MeshDev& D, bool mixed) {
   SolveArgs a{};
   a.n = H.n; a.nlev = H.nlev; a.lev_ptr = D.lev_ptr;

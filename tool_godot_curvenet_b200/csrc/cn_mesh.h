@@ -70,6 +70,11 @@ cn_status assemble_factor(const MeshHost& H, const MeshDev& D, const cn_build_op
 // vectors, partials, control, targets and outputs are filled by the caller.
 SolveArgs solve_args(const MeshHost& H, const MeshDev& D, bool mixed);
 
+// Relabel the solve order: new row p is old row order[p] (A, its source map,
+// the diagonal positions and free_of follow).  Only for a mesh without an
+// IC(0) pattern (one level, empty L).
+void permute_solve_order(MeshHost& H, const std::vector<int>& order);
+
 // Vertex -> incident faces (ascending face id) with the vertex's corner.
 void vertex_faces(int nv, int nt, const int* tris, std::vector<int>& ptr, std::vector<int>& face,
                   std::vector<int>& corner);

@@ -381,6 +381,125 @@ __device__ void solve_body(const SolveArgs& a, const Team& team, Smem<K>* s) {
       T alpha[K];
 #pragma unroll
       for (int c = 0; c < K; ++c) alpha[c] = (T)s->alpha[c];
+      if (a.hsc) {
+        // HSC V-cycle (the block-LDL^T solve of the hierarchy): w = r (with
+        // the CG update), down the levels w_C -= R w_F, the coarse
+        // z_c = S^{-1} w_c, up the levels z_F = D_F^{-1} (w_F - P z_C).
+        T* w = y;
+        const T* Rv = (const T*)a.hsc_rval;
+        const T* Pv = (const T*)a.hsc_pval;
+        const T* hd = (const T*)a.hsc_dinv;
+        const T* Si = (const T*)a.hsc_sinv;
+        for (int row = row0; row < n; row += rstride) {
+          if (sub == 0) {
+#pragma unroll
+            for (int c = 0; c < K; ++c) {
+              const size_t ix = (size_t)row * K + c;
+              T rv = r[ix];
+              if (!first) {
+                xin[ix] += alpha[c] * pcur[ix];
+                rv -= alpha[c] * Ap[ix];
+                r[ix] = rv;
+              }
+              w[ix] = rv;
+              rrp[c] += (double)rv * (double)rv;
+            }
+          }
+        }
+        if (!team.sync()) { status = CN_TIMEOUT; goto done; }
+        const int HL = a.hsc_L, tail = a.hsc_tail;
+        auto down = [&](int l, int q0, int qs) {
+          for (int q = a.hsc_rlev[l] + q0; q < a.hsc_rlev[l + 1]; q += qs) {
+            T acc[K];
+#pragma unroll
+            for (int c = 0; c < K; ++c) acc[c] = (T)0;
+            gather_row<K, G, UR>(a.hsc_rptr[q], a.hsc_rptr[q + 1], sub, a.hsc_rcol, Rv,
+                                 [&](int j, T* x) {
+#pragma unroll
+                                   for (int c = 0; c < K; ++c) x[c] = w[(size_t)j * K + c];
+                                 },
+                                 acc);
+#pragma unroll
+            for (int c = 0; c < K; ++c) acc[c] = group_sum<G>(acc[c], gmask);
+            if (sub == 0) {
+              const int i = a.hsc_rrow[q];
+#pragma unroll
+              for (int c = 0; c < K; ++c) w[(size_t)i * K + c] -= acc[c];
+            }
+          }
+        };
+        auto up = [&](int l, int v0, int vs) {
+          for (int v = a.hsc_off[l] + v0; v < a.hsc_off[l + 1]; v += vs) {
+            T acc[K];
+#pragma unroll
+            for (int c = 0; c < K; ++c) acc[c] = (T)0;
+            gather_row<K, G, UR>(a.hsc_pptr[v], a.hsc_pptr[v + 1], sub, a.hsc_pcol, Pv,
+                                 [&](int j, T* x) {
+#pragma unroll
+                                   for (int c = 0; c < K; ++c) x[c] = z[(size_t)j * K + c];
+                                 },
+                                 acc);
+#pragma unroll
+            for (int c = 0; c < K; ++c) acc[c] = group_sum<G>(acc[c], gmask);
+            if (sub == 0) {
+              const T di = hd[v];
+#pragma unroll
+              for (int c = 0; c < K; ++c) {
+                const size_t ix = (size_t)v * K + c;
+                const T zv = (w[ix] - acc[c]) * di;
+                z[ix] = zv;
+                rzp[c] += (double)r[ix] * (double)zv;
+              }
+            }
+          }
+        };
+        for (int l = 0; l < tail; ++l) {
+          down(l, row0, rstride);
+          if (!team.sync()) { status = CN_TIMEOUT; goto done; }
+        }
+        if (team.rank() == 0) {
+          // the small levels and the dense coarse solve: one block,
+          // __syncthreads between the steps
+          for (int l = tail; l < HL; ++l) {
+            down(l, grp, gpb);
+            __syncthreads();
+          }
+          const int co = a.hsc_off[HL], nc = a.hsc_nc;
+          const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+          for (int i = co + warp; i < n; i += nw) {
+            T acc[K];
+#pragma unroll
+            for (int c = 0; c < K; ++c) acc[c] = (T)0;
+            const T* srow = Si + (size_t)(i - co) * nc;
+            for (int j = lane; j < nc; j += 32) {
+              const T sv = srow[j];
+#pragma unroll
+              for (int c = 0; c < K; ++c) acc[c] += sv * w[(size_t)(co + j) * K + c];
+            }
+#pragma unroll
+            for (int c = 0; c < K; ++c)
+#pragma unroll
+              for (int o = 16; o > 0; o >>= 1) acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], o);
+            if (lane == 0) {
+#pragma unroll
+              for (int c = 0; c < K; ++c) {
+                const size_t ix = (size_t)i * K + c;
+                z[ix] = acc[c];
+                rzp[c] += (double)r[ix] * (double)acc[c];
+              }
+            }
+          }
+          __syncthreads();
+          for (int l = HL - 1; l >= tail; --l) {
+            up(l, grp, gpb);
+            __syncthreads();
+          }
+        }
+        for (int l = tail - 1; l >= 0; --l) {
+          if (!team.sync()) { status = CN_TIMEOUT; goto done; }
+          up(l, row0, rstride);
+        }
+      } else {
       for (int l = 0; l < nlev; ++l) {
         const int lo = a.lev_ptr[l], hi = a.lev_ptr[l + 1];
         const bool last = l == nlev - 1;
@@ -450,6 +569,7 @@ __device__ void solve_body(const SolveArgs& a, const Team& team, Smem<K>* s) {
           }
         }
       }
+      }  // IC(0) / Jacobi sweeps
       write_partial(kRR, rrp);
       write_partial(kRZ, rzp);
       if (!team.sync()) { status = CN_TIMEOUT; goto done; }

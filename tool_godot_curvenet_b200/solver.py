@@ -79,7 +79,7 @@ class CutMeshSolver:
 
     def __init__(self, positions, tris, handles, precond="ic0", ordering="color",
                  laplacian="cot", mollify_delta=1e-4, max_rhs=3, device=0, lanes=0,
-                 block=0, grid=0):
+                 block=0, grid=0, hsc_tail_rows=0, hsc_theta=0.0):
         self.positions = _f64(positions).reshape(-1, 3)
         self.tris = _i32(tris).reshape(-1, 3)
         self.handles = _i32(handles).reshape(-1)
@@ -95,6 +95,7 @@ class CutMeshSolver:
         opts.max_rhs = max_rhs
         opts.device = device
         opts.lanes, opts.block, opts.grid = lanes, block, grid
+        opts.hsc_tail_rows, opts.hsc_theta = hsc_tail_rows, hsc_theta
         h = C.c_void_p()
         st = L.lib().cn_build(C.byref(desc), C.byref(opts), C.byref(h))
         if st != L.CN_OK:
@@ -130,6 +131,17 @@ class CutMeshSolver:
 
     def stream(self):
         return L.lib().cn_stream(self._h)
+
+    def hsc_info(self):
+        """(n_levels, tail, n_coarse, level_off, order) of an HSC handle."""
+        i = self.info()
+        nl, tail, nc = C.c_int32(), C.c_int32(), C.c_int32()
+        off = np.zeros(65, np.int32)
+        order = np.zeros(i["n_free"], np.int32)
+        st = L.lib().cn_hsc_info(self._h, C.byref(nl), C.byref(tail), C.byref(nc), _ip(off), _ip(order))
+        if st != L.CN_OK:
+            raise CnError(st, "cn_hsc_info")
+        return nl.value, tail.value, nc.value, off[: nl.value + 1].copy(), order
 
     def export_csr(self):
         i = self.info()
