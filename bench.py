@@ -161,11 +161,11 @@ def batch_section(torch, dist, world, rank, local, steps, warmup):
     sharded (longest-processing-time partition) and each rank launches its
     share."""
     from tool_godot_curvenet_b200 import BatchSolver, cut_mesh, synth
-    from tool_godot_curvenet_b200.shard import lpt_partition, mesh_cost
+    from tool_godot_curvenet_b200.shard import mesh_cost, rank_share, reduce_over_ranks
     n_meshes = 512
     specs = [synth.config3_mesh(i) for i in range(n_meshes)]
     costs = [mesh_cost(m.positions.shape[0] + sum(len(l) for l in m.loops), m.tris.shape[0]) for m, _, _ in specs]
-    mine = lpt_partition(costs, world)[rank]
+    mine = rank_share(costs, world, rank)
     meshes, targets = [], []
     for i in mine:
         m, h, t = specs[i]
@@ -208,17 +208,11 @@ def batch_section(torch, dist, world, rank, local, steps, warmup):
     if chk_m.n_failed or chk_f.n_failed or chk_m.max_rel_residual > 1e-8 or chk_f.max_rel_residual > 1e-8:
         raise SystemExit(f"batch solve did not converge: mixed {chk_m.n_failed} failed, fp64 {chk_f.n_failed} failed")
 
-    def red(v, op):
-        if world == 1:
-            return v
-        tt = torch.tensor([v], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(tt, op=op)
-        return float(tt.item())
-    mx = dist.ReduceOp.MAX if world > 1 else None
-    p50 = red(float(np.percentile(tm, 50)), mx)
-    p99 = red(float(np.percentile(tm, 99)), mx)
-    ms_m = red(sum(tm) / len(tm), mx)
-    ms_f = red(sum(tf) / len(tf), mx)
+    dev = f"cuda:{local}"
+    p50 = reduce_over_ranks(dist, world, float(np.percentile(tm, 50)), "max", dev)
+    p99 = reduce_over_ranks(dist, world, float(np.percentile(tm, 99)), "max", dev)
+    ms_m = reduce_over_ranks(dist, world, sum(tm) / len(tm), "max", dev)
+    ms_f = reduce_over_ranks(dist, world, sum(tf) / len(tf), "max", dev)
     solves = n_meshes * 8  # (mesh, pose) solves of 3 RHS each, over all ranks
     # algorithmic bytes of the batch (mixed): per mesh iterations x B_iter + residuals
     nnz = info["nnz_A"]
@@ -342,12 +336,10 @@ def main():
                 raise SystemExit(f"cn_solve failed {rc}")
             e2e_ms.append(a.elapsed_time(b))
 
+    from tool_godot_curvenet_b200.shard import reduce_over_ranks
+
     def maxred(v):
-        if world == 1:
-            return v
-        tt = torch.tensor([v], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        return float(tt.item())
+        return reduce_over_ranks(dist, world, v, "max", f"cuda:{local}")
 
     ms_mixed = maxred(sum(t_mixed) / len(t_mixed))
     ms_fp64 = maxred(sum(t_fp64) / len(t_fp64))

@@ -147,6 +147,15 @@ cn_status cn_export_csr(cn_handle h, int32_t* free_of, int32_t* rowptr, int32_t*
 cn_status cn_export_factor(cn_handle h, int32_t* rowptr, int32_t* colidx, double* vals);
 cn_status cn_export_k(cn_handle h, int32_t* rowptr, int32_t* colidx, double* vals);
 
+/* The full DeGoes22 two-stage solve (DeformSolve.lean:110-135): Stage 1
+ * solves the 9 entries of the deformation gradient from F_c (n_handles x 9,
+ * row-major 3x3 per handle), the Eq.(3) bridge averages them per face and
+ * builds y_h = F_f rest, Stage 2 solves the positions from
+ * -V^T L_h (C X_c - y_h).  X_c: n_handles x 3; x_out: n_verts x 3 with the
+ * handles overlaid.  Needs a build with max_rhs = 9. */
+cn_status cn_solve_deformation(cn_handle h, const double* Fc, const double* Xc, double* x_out,
+                               const cn_solve_opts* opts, cn_solve_stats* stats);
+
 /* Launch shape of the persistent solve: lanes per row (1, 2, 4, 8, 16),
  * threads per block, blocks (1 = one block, __syncthreads barriers; more =
  * cooperative grid, clamped to the co-resident maximum). */

@@ -50,3 +50,58 @@ def csr_to_dict(ptr, col, val, rows_map=None, cols_map=None):
 
 def rel_err(x, ref):
     return float(np.abs(x - ref).max() / max(np.abs(ref).max(), 1e-300))
+
+
+def random_gradients(nh, seed, scale=0.15):
+    """(nh, 9) per-handle deformation gradients R (I + scale N(0, 1))."""
+    rng = np.random.default_rng(seed)
+    ax = rng.normal(size=3)
+    ax /= np.linalg.norm(ax)
+    ang = rng.uniform(0, np.pi / 3)
+    Kx = np.array([[0, -ax[2], ax[1]], [ax[2], 0, -ax[0]], [-ax[1], ax[0], 0]])
+    R = np.eye(3) + np.sin(ang) * Kx + (1 - np.cos(ang)) * Kx @ Kx
+    F = np.stack([R @ (np.eye(3) + scale * rng.normal(size=(3, 3))) for _ in range(nh)])
+    return F.reshape(nh, 9)
+
+
+def sample_col(nv, h):
+    sc = np.full(nv, -1, np.int32)
+    sc[h] = np.arange(h.size, dtype=np.int32)
+    return sc
+
+
+def composed_deformation(oracle, pos, tris, h, Fc, Xc):
+    """DeformSolve.lean:110-135 composed from oracle pieces: the oracle's
+    k = 9 harmonic solve (CG to 1e-14), the bridge in numpy over the oracle's
+    per-face cot Laplacian, Stage 2 by a sparse direct solve of the oracle's
+    A.  Handles overlaid with X_c."""
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spl
+
+    nv = pos.shape[0]
+    ref = oracle.System(pos, tris, h)
+    st, Fv, _, _ = ref.solve(Fc, mode=0, tol=1e-14)
+    assert st == 0
+    Fv = Fv.copy()
+    Fv[h] = Fc  # harmonic overlay of the handles (computeFh :40-53)
+    rest = pos
+    cx = np.zeros((nv, 3))
+    cx[h] = Xc
+    rhs = np.zeros((nv, 3))
+    for f, (a, b, c) in enumerate(tris):
+        corners = (b, c, a)  # faceLoop order t1, t2, t0
+        Ff = (Fv[b] + Fv[c] + Fv[a]) / 3.0
+        Fm = Ff.reshape(3, 3)
+        Lf = oracle.triangle_cot_laplacian(pos[corners[0]], pos[corners[1]], pos[corners[2]])
+        diff = np.stack([cx[v] - Fm @ rest[v] for v in corners])
+        contrib = Lf @ diff
+        for q, v in enumerate(corners):
+            rhs[v] -= contrib[q]
+    e = ref.export()
+    free_of = e["free_of"]
+    Ap, Ac, Av = e["A"]
+    A = sp.csr_matrix((Av, Ac, Ap), shape=(free_of.size, free_of.size))
+    x = np.zeros((nv, 3))
+    x[free_of] = spl.spsolve(A.tocsc(), rhs[free_of])
+    x[h] = Xc
+    return x

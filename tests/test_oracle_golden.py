@@ -226,3 +226,20 @@ def test_known_answer(f, oracle):
                 assert np.all(np.abs(X[int(r)] - want) < eps)
     else:
         pytest.fail(f"unknown fixture kind {k}")
+
+
+def test_composed_deformation_matches_dense_oracle():
+    """The composition used by the GPU deform tests on larger meshes agrees
+    with the dense restatement of DeformSolve.lean:110-135 on the free rows."""
+    from oracle import oracle as O
+    from tests.helpers import composed_deformation, random_gradients, rel_err, sample_col, workload
+    O.build()
+    pos, tris, h, t = workload("cyl_tiny")
+    nv = pos.shape[0]
+    Fc = random_gradients(h.size, 3)
+    he = O.halfedges_from_triangles(nv, tris)
+    want = O.solve_deformation(nv, tris.shape[0], he, sample_col(nv, h), pos, Fc, t)
+    got = composed_deformation(O, pos, tris, h, Fc, t)
+    free = np.setdiff1d(np.arange(nv), h)
+    assert rel_err(got[free], want[free]) < 1e-12
+    assert np.array_equal(got[h], t)

@@ -59,6 +59,9 @@ struct cn_system {
       *d_hpptr = nullptr, *d_hpcol = nullptr;
   double *d_hrval64 = nullptr, *d_hpval64 = nullptr, *d_hdinv64 = nullptr, *d_hsinv64 = nullptr;
   float *d_hrval32 = nullptr, *d_hpval32 = nullptr, *d_hdinv32 = nullptr, *d_hsinv32 = nullptr;
+  // two-stage deform (cn_solve_deformation), own allocations
+  int *d_vf_ptr = nullptr, *d_vf_face = nullptr, *d_vf_corner = nullptr;
+  double *d_contrib = nullptr, *d_Xc = nullptr;
   // profile-curve binding (cn_bind_curves), own allocations
   int ncurves = 0, nseg = 0;
   bool have_forward = false;
@@ -375,7 +378,9 @@ void cn_destroy(cn_handle S) {
   if (S->buf) cudaFree(S->buf);
   for (void* p : S->hsc_mem) cudaFree(p);
   for (void* p : {(void*)S->d_curve_of, (void*)S->d_row_of, (void*)S->d_tau, (void*)S->d_rest_cp,
-                  (void*)S->d_posed_cp, (void*)S->d_weights, (void*)S->d_dLdx, (void*)S->d_dP, (void*)S->d_dw})
+                  (void*)S->d_posed_cp, (void*)S->d_weights, (void*)S->d_dLdx, (void*)S->d_dP, (void*)S->d_dw,
+                  (void*)S->d_vf_ptr, (void*)S->d_vf_face, (void*)S->d_vf_corner, (void*)S->d_contrib,
+                  (void*)S->d_Xc})
     if (p) cudaFree(p);
   if (S->ev0) cudaEventDestroy(S->ev0);
   if (S->ev1) cudaEventDestroy(S->ev1);
@@ -758,6 +763,77 @@ cn_status cn_adjoint(cn_handle S, const double* dL_dx, double* dL_dcp, double* d
   CN_CUDA(cudaMemcpyAsync(dL_dcp, S->d_dP, sizeof(double) * ncp, cudaMemcpyDeviceToHost, S->stream));
   CN_CUDA(cudaMemcpyAsync(dL_dw, S->d_dw, sizeof(double) * S->ncurves, cudaMemcpyDeviceToHost, S->stream));
   CN_CUDA(cudaStreamSynchronize(S->stream));
+  return st;
+}
+
+// DeGoes22 two-stage solve (DeformSolve.lean:110-135): Stage 1 (k = 9
+// harmonic solve of F), the bridge (cn_deform.cu), Stage 2 (k = 3).
+cn_status cn_solve_deformation(cn_handle S, const double* Fc, const double* Xc, double* x_out,
+                               const cn_solve_opts* opts, cn_solve_stats* stats) {
+  if (!S || !Fc || !Xc || !x_out) {
+    set_err("null argument");
+    return CN_BAD_INPUT;
+  }
+  if (S->kmax < 9) {
+    set_err("the two-stage solve needs a build with max_rhs = 9");
+    return CN_BAD_INPUT;
+  }
+  const MeshHost& H = S->H;
+  for (size_t i = 0; i < 9 * (size_t)H.nh; ++i)
+    if (!std::isfinite(Fc[i])) {
+      set_err("F_c %zu is not finite", i);
+      return CN_NAN;
+    }
+  for (size_t i = 0; i < 3 * (size_t)H.nh; ++i)
+    if (!std::isfinite(Xc[i])) {
+      set_err("X_c %zu is not finite", i);
+      return CN_NAN;
+    }
+  CN_CUDA(cudaSetDevice(S->device));
+  if (!S->d_vf_ptr) {
+    CN_CUDA(cudaMalloc((void**)&S->d_vf_ptr, sizeof(int) * H.vf_ptr.size()));
+    CN_CUDA(cudaMalloc((void**)&S->d_vf_face, sizeof(int) * std::max<size_t>(H.vf_face.size(), 1)));
+    CN_CUDA(cudaMalloc((void**)&S->d_vf_corner, sizeof(int) * std::max<size_t>(H.vf_corner.size(), 1)));
+    CN_CUDA(cudaMalloc((void**)&S->d_contrib, sizeof(double) * 9 * std::max(H.nt, 1)));
+    CN_CUDA(cudaMalloc((void**)&S->d_Xc, sizeof(double) * 3 * std::max(H.nh, 1)));
+    CN_CUDA(cudaMemcpy(S->d_vf_ptr, H.vf_ptr.data(), sizeof(int) * H.vf_ptr.size(), cudaMemcpyHostToDevice));
+    if (!H.vf_face.empty()) {
+      CN_CUDA(cudaMemcpy(S->d_vf_face, H.vf_face.data(), sizeof(int) * H.vf_face.size(), cudaMemcpyHostToDevice));
+      CN_CUDA(cudaMemcpy(S->d_vf_corner, H.vf_corner.data(), sizeof(int) * H.vf_corner.size(),
+                         cudaMemcpyHostToDevice));
+    }
+  }
+  cn_solve_opts o;
+  if (opts) o = *opts;
+  else cn_default_solve_opts(&o);
+  o.warm_start = 0;
+  // Stage 1: F_v, handles overlaid with F_c, into d_xout (n_verts x 9)
+  if (H.nh) CN_CUDA(cudaMemcpyAsync(S->d_targets, Fc, sizeof(double) * 9 * H.nh, cudaMemcpyHostToDevice, S->stream));
+  CN_CUDA(cudaMemcpyAsync(S->d_Xc, Xc, sizeof(double) * 3 * std::max(H.nh, 0), cudaMemcpyHostToDevice, S->stream));
+  cn_solve_opts o1 = o;
+  o1.mode = CN_MODE_HARMONIC;
+  cn_solve_stats s1;
+  cn_status st = cn_solve_device(S, 9, S->d_targets, S->d_xout, &o1, &s1);
+  if (st != CN_OK) return st;
+  // bridge: Stage-2 right-hand side (solve order) into d_targets
+  cn::DeformArgs d{};
+  d.nt = H.nt; d.n = H.n; d.tris = S->D.tris; d.pos = S->D.pos; d.face_m = S->D.face_m;
+  d.hidx = S->D.hidx; d.Fv = S->d_xout; d.Xc = S->d_Xc; d.free_of = S->D.free_of;
+  d.vf_ptr = S->d_vf_ptr; d.vf_face = S->d_vf_face; d.vf_corner = S->d_vf_corner;
+  d.contrib = S->d_contrib; d.b = S->d_targets;
+  CN_CUDA(cn::launch_deform_bridge(d, S->stream));
+  // Stage 2, then the overlay of X_c on the handles (DeformSolve.lean:108-109)
+  cn_solve_opts o2 = o;
+  o2.mode = CN_MODE_RHS;
+  cn_solve_stats s2;
+  st = cn_solve_device(S, 3, S->d_targets, S->d_xout, &o2, stats ? stats : &s2);
+  S->have_solution = false;
+  if (st != CN_OK && st != CN_MAX_ITER) return st;
+  CN_CUDA(cudaMemcpyAsync(x_out, S->d_xout, sizeof(double) * 3 * (size_t)H.nv, cudaMemcpyDeviceToHost, S->stream));
+  CN_CUDA(cudaStreamSynchronize(S->stream));
+  for (int h = 0; h < H.nh; ++h)
+    for (int c = 0; c < 3; ++c) x_out[3 * (size_t)H.handles[h] + c] = Xc[3 * (size_t)h + c];
+  if (stats) stats->iterations += s1.iterations;
   return st;
 }
 

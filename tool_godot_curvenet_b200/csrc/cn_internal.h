@@ -163,6 +163,24 @@ cudaError_t launch_adjoint_grad(const CurveArgs& c, const int* K_ptr, const int*
                                 const int* row_of, const double* lambda, const double* dLdx, double* dP,
                                 double* dw, cudaStream_t s);
 
+// The Stage 1 -> Stage 2 bridge of the DeGoes22 solve (cn_deform.cu).
+struct DeformArgs {
+  int nt, n;
+  const int* tris;
+  const double* pos;
+  const double* face_m;   // nt x 6 (the face's 3x3 in faceLoop order)
+  const int* hidx;
+  const double* Fv;       // nv x 9 (Stage 1, handles overlaid with F_c)
+  const double* Xc;       // nh x 3
+  const int* free_of;
+  const int* vf_ptr;      // vertex -> incident faces, ascending
+  const int* vf_face;
+  const int* vf_corner;
+  double* contrib;        // 3 nt x 3
+  double* b;              // n x 3 Stage-2 right-hand side (solve order)
+};
+cudaError_t launch_deform_bridge(const DeformArgs& d, cudaStream_t s);
+
 // Plain FP64 Jacobi-PCG with one kernel per primitive and the scalars folded
 // on the host each iteration (the reference's GPU orchestration).
 struct PlainArgs {

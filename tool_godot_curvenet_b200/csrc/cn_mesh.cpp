@@ -90,7 +90,9 @@ cn_status build_host(const cn_mesh_desc* m, const cn_build_opts& o, MeshHost& H)
   const int nv = m->n_verts, nt = m->n_tris;
   const int* tris = m->tris;
   // --- K pattern and the face contributions of every entry
-  std::vector<int> vf_ptr, vf_face, vf_corner;
+  std::vector<int>& vf_ptr = H.vf_ptr;
+  std::vector<int>& vf_face = H.vf_face;
+  std::vector<int>& vf_corner = H.vf_corner;
   vertex_faces(nv, nt, tris, vf_ptr, vf_face, vf_corner);
   S->K_ptr.assign(nv + 1, 0);
   S->K_col.clear();

@@ -27,6 +27,7 @@ struct MeshHost {
   std::vector<int> A_ptr, A_col, A_src, A_diag;        // A = K[free, free]
   std::vector<int> L_ptr, L_col, L_src, T_ptr, T_a, T_b;  // strictly-lower IC(0) pattern
   std::vector<int> U_ptr, U_col, U_src;                // U = L^T
+  std::vector<int> vf_ptr, vf_face, vf_corner;         // vertex -> incident faces (ascending)
 };
 
 // Device arrays of one mesh (sub-allocations of one buffer).

@@ -27,3 +27,21 @@ def lpt_partition(costs, world):
         parts[r].append(int(i))
         load[r] += costs[i]
     return [sorted(p) for p in parts]
+
+
+def rank_share(costs, world, rank):
+    """The meshes of `rank` under the LPT partition (same on every rank)."""
+    return lpt_partition(costs, world)[rank]
+
+
+def reduce_over_ranks(dist, world, value, op="max", device="cpu"):
+    """Reduce one host float over the ranks (identity with one rank).  Device
+    timings are taken per rank with CUDA events; the job's time is their max.
+    `device`: where the one-element tensor lives ("cuda:<local>" under NCCL,
+    "cpu" under gloo)."""
+    if world == 1:
+        return float(value)
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+    return float(t.item())

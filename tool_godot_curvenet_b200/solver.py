@@ -203,6 +203,19 @@ class CutMeshSolver:
             raise CnError(st, "cn_solve")
         return SolveResult(x, stats)
 
+    def solve_deformation(self, Fc, Xc, **kw):
+        """DeformSolve.lean:110-135: Stage 1 (F), the Eq.(3) bridge, Stage 2
+        (positions).  Fc: (n_handles, 9) row-major 3x3; Xc: (n_handles, 3)."""
+        Fc = _f64(Fc).reshape(-1, 9)
+        Xc = _f64(Xc).reshape(-1, 3)
+        x = np.empty((self.n_verts, 3))
+        o = self.make_opts(**kw)
+        stats = L.SolveStats()
+        st = L.lib().cn_solve_deformation(self._h, _dp(Fc), _dp(Xc), _dp(x), C.byref(o), C.byref(stats))
+        if st != L.CN_OK:
+            raise CnError(st, "cn_solve_deformation")
+        return SolveResult(x, stats)
+
     def solve_device(self, k, d_targets, d_x_out, stats=True, **kw):
         """Device-pointer solve on the handle's stream (ints are device addresses)."""
         o = self.make_opts(**kw)
