@@ -104,6 +104,21 @@ def algorithmic_bytes(info, stats, k, mixed):
     return stats.iterations * b_iter + (stats.refinements + 1) * b_res + b_rhs
 
 
+def algorithmic_bytes_pipelined(info, stats, k, mixed):
+    """Bytes the pipelined Jacobi-PCG must move: per inner iteration one SpMV
+    (A's values and columns, row pointer, the gathered m), the store of m', and
+    a read and a write of the six own-row vectors r, w, z, s, p, x plus
+    1/A_ii; per FP64 residual evaluation one FP64 SpMV; plus the FP64
+    right-hand side."""
+    n, nnz = info["n_free"], info["nnz_A"]
+    sv = 4 if mixed else 8
+    sx = 4 if mixed else 8
+    b_iter = nnz * (sv + 4) + 4 * (n + 1) + 2 * n * k * sx + 12 * n * k * sx + n * sx
+    b_res = nnz * 12 + 4 * (n + 1) + 3 * n * k * 8
+    b_rhs = info["nnz_K"] * 12 + 4 * (info["n_verts"] + 1) + n * k * 8
+    return stats.iterations * b_iter + (stats.refinements + 1) * b_res + b_rhs
+
+
 def cpu_baseline(pos, tris, h, t, seconds=12.0):
     """The oracle's FP64 IC(0)-PCG (the reference's CPU path restated), columns
     on parallel threads; bounded sample of whole solves."""
@@ -262,40 +277,47 @@ def main():
     m, h, t = synth.config2()
     tris, parent = cut_mesh(m.positions.shape[0], m.tris, m.loops)
     pos = np.ascontiguousarray(m.positions[parent])
-    solver = CutMeshSolver(pos, tris, h, device=local)
+    # the headline path: Jacobi preconditioner, pipelined CG (one team barrier
+    # per iteration, rows of A and the own-row state in shared memory)
+    solver = CutMeshSolver(pos, tris, h, device=local, precond="jacobi")
+    solver_ic = CutMeshSolver(pos, tris, h, device=local, precond="ic0")
     info = solver.info()
+    info_ic = solver_ic.info()
     stream = torch.cuda.ExternalStream(solver.stream(), device=local)
     nv, k = pos.shape[0], 3
     d_t = torch.from_numpy(t).to(f"cuda:{local}")
     d_x = torch.empty((nv, k), dtype=torch.float64, device=f"cuda:{local}")
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")  # > L2 (126 MB)
 
-    def one(precision, algo="fused", stats=False):
-        return solver.solve_device(k, d_t.data_ptr(), d_x.data_ptr(), stats=stats, mode="deform",
-                                   precision=precision, algo=algo, tol=1e-8)
+    def one(precision, algo="fused", stats=False, sv=None):
+        return (sv or solver).solve_device(k, d_t.data_ptr(), d_x.data_ptr(), stats=stats, mode="deform",
+                                           precision=precision, algo=algo, tol=1e-8)
 
-    # reference statistics of each variant (deterministic: same inputs, cold start)
+    # reference statistics of each variant (same inputs, cold start)
     st_mixed = one("mixed", stats=True)
     st_fp64 = one("fp64", stats=True)
     st_plain = one("fp64", "plain", stats=True)
-    for s in (st_mixed, st_fp64, st_plain):
+    st_ic = one("mixed", stats=True, sv=solver_ic)
+    st_classic = one("mixed", "classic", stats=True)
+    for s in (st_mixed, st_fp64, st_plain, st_ic, st_classic):
         if s.status != 0:
             raise SystemExit(f"solve failed: status {s.status}")
 
-    def timed(precision, algo, steps, warmup):
-        with torch.cuda.stream(stream):
+    def timed(precision, algo, steps, warmup, sv=None):
+        with torch.cuda.stream(stream if sv is None else torch.cuda.ExternalStream(sv.stream(), device=local)):
             for _ in range(warmup):
-                one(precision, algo)
+                one(precision, algo, sv=sv)
             evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
             torch.cuda.synchronize()
             if world > 1:
                 dist.barrier()
             torch.cuda.synchronize()
+            st_ = torch.cuda.current_stream()
             for a, b in evs:
                 flush.fill_(1)  # L2 flush between timed solves (outside the events)
-                a.record(stream)
-                one(precision, algo)
-                b.record(stream)
+                a.record(st_)
+                one(precision, algo, sv=sv)
+                b.record(st_)
             torch.cuda.synchronize()
             if world > 1:
                 dist.barrier()
@@ -308,6 +330,8 @@ def main():
     clk = clocks.stop()
     t_fp64 = timed("fp64", "fused", max(3, args.steps // 3), 2)
     t_plain = timed("fp64", "plain", 3, 1)
+    t_ic = timed("mixed", "fused", max(3, args.steps // 3), 2, sv=solver_ic)
+    t_classic = timed("mixed", "classic", max(3, args.steps // 3), 2)
 
     # e2e: host (pinned) buffers through cn_solve, H2D of the targets and D2H of
     # the deformed positions inside the timed region
@@ -345,20 +369,23 @@ def main():
     ms_fp64 = maxred(sum(t_fp64) / len(t_fp64))
     ms_plain = maxred(sum(t_plain) / len(t_plain))
     ms_e2e = maxred(sum(e2e_ms) / len(e2e_ms))
+    ms_ic = maxred(sum(t_ic) / len(t_ic))
+    ms_classic = maxred(sum(t_classic) / len(t_classic))
     peak, peak_kind = load_peaks()
-    bytes_mixed = algorithmic_bytes(info, st_mixed, k, True)
-    bytes_fp64 = algorithmic_bytes(info, st_fp64, k, False)
+    bytes_mixed = algorithmic_bytes_pipelined(info, st_mixed, k, True)
+    bytes_fp64 = algorithmic_bytes_pipelined(info, st_fp64, k, False)
     ach = bytes_mixed / (ms_mixed * 1e-3) / 1e9
     traffic = None
     try:
         with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
             tj = json.load(f)
-        traffic = tj.get("cn_persistent_solve_mixed", {}).get("dram_bytes_per_launch")
+        traffic = tj.get("cn_pipe_solve_mixed", {}).get("dram_bytes_per_launch")
     except Exception:
         pass
     batch = None
     if not args.no_batch:
         solver.close()
+        solver_ic.close()
         batch = batch_section(torch, dist, world, rank, local, max(3, args.steps // 6), 2)
     if rank == 0:
         x = d_x.cpu().numpy()
@@ -376,8 +403,8 @@ def main():
             "dtype": "f32 inner / f64 residual",
             "data": "synthetic (seeded torus, see tool_godot_curvenet_b200/synth.py config2)",
             "config": {"workload": WORKLOAD, "n_verts": nv, "n_free": info["n_free"], "nnz_A": info["nnz_A"],
-                       "rhs": k, "tol": 1e-8, "precond": "IC(0), greedy-colour order",
-                       "n_levels": info["n_levels"], "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                       "rhs": k, "tol": 1e-8, "precond": "Jacobi, pipelined CG (one team barrier per iteration)",
+                       "launch": f"grid {info['grid']} x block auto (2 rows per thread)", "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
                        "l2": "flushed (256 MB write) before every timed solve, outside the events"},
             "mixed": {"iterations": st_mixed.iterations, "refinements": st_mixed.refinements,
                       "max_rel_residual": st_mixed.max_rel_residual},
@@ -385,12 +412,18 @@ def main():
                            "max_rel_residual": st_fp64.max_rel_residual},
             "fp64_plain": {"solves_per_s": 1e3 / ms_plain, "ms": ms_plain, "iterations": st_plain.iterations,
                            "note": "Jacobi-PCG, one kernel per primitive, dots folded on the host each iteration"},
+            "ic0_mixed": {"solves_per_s": 1e3 / ms_ic, "ms": ms_ic, "iterations": st_ic.iterations,
+                          "n_levels": info_ic["n_levels"],
+                          "note": "IC(0) in greedy-colour order, classic CG: 2 x n_levels team barriers per iteration"},
+            "jacobi_classic_mixed": {"solves_per_s": 1e3 / ms_classic, "ms": ms_classic,
+                                     "iterations": st_classic.iterations,
+                                     "note": "same preconditioner, classic CG: 2 team barriers per iteration"},
             "speedup_mixed_vs_fp64_plain": ms_plain / ms_mixed,
             "speedup_mixed_vs_fp64_fused": ms_fp64 / ms_mixed,
             "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
                          "peak_kind": peak_kind, "traffic": traffic,
-                         "kernel": f"k_solve_grid<float,3,{info['lanes']}> (persistent solve, grid {info['grid']} x {info['block']})",
-                         "note": "L2-resident working set: DRAM traffic per launch is ~1% of the algorithmic bytes; latency-bound (barriers, dependent L2 loads)",
+                         "kernel": f"k_pipe_grid<float,3,2> (pipelined persistent solve, grid {info['grid']})",
+                         "note": "rows of A and the own-row state stay in shared memory, m in L2: DRAM traffic per launch is a small fraction of the algorithmic bytes; latency-bound (one team barrier and one L2 round trip per iteration)",
                          "algorithmic_bytes_per_launch": bytes_mixed,
                          "fp64_fused_achieved": bytes_fp64 / (ms_fp64 * 1e-3) / 1e9},
             "e2e": {"value": world * 1e3 / ms_e2e, "unit": "solves/s", "h2d_bytes_per_step": int(h_t.numel() * 8),
@@ -405,6 +438,7 @@ def main():
             line["cpu_baseline"] = cpu_baseline(pos, tris, h, t)
         print(json.dumps(line), flush=True)
     solver.close()
+    solver_ic.close()
     if world > 1:
         dist.destroy_process_group()
 

@@ -58,7 +58,11 @@ enum { CN_ORDER_NATURAL = 0, CN_ORDER_COLOR = 1 };
 enum { CN_LAPLACIAN_COT = 0, CN_LAPLACIAN_ROBUST = 1 };
 enum { CN_PREC_FP64 = 0, CN_PREC_MIXED = 1 };
 enum { CN_MODE_HARMONIC = 0, CN_MODE_DEFORM = 1, CN_MODE_RHS = 2 };
-enum { CN_ALGO_FUSED = 0, CN_ALGO_PLAIN = 1 };
+/* FUSED: one persistent launch; with Jacobi the pipelined CG (one team
+ * barrier per iteration), otherwise the classic CG.  CLASSIC: one persistent
+ * launch of the classic CG (two reductions per iteration) for every
+ * preconditioner.  PLAIN: one kernel per primitive, FP64 Jacobi. */
+enum { CN_ALGO_FUSED = 0, CN_ALGO_PLAIN = 1, CN_ALGO_CLASSIC = 2 };
 
 typedef struct {
   int32_t precond;       /* CN_PRECOND_* (default IC0) */
@@ -78,7 +82,7 @@ typedef struct {
 typedef struct {
   int32_t precision;   /* CN_PREC_FP64 or CN_PREC_MIXED */
   int32_t mode;        /* CN_MODE_HARMONIC, CN_MODE_DEFORM (targets) or CN_MODE_RHS */
-  int32_t algo;        /* CN_ALGO_FUSED (one persistent launch) or CN_ALGO_PLAIN */
+  int32_t algo;        /* CN_ALGO_FUSED, CN_ALGO_CLASSIC or CN_ALGO_PLAIN */
   double tol;          /* relative residual ||b - A x|| / ||b|| per column */
   int32_t max_iter;    /* inner PCG iterations per refinement step */
   int32_t max_refine;  /* FP64 residual refinements (mixed precision) */

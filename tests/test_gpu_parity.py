@@ -229,3 +229,39 @@ def test_autotuner_picks_a_shape_that_solves(oracle, tmp_path):
         assert rel_err(r.x, xo) <= FP64_TOL
         with CutMeshSolver(pos, tris, h) as s2:
             assert tune.apply_cached(s2, cache=str(tmp_path / "c.json")) == best
+
+
+@pytest.mark.parametrize("k", [1, 3, 9])
+@pytest.mark.parametrize("grid,block", [(1, 1024), (8, 256), (2, 128), (148, 1024)])
+def test_jacobi_pipelined_matches_oracle_and_classic(k, grid, block, oracle):
+    """The pipelined Jacobi-PCG (one barrier per iteration; shared-memory row
+    cache with one or several row slices per thread, or global rows when a
+    block holds more slices than the cache does) against the oracle and the
+    classic two-reduction form."""
+    pos, tris, h, _ = workload("torus_small")
+    rng = np.random.default_rng(11 + k)
+    t = rng.normal(size=(h.size, k))
+    ref = oracle.System(pos, tris, h)
+    st, xo, _, _ = ref.solve(t, mode=0, tol=1e-13)
+    with CutMeshSolver(pos, tris, h, max_rhs=k, precond="jacobi", grid=grid, block=block) as s:
+        r = s.solve(t, mode="harmonic", precision="fp64", tol=1e-13, max_iter=20000)
+        rm = s.solve(t, mode="harmonic", precision="mixed", tol=1e-8, max_iter=20000)
+        rc = s.solve(t, mode="harmonic", precision="fp64", tol=1e-13, max_iter=20000, algo="classic")
+    assert r.status == 0 and rm.status == 0 and rc.status == 0
+    assert np.all(r.rel_residual <= 1e-13) and np.all(rm.rel_residual <= 1e-8)
+    assert rel_err(r.x, xo) <= FP64_TOL
+    assert rel_err(rm.x, xo) <= MIXED_TOL
+    assert rel_err(rc.x, xo) <= FP64_TOL
+    # pipelined and classic take about the same number of iterations
+    assert r.iterations <= 1.5 * rc.iterations + 20
+
+
+def test_bad_algo_rejected():
+    pos, tris, h, t = workload("cyl_tiny")
+    with CutMeshSolver(pos, tris, h) as s:
+        o = s.make_opts()
+        o.algo = 7
+        st = L.lib().cn_solve(s._h, 3, t.ctypes.data_as(L.C.POINTER(L.C.c_double)), None,
+                              np.empty((pos.shape[0], 3)).ctypes.data_as(L.C.POINTER(L.C.c_double)),
+                              L.C.byref(o), None)
+    assert st == L.CN_BAD_INPUT

@@ -16,7 +16,7 @@ ORDER_NATURAL, ORDER_COLOR = 0, 1
 LAPLACIAN_COT, LAPLACIAN_ROBUST = 0, 1
 PREC_FP64, PREC_MIXED = 0, 1
 MODE_HARMONIC, MODE_DEFORM, MODE_RHS = 0, 1, 2
-ALGO_FUSED, ALGO_PLAIN = 0, 1
+ALGO_FUSED, ALGO_PLAIN, ALGO_CLASSIC = 0, 1, 2
 
 
 class MeshDesc(C.Structure):

@@ -279,7 +279,7 @@ cn_status cn_solve_batch_device(cn_batch_handle B, const double* d_targets, doub
   cn_solve_opts o;
   if (opts) o = *opts;
   else cn_default_solve_opts(&o);
-  if (!(o.tol > 0.0) || o.max_iter < 0 || o.max_refine < 1 || o.algo != CN_ALGO_FUSED) {
+  if (!(o.tol > 0.0) || o.max_iter < 0 || o.max_refine < 1 || o.algo == CN_ALGO_PLAIN) {
     set_err("bad solve options for a batch");
     return CN_BAD_INPUT;
   }

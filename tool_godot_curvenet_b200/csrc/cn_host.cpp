@@ -47,7 +47,11 @@ struct cn_system {
   Control* d_ctl = nullptr;
   DevStats* d_stats = nullptr;
   double *d_targets = nullptr, *d_xout = nullptr, *d_scal = nullptr;
+  double *d_pown = nullptr, *d_m[2] = {};   // pipelined solve: FP64 own-row state, two copies of m
   int* d_status = nullptr;
+  // pipelined solve: shared-memory needs of the last (grid, block, precision, k)
+  int pipe_grid = -1, pipe_block = -1, pipe_prec = -1, pipe_k = -1;
+  size_t pipe_cache = 0, pipe_full = 0;
   int max_grid_alloc = 0;
   bool have_solution = false;
   // HSC preconditioner tables (own allocations)
@@ -86,6 +90,8 @@ void layout_all(cn::Bump& b, cn_system* S) {
     S->d_w64[i] = b.take<double>(nk);
     S->d_w32[i] = b.take<float>(nk);
   }
+  S->d_pown = b.take<double>(7 * nk);
+  for (int i = 0; i < 2; ++i) S->d_m[i] = b.take<double>((size_t)std::max(S->H.n, 1) * (S->kmax + 1));
   S->d_partials = b.take<double>((size_t)cn::kSlots * S->max_grid_alloc * S->kmax);
   S->d_scal = b.take<double>(64);
   S->d_ctl = b.take<Control>(1);
@@ -441,7 +447,8 @@ cn_status cn_solve_device(cn_handle S, int32_t k, const double* d_targets, doubl
     set_err("deform mode needs k a multiple of 3");
     return CN_BAD_INPUT;
   }
-  if (!(o.tol > 0.0) || o.max_iter < 0 || o.max_refine < 1) {
+  if (!(o.tol > 0.0) || o.max_iter < 0 || o.max_refine < 1 || o.algo < CN_ALGO_FUSED ||
+      o.algo > CN_ALGO_CLASSIC) {
     set_err("bad solve options");
     return CN_BAD_INPUT;
   }
@@ -478,6 +485,48 @@ cn_status cn_solve_device(cn_handle S, int32_t k, const double* d_targets, doubl
   a.max_refine = o.max_refine;
   a.ctl = S->d_ctl; a.stats = S->d_stats;
   a.timeout_ns = 2000000000LL;
+  a.m0 = S->d_m[0]; a.m1 = S->d_m[1]; a.pown = S->d_pown; a.dinv64 = S->D.dinv64;
+  if (!S->hsc && S->opts.precond == CN_PRECOND_JACOBI && o.algo == CN_ALGO_FUSED) {
+    int grid = S->grid, block = S->block, qr = 1;
+    a.cache_bytes = 0;
+    if (grid > 1) {
+      grid = std::min(grid, S->max_grid_alloc);
+      // two rows per thread, gathered together: block = n / (2 grid) rounded
+      // up to a warp (an explicit block above 512 runs one row per thread)
+      if (S->opts.block <= 0) block = std::min(512, std::max(128, ((S->H.n + 2 * grid - 1) / (2 * grid) + 31) / 32 * 32));
+      qr = block <= 512 ? 2 : 1;
+      const size_t cap = 220 * 1024;
+      int level = 2;  // 2: row cache and own state in shared memory, 1: row cache only, 0: none
+      for (int tries = 0; tries < 6; ++tries) {
+        if (S->pipe_grid != grid || S->pipe_block != block || S->pipe_prec != o.precision || S->pipe_k != k) {
+          cn::pipelined_smem_need(S->H.A_ptr.data(), S->H.n, grid, block, o.precision, k, &S->pipe_cache,
+                                  &S->pipe_full);
+          S->pipe_grid = grid; S->pipe_block = block; S->pipe_prec = o.precision; S->pipe_k = k;
+        }
+        if (level == 2 && S->pipe_full > cap) level = 1;
+        if (level == 1 && S->pipe_cache > cap) level = 0;
+        a.cache_bytes = level == 2 ? (int)S->pipe_full : level == 1 ? (int)S->pipe_cache : 0;
+        const int mg = cn::pipelined_max_grid(o.precision, k, block, a.cache_bytes, qr);
+        if (mg >= grid) break;
+        if (mg <= 0) {
+          if (level == 0) {
+            set_err("the pipelined solve does not fit on this device (block %d)", block);
+            return CN_CUDA_ERROR;
+          }
+          --level;
+          continue;
+        }
+        grid = mg;
+      }
+    }
+    CN_CUDA(cudaMemsetAsync(S->d_ctl, 0, sizeof(Control), S->stream));
+    CN_CUDA(cudaEventRecord(S->ev0, S->stream));
+    CN_CUDA(cn::launch_pipelined_solve(a, o.precision, k, block, grid, qr, S->stream));
+    CN_CUDA(cudaEventRecord(S->ev1, S->stream));
+    S->have_solution = true;
+    if (!stats) return CN_OK;
+    return fill_stats(S, k, stats);
+  }
   int grid = S->grid;
   if (grid > 1) {
     const int mg = cn::persistent_max_grid(o.precision, k, S->lanes, S->block);

@@ -71,6 +71,13 @@ struct SolveArgs {
   void* p1;   // T
   void* Ap;   // T
   void* xin;  // T
+  // pipelined Jacobi-PCG (cn_pipe.cu): the ping-pong copies of m = M^-1 w
+  // that neighbouring rows gather ([rows][round_up(K, 16 B)])
+  void* m0;   // T
+  void* m1;   // T
+  double* pown;            // FP64 own-row state when it is not in shared memory: 7 x [rows][K]
+  const double* dinv64;    // 1 / sqrt(A_ii), FP64
+  int cache_bytes;         // dynamic shared memory (row cache, then own-row state)
   double* partials;        // [kSlots][grid][K]
   // HSC preconditioner (hsc != 0): rows are in HSC order; F_l = positions
   // [hsc_off[l], hsc_off[l + 1]); the coarse set starts at hsc_off[hsc_L];
@@ -97,7 +104,9 @@ struct SolveArgs {
   long long timeout_ns;
 };
 
-constexpr int kSlots = 6;
+constexpr int kSlots = 8;
+// Row slices per thread that the pipelined solve's shared-memory row cache holds.
+constexpr int kPipeSlices = 16;
 
 // Sets the text cn_last_error() returns on this thread (cn_host.cpp).
 void set_last_error_text(const char* msg);
@@ -107,6 +116,21 @@ cudaError_t launch_persistent_solve(const SolveArgs& a, int precision, int K, in
                                     int block, int grid, cudaStream_t s);
 // Largest co-resident grid of the persistent solve for this configuration.
 int persistent_max_grid(int precision, int K, int lanes, int block);
+
+// The pipelined Jacobi-PCG persistent solve (cn_pipe.cu): one team barrier
+// per iteration.  a.cache_bytes of dynamic shared memory hold each block's
+// rows of A.
+// qr: rows per thread gathered together (1: up to 1024 threads per block,
+// 2: up to 512).
+cudaError_t launch_pipelined_solve(const SolveArgs& a, int precision, int K, int block, int grid, int qr,
+                                   cudaStream_t s);
+int pipelined_max_grid(int precision, int K, int block, int cache_bytes, int qr);
+// Shared memory of the pipelined solve for this launch shape (the largest
+// block's share), given the row pointer of A: *cache = the row cache alone,
+// *full = the row cache and the FP64 own-row state; SIZE_MAX when a block
+// holds more than kPipeSlices row slices.
+void pipelined_smem_need(const int* A_ptr, int n, int grid, int block, int precision, int K, size_t* cache,
+                         size_t* full);
 
 // Build-time kernels (cn_assemble.cu).
 struct BuildArgs {

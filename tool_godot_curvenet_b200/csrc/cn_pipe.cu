@@ -1,0 +1,748 @@
+// cn_pipe.cu -- the pipelined Jacobi-PCG persistent solve (sm_100a).
+//
+// Same problem, right-hand sides, FP64 residual refinement and output as the
+// classic persistent solve (cn_pcg.cu); the inner solve is the pipelined
+// preconditioned CG of Ghysels & Vanroose ("Hiding global synchronization
+// latency in the preconditioned Conjugate Gradient algorithm", Parallel
+// Computing 40, 2014, Alg. 4) with the Jacobi preconditioner M = diag(A):
+//
+//   gamma = (r, u), delta = (w, u)               one reduction per iteration
+//   m = M^-1 w ; n = A m                         overlaps that reduction
+//   beta = gamma / gamma' ; alpha = gamma / (delta - beta gamma / alpha')
+//   z = n + beta z ; s = w + beta s ; p = u + beta p
+//   x += alpha p ; r -= alpha s ; w -= alpha z ; u = M^-1 r
+//
+// (with a diagonal M the recurrences u -= alpha q, q = m + beta q of the
+// general form reduce to u = M^-1 r, so q is not kept).  The classic form
+// needs two reductions per iteration (p.Ap before the update, r.z after it),
+// hence two team barriers; here an iteration is ONE phase between two
+// barriers:
+//   after the barrier a block issues the gathers of m (its rows' neighbours,
+//   written by their owners in the previous phase) and the loads of its own
+//   rows' state, and, in the same memory round trip, three warps sum the
+//   previous phase's partials (gamma, delta, ||r||^2 per column, a fixed
+//   order, so every block derives the same alpha, beta and stopping
+//   decision); the own rows update, store m' = M^-1 w' into the other copy
+//   of m, and the block's partial sums of (gamma', delta', ||r'||^2) are
+//   written before the next barrier.
+// Each thread owns the rows t + q * (grid * block) of its block for the whole
+// launch, and the block keeps its rows of A (column index and T value) in
+// shared memory (one ELL slice per row slice, column-major, padding column
+// -1), so a row costs one L2 round trip (the gathers of m) per phase.
+// Partial sums alternate between two slot groups by phase parity (a block
+// may write phase i+1's partials while a slower block still reads phase i's);
+// m alternates between two buffers for the same reason.
+#include <algorithm>
+
+#include "cn_pcg_body.cuh"
+
+namespace cn {
+namespace {
+
+using namespace pcg;
+
+// Row of m as gathered: K values padded to a multiple of 16 bytes.
+template <typename T, int K>
+struct MRow {
+  static constexpr int W = ((K * (int)sizeof(T) + 15) / 16) * 16 / (int)sizeof(T);
+  static constexpr int NC = W * (int)sizeof(T) / 16;
+};
+
+constexpr int kPipeSplits = 8;  // partial-sum read: up to 8 x 128 blocks
+// The pipelined recurrences in FP32 lose track of the true residual below
+// about 1e-4 of the starting one, so each refinement step of the mixed solve
+// asks the inner solve for at most this much reduction.
+constexpr double kPipeInnerFloor = 1e-3;
+
+template <int K>
+struct PipeSmem {
+  Smem<K> sm;
+  double red2[kMaxWarps * 2 * K];
+  double psum[2 * K][kPipeSplits];
+  double tau2[K], stop[K], gprev[K], aprev[K], alpha[K], beta[K];
+  int act[K];
+  int flag;
+  int wmax[kPipeSlices];
+  int base[kPipeSlices + 1];
+  int cached, own_s;
+};
+
+__host__ __device__ inline size_t align16(size_t b) { return (b + 15) & ~(size_t)15; }
+
+template <typename T, int K>
+__device__ __forceinline__ void load_m(const T* __restrict__ m, int j, T (&x)[K]) {
+  constexpr int W = MRow<T, K>::W, NC = MRow<T, K>::NC;
+  if (j < 0) {
+#pragma unroll
+    for (int c = 0; c < K; ++c) x[c] = (T)0;
+    return;
+  }
+  const uint4* src = reinterpret_cast<const uint4*>(m + (size_t)j * W);
+  T buf[W];
+#pragma unroll
+  for (int i = 0; i < NC; ++i) {
+    const uint4 v = src[i];
+    if constexpr (sizeof(T) == 4) {
+      buf[4 * i + 0] = __uint_as_float(v.x);
+      buf[4 * i + 1] = __uint_as_float(v.y);
+      buf[4 * i + 2] = __uint_as_float(v.z);
+      buf[4 * i + 3] = __uint_as_float(v.w);
+    } else {
+      buf[2 * i + 0] = __hiloint2double((int)v.y, (int)v.x);
+      buf[2 * i + 1] = __hiloint2double((int)v.w, (int)v.z);
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < K; ++c) x[c] = buf[c];
+}
+
+template <typename T, int K>
+__device__ __forceinline__ void store_m(T* __restrict__ m, int j, const T (&x)[K]) {
+  constexpr int W = MRow<T, K>::W, NC = MRow<T, K>::NC;
+  T buf[W];
+#pragma unroll
+  for (int c = 0; c < W; ++c) buf[c] = c < K ? x[c] : (T)0;
+  uint4* dst = reinterpret_cast<uint4*>(m + (size_t)j * W);
+#pragma unroll
+  for (int i = 0; i < NC; ++i) {
+    uint4 v;
+    if constexpr (sizeof(T) == 4) {
+      v.x = __float_as_uint(buf[4 * i + 0]);
+      v.y = __float_as_uint(buf[4 * i + 1]);
+      v.z = __float_as_uint(buf[4 * i + 2]);
+      v.w = __float_as_uint(buf[4 * i + 3]);
+    } else {
+      v.x = (unsigned)__double2loint(buf[2 * i + 0]);
+      v.y = (unsigned)__double2hiint(buf[2 * i + 0]);
+      v.z = (unsigned)__double2loint(buf[2 * i + 1]);
+      v.w = (unsigned)__double2hiint(buf[2 * i + 1]);
+    }
+    dst[i] = v;
+  }
+}
+
+// One row of A: entries at c[e * stride], v[e * stride] for e < len; a
+// column index < 0 is padding.
+template <typename T>
+struct RowRef {
+  const int* c;
+  const T* v;
+  int stride;
+  int len;
+};
+
+// acc = sum_e v_e m(c_e): U entries' indices and values first, then their U
+// row gathers, then the multiply-adds.
+template <typename T, int K, int U>
+__device__ __forceinline__ void gather_m(const RowRef<T>& rr, const T* __restrict__ m, T (&acc)[K]) {
+#pragma unroll
+  for (int c = 0; c < K; ++c) acc[c] = (T)0;
+  for (int e = 0; e < rr.len; e += U) {
+    int j[U];
+    T v[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const bool ok = e + u < rr.len;
+      j[u] = ok ? rr.c[(e + u) * rr.stride] : -1;
+      v[u] = ok ? rr.v[(e + u) * rr.stride] : (T)0;
+    }
+    T x[U][K];
+#pragma unroll
+    for (int u = 0; u < U; ++u) load_m<T, K>(m, j[u], x[u]);
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+#pragma unroll
+      for (int c = 0; c < K; ++c) acc[c] += v[u] * x[u][c];
+  }
+}
+
+// The gathers of QR rows at once (so all of their loads are in flight
+// together): acc[q] = sum_e v_e m(c_e) over row q's entries, rows with
+// ok[q] false give zero.
+template <typename T, int K, int U, int QR>
+__device__ __forceinline__ void gather_rows(const RowRef<T> (&rr)[QR], const bool (&ok)[QR],
+                                            const T* __restrict__ m, T (&acc)[QR][K]) {
+  int len = 0;
+#pragma unroll
+  for (int q = 0; q < QR; ++q) {
+#pragma unroll
+    for (int c = 0; c < K; ++c) acc[q][c] = (T)0;
+    if (ok[q] && rr[q].len > len) len = rr[q].len;
+  }
+  for (int e = 0; e < len; e += U) {
+    int j[QR][U];
+    T v[QR][U];
+#pragma unroll
+    for (int q = 0; q < QR; ++q)
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const bool g = ok[q] && e + u < rr[q].len;
+        j[q][u] = g ? rr[q].c[(e + u) * rr[q].stride] : -1;
+        v[q][u] = g ? rr[q].v[(e + u) * rr[q].stride] : (T)0;
+      }
+    T x[QR][U][K];
+#pragma unroll
+    for (int q = 0; q < QR; ++q)
+#pragma unroll
+      for (int u = 0; u < U; ++u) load_m<T, K>(m, j[q][u], x[q][u]);
+#pragma unroll
+    for (int q = 0; q < QR; ++q)
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+#pragma unroll
+        for (int c = 0; c < K; ++c) acc[q][c] += v[q][u] * x[q][u][c];
+  }
+}
+
+// Sum v[0..N) over the block and store sum c at out[c * stride] from thread
+// 0: warp level in A (one shuffle per value for the FP32 solve), then the
+// warp sums in FP64 in a fixed order.  The caller synchronises the block
+// before `red` is written again.
+template <int N, typename A>
+__device__ void block_reduce_strided(const A (&v)[N], double* red, double* out, int stride) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int c = 0; c < N; ++c) {
+    A t = v[c];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    if (lane == 0) red[warp * N + c] = (double)t;
+  }
+  __syncthreads();
+  if (warp == 0) {
+#pragma unroll
+    for (int c = 0; c < N; ++c) {
+      double t = lane < nw ? red[lane * N + c] : 0.0;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+      if (lane == 0) out[(size_t)c * stride] = t;
+    }
+  }
+}
+
+// Own-row state in T, one contiguous record of 6K + 1 values per row:
+// quantities r, w, z, s, p, x (K columns each), then 1/A_ii.  An odd record
+// length keeps the shared-memory accesses of a warp on distinct banks.
+enum { kQr = 0, kQw = 1, kQz = 2, kQs = 3, kQp = 4, kQx = 5, kQminv = 6 };
+template <typename T, int K>
+struct OwnRef {
+  static constexpr int kLen = 6 * K + 1;
+  T* p;
+  __device__ __forceinline__ T& operator()(int qy, int c) const { return p[qy * K + c]; }
+};
+
+// One own row's update of a pipelined iteration: z = n + beta z,
+// s = w + beta s, p = M^-1 r + beta p, x += alpha p, r -= alpha s,
+// w -= alpha z; m = M^-1 w to mnext; (r, M^-1 r) and (w, M^-1 r) into d2.
+template <typename T, int K>
+__device__ __forceinline__ void pipe_update(const OwnRef<T, K>& o, int row, const T (&nn)[K], const T (&alpha)[K],
+                                            const T (&beta)[K], bool b0, T* __restrict__ mnext, T (&d2)[2 * K]) {
+  const T mi = o(kQminv, 0);
+  T m[K];
+#pragma unroll
+  for (int c = 0; c < K; ++c) {
+    const T r0 = o(kQr, c), w0 = o(kQw, c);
+    const T zo = b0 ? (T)0 : o(kQz, c);
+    const T so = b0 ? (T)0 : o(kQs, c);
+    const T po = b0 ? (T)0 : o(kQp, c);
+    const T z = nn[c] + beta[c] * zo;
+    const T sx = w0 + beta[c] * so;
+    const T p = mi * r0 + beta[c] * po;
+    const T r = r0 - alpha[c] * sx;
+    const T w = w0 - alpha[c] * z;
+    o(kQx, c) += alpha[c] * p;
+    o(kQz, c) = z;
+    o(kQs, c) = sx;
+    o(kQp, c) = p;
+    o(kQr, c) = r;
+    o(kQw, c) = w;
+    m[c] = mi * w;
+    const T u = mi * r;
+    d2[c] += r * u;
+    d2[K + c] += w * u;
+  }
+  store_m<T, K>(mnext, row, m);
+}
+
+template <typename T, int K, int U, int QR, class Team>
+__device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, unsigned char* dyn) {
+  const T* Aval = (const T*)a.A_val;
+  T* mb0 = (T*)a.m0;
+  T* mb1 = (T*)a.m1;
+  const int n = a.n, B = blockDim.x, t = threadIdx.x;
+  const int R = team.size() * B;
+  const int blk0 = team.rank() * B;
+  const int row0 = blk0 + t;
+  const int Qb = n > blk0 ? (n - blk0 + R - 1) / R : 0;  // row slices of this block
+  const int tsize = team.size();
+  const int warp = t >> 5, lane = t & 31, nw = B >> 5;
+  double* part = a.partials;
+  auto slot_ptr = [&](int slot) { return part + ((size_t)slot * tsize) * K; };
+  // the pipelined partials (gamma, delta per column): parity g uses slots
+  // 2 + 2g .. 3 + 2g as a [2K][blocks] table (quantity-major, so a warp reads
+  // one quantity's partials with consecutive loads)
+  auto pipe_ptr = [&](int g) { return part + ((size_t)(2 + 2 * g) * tsize) * K; };
+  int status = CN_OK, total_iters = 0, refinements = 0;
+
+  // ---- shared memory: the block's rows of A, then (if it fits) the own-row
+  // state
+  {
+    if (t < kPipeSlices) s->wmax[t] = 0;
+    __syncthreads();
+    const int qc = Qb < kPipeSlices ? Qb : kPipeSlices;
+    for (int q = 0; q < qc; ++q) {
+      const int row = row0 + q * R;
+      if (row < n) atomicMax(&s->wmax[q], a.A_ptr[row + 1] - a.A_ptr[row]);
+    }
+    __syncthreads();
+    if (t == 0) {
+      int ents = 0;
+      for (int q = 0; q < qc; ++q) {
+        s->base[q] = ents;
+        ents += s->wmax[q] * B;
+      }
+      s->base[qc] = ents;
+      const size_t need = align16((size_t)ents * sizeof(int)) + align16((size_t)ents * sizeof(T));
+      const size_t own = (size_t)(6 * K + 1) * Qb * B * sizeof(T);
+      s->cached = (qc == Qb && Qb > 0 && need <= (size_t)a.cache_bytes) ? 1 : 0;
+      s->own_s = (s->cached && need + own <= (size_t)a.cache_bytes) ? 1 : 0;
+    }
+    __syncthreads();
+  }
+  const bool cached = s->cached != 0, own_s = s->own_s != 0;
+  const int ents = s->base[Qb < kPipeSlices ? Qb : kPipeSlices];
+  int* ccol = (int*)dyn;
+  T* cval = (T*)(dyn + align16((size_t)ents * sizeof(int)));
+  T* os = (T*)(dyn + align16((size_t)ents * sizeof(int)) + align16((size_t)ents * sizeof(T)));
+  T* pown = (T*)a.pown;
+  auto own_ref = [&](int q, int row) {
+    OwnRef<T, K> o;
+    o.p = own_s ? os + ((size_t)q * B + t) * OwnRef<T, K>::kLen : pown + (size_t)row * OwnRef<T, K>::kLen;
+    return o;
+  };
+  if (cached) {
+    for (int q = 0; q < Qb; ++q) {
+      const int row = row0 + q * R;
+      const int e0 = row < n ? a.A_ptr[row] : 0;
+      const int len = row < n ? a.A_ptr[row + 1] - e0 : 0;
+      const int wq = s->wmax[q], bq = s->base[q];
+      for (int e = 0; e < wq; ++e) {
+        const int ix = bq + e * B + t;
+        ccol[ix] = e < len ? a.A_col[e0 + e] : -1;
+        cval[ix] = e < len ? Aval[e0 + e] : (T)0;
+      }
+    }
+  }
+  for (int q = 0; q < Qb; ++q) {
+    const int row = row0 + q * R;
+    if (row >= n) break;
+    const double d = a.dinv64[row];
+    own_ref(q, row)(kQminv, 0) = (T)(d * d);  // dinv = 1 / sqrt(A_ii) (the pivots of the empty factor)
+  }
+  __syncthreads();
+  auto row_ref = [&](int q, int row) {
+    RowRef<T> rr;
+    if (cached) {
+      const int bq = s->base[q];
+      rr.c = ccol + bq + t;
+      rr.v = cval + bq + t;
+      rr.stride = B;
+      rr.len = s->wmax[q];
+    } else {
+      const int e0 = a.A_ptr[row];
+      rr.c = a.A_col + e0;
+      rr.v = Aval + e0;
+      rr.stride = 1;
+      rr.len = a.A_ptr[row + 1] - e0;
+    }
+    return rr;
+  };
+  // row slices q < QR: gathered together before the partial sums are needed
+  bool okq[QR];
+  RowRef<T> rrq[QR];
+  OwnRef<T, K> ownq[QR];
+#pragma unroll
+  for (int q = 0; q < QR; ++q) {
+    const int row = row0 + q * R;
+    okq[q] = q < Qb && row < n;
+    if (okq[q]) rrq[q] = row_ref(q, row);
+    ownq[q] = own_ref(q, okq[q] ? row : 0);
+  }
+
+  // ---- phase A: right-hand side (HarmonicSolve.lean:51-66 / DeformSolve.lean:123-135)
+  {
+    double bb[K];
+#pragma unroll
+    for (int c = 0; c < K; ++c) bb[c] = 0.0;
+    for (int q = 0; q < Qb; ++q) {
+      const int row = row0 + q * R;
+      if (row >= n) break;
+      double acc[K];
+#pragma unroll
+      for (int c = 0; c < K; ++c) acc[c] = 0.0;
+      const int v = a.free_of[row];
+      if (a.mode != CN_MODE_RHS) {
+        const bool deform = a.mode == CN_MODE_DEFORM;
+        gather_row<K, 1, 4>(a.K_ptr[v], a.K_ptr[v + 1], 0, a.K_col, a.K_val,
+                            [&](int u, double* d) {
+                              const int h = a.hidx[u];
+#pragma unroll
+                              for (int c = 0; c < K; ++c) {
+                                const double rest = deform ? a.pos[3 * u + c % 3] : 0.0;
+                                d[c] = h >= 0 ? a.targets[(size_t)h * K + c] - rest : -rest;
+                              }
+                            },
+                            acc);
+      }
+#pragma unroll
+      for (int c = 0; c < K; ++c) {
+        const double b = a.mode == CN_MODE_RHS ? a.targets[(size_t)row * K + c] : -acc[c];
+        a.b64[(size_t)row * K + c] = b;
+        bb[c] += b * b;
+        if (!a.warm) a.x64[(size_t)row * K + c] = a.x0 ? a.x0[(size_t)v * K + c] : 0.0;
+      }
+    }
+    block_reduce_store<K>(bb, s->sm.red, slot_ptr(kBB) + (size_t)team.rank() * K);
+    if (!team.sync()) { status = CN_TIMEOUT; goto done; }
+    team_sum<K>(slot_ptr(kBB), tsize, &s->sm);
+    if (t < K) s->sm.bb[t] = s->sm.sum[t];
+    __syncthreads();
+  }
+
+  for (int refine = 0;; ++refine) {
+    // ---- phase R: FP64 residual r = b - A x; u = M^-1 r goes to m0 for the
+    // first product w = A u
+    {
+      double rr[K];
+#pragma unroll
+      for (int c = 0; c < K; ++c) rr[c] = 0.0;
+      for (int q = 0; q < Qb; ++q) {
+        const int row = row0 + q * R;
+        if (row >= n) break;
+        double acc[K];
+#pragma unroll
+        for (int c = 0; c < K; ++c) acc[c] = 0.0;
+        gather_row<K, 1, 4>(a.A_ptr[row], a.A_ptr[row + 1], 0, a.A_col, a.A_val64,
+                            [&](int j, double* x) {
+#pragma unroll
+                              for (int c = 0; c < K; ++c) x[c] = a.x64[(size_t)j * K + c];
+                            },
+                            acc);
+        const OwnRef<T, K> o = own_ref(q, row);
+        const T mi = o(kQminv, 0);
+        T u[K];
+#pragma unroll
+        for (int c = 0; c < K; ++c) {
+          const double rv = a.b64[(size_t)row * K + c] - acc[c];
+          const T rt = (T)rv;
+          o(kQr, c) = rt;
+          o(kQx, c) = (T)0;
+          u[c] = mi * rt;
+          rr[c] += rv * rv;
+        }
+        store_m<T, K>(mb0, row, u);
+      }
+      block_reduce_store<K>(rr, s->sm.red, slot_ptr(kRR64) + (size_t)team.rank() * K);
+      if (!team.sync()) { status = CN_TIMEOUT; goto done; }
+      team_sum<K>(slot_ptr(kRR64), tsize, &s->sm);
+      if (t == 0) {
+        int any = 0, bad = 0;
+        for (int c = 0; c < K; ++c) {
+          const double rr64 = s->sm.sum[c], bb = s->sm.bb[c];
+          const double rel = bb > 0.0 ? sqrt(rr64 / bb) : sqrt(rr64);
+          if (c < 32) a.stats->rel_residual[c] = rel;
+          if (!(rel == rel)) bad = 1;
+          const int act = rel > a.tol;
+          s->act[c] = act;
+          any |= act;
+          // the inner solve stops when (r, M^-1 r) has fallen by tau^2
+          const double want = bb > 0.0 ? 0.5 * a.tol * sqrt(bb / (rr64 > 0.0 ? rr64 : 1.0)) : 0.0;
+          double tau = fmax(a.inner_tol, want);
+          if (sizeof(T) == 4) tau = fmax(tau, kPipeInnerFloor);
+          s->tau2[c] = tau * tau;
+        }
+        s->flag = bad ? 2 : (any ? 1 : 0);
+      }
+      __syncthreads();
+      if (s->flag == 2) { status = CN_NAN; break; }
+      if (s->flag == 0) { status = CN_OK; break; }
+      // max_refine bounds the number of inner solves
+      if (refine >= a.max_refine) { status = CN_MAX_ITER; break; }
+      refinements = refine + 1;
+    }
+
+    // ---- phase I: w = A u, m = M^-1 w (to m1), gamma = (r, u), delta = (w, u)
+    {
+      T d2[2 * K];
+#pragma unroll
+      for (int c = 0; c < 2 * K; ++c) d2[c] = (T)0;
+      for (int q = 0; q < Qb; ++q) {
+        const int row = row0 + q * R;
+        if (row >= n) break;
+        T acc[K];
+        gather_m<T, K, U>(row_ref(q, row), mb0, acc);
+        const OwnRef<T, K> o = own_ref(q, row);
+        const T mi = o(kQminv, 0);
+        T m[K];
+#pragma unroll
+        for (int c = 0; c < K; ++c) {
+          const T r = o(kQr, c), u = mi * r, w = acc[c];
+          o(kQw, c) = w;
+          m[c] = mi * w;
+          d2[c] += r * u;
+          d2[K + c] += w * u;
+        }
+        store_m<T, K>(mb1, row, m);
+      }
+      block_reduce_strided<2 * K, T>(d2, s->red2, pipe_ptr(0) + team.rank(), tsize);
+      if (!team.sync()) { status = CN_TIMEOUT; goto done; }
+    }
+
+    // ---- the pipelined iterations, one team barrier each
+    for (int it = 0;; ++it) {
+      const int g = it & 1;
+      const T* mcur = g ? mb0 : mb1;
+      T* mnext = g ? mb1 : mb0;
+      const bool b0 = it == 0;
+      // (1) the previous phase's partials: item (quantity fc, split sp) sums
+      // blocks [128 sp, 128 sp + 128); a warp's first item is loaded before
+      // the gathers, so both round trips overlap
+      const int ns = (tsize + 127) >> 7, items = 2 * K * ns;
+      const double* pp = pipe_ptr(g);
+      double pl[4];
+      const bool item0 = warp < items;
+      if (item0) {
+        const int fc = warp / ns, sp = warp - fc * ns;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const int b = sp * 128 + i * 32 + lane;
+          pl[i] = b < tsize ? __ldcg(pp + (size_t)fc * tsize + b) : 0.0;
+        }
+      }
+      // (2) row slices q < QR: the gathers of n = A m
+      T nq[QR][K];
+      gather_rows<T, K, U, QR>(rrq, okq, mcur, nq);
+      // (3) finish the partial sums
+      auto reduce_item = [&](int item, const double (&v)[4]) {
+        double x = (v[0] + v[1]) + (v[2] + v[3]);
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) x += __shfl_xor_sync(0xffffffffu, x, off);
+        const int fc = item / ns;
+        if (lane == 0) s->psum[fc][item - fc * ns] = x;
+      };
+      if (item0) reduce_item(warp, pl);
+      for (int item = warp + nw; item < items; item += nw) {
+        const int fc = item / ns, sp = item - fc * ns;
+        double v[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const int b = sp * 128 + i * 32 + lane;
+          v[i] = b < tsize ? __ldcg(pp + (size_t)fc * tsize + b) : 0.0;
+        }
+        reduce_item(item, v);
+      }
+      __syncthreads();
+      // (4) the scalars: lane c of warp 0 for column c
+      if (warp == 0) {
+        int act = 0, bad = 0;
+        if (lane < K) {
+          const int c = lane;
+          double gam = 0.0, del = 0.0;
+          for (int sp = 0; sp < ns; ++sp) {
+            gam += s->psum[c][sp];
+            del += s->psum[K + c][sp];
+          }
+          if (!(gam == gam) || !(del == del)) bad = 1;
+          act = s->act[c];
+          if (b0) s->stop[c] = s->tau2[c] * gam;
+          else if (act && gam < s->stop[c]) act = 0;
+          double be = 0.0, den = del;
+          if (!b0) {
+            const double gp = s->gprev[c];
+            be = gp == 0.0 ? 0.0 : gam / gp;
+            den = del - be * gam / s->aprev[c];
+          }
+          // a non-positive (p, Ap) ends this column's inner solve; the next
+          // FP64 residual decides whether it restarts
+          if (act && !(den > 0.0)) act = 0;
+          const double al = act ? gam / den : 0.0;
+          s->alpha[c] = al;
+          s->beta[c] = act ? be : 0.0;
+          s->act[c] = act;
+          s->gprev[c] = gam;
+          s->aprev[c] = act ? al : 1.0;
+        }
+        const int any = __any_sync(0xffffffffu, act), anybad = __any_sync(0xffffffffu, bad);
+        if (lane == 0) s->flag = anybad ? 2 : (any ? 1 : 0);
+      }
+      __syncthreads();
+      if (s->flag == 2) { status = CN_NAN; goto done; }
+      if (s->flag == 0 || it >= a.max_iter) break;
+      T alpha[K], beta[K];
+#pragma unroll
+      for (int c = 0; c < K; ++c) {
+        alpha[c] = (T)s->alpha[c];
+        beta[c] = (T)s->beta[c];
+      }
+      // (5) the updates of the own rows
+      T d2[2 * K];
+#pragma unroll
+      for (int c = 0; c < 2 * K; ++c) d2[c] = (T)0;
+#pragma unroll
+      for (int q = 0; q < QR; ++q)
+        if (okq[q]) pipe_update<T, K>(ownq[q], row0 + q * R, nq[q], alpha, beta, b0, mnext, d2);
+      for (int q = QR; q < Qb; ++q) {
+        const int row = row0 + q * R;
+        if (row >= n) break;
+        T nn[K];
+        gather_m<T, K, U>(row_ref(q, row), mcur, nn);
+        pipe_update<T, K>(own_ref(q, row), row, nn, alpha, beta, b0, mnext, d2);
+      }
+      block_reduce_strided<2 * K, T>(d2, s->red2, pipe_ptr(g ^ 1) + team.rank(), tsize);
+      ++total_iters;
+      if (!team.sync()) { status = CN_TIMEOUT; goto done; }
+    }
+    // ---- x64 += x (FP64 accumulation of the correction)
+    for (int q = 0; q < Qb; ++q) {
+      const int row = row0 + q * R;
+      if (row >= n) break;
+      const OwnRef<T, K> o = own_ref(q, row);
+#pragma unroll
+      for (int c = 0; c < K; ++c) a.x64[(size_t)row * K + c] += (double)o(kQx, c);
+    }
+    if (!team.sync()) { status = CN_TIMEOUT; goto done; }
+  }
+
+  // ---- output: free rows, then the handle overlay (DeformSolve.lean:108-109)
+  if (a.x_out) {
+    for (int q = 0; q < Qb; ++q) {
+      const int row = row0 + q * R;
+      if (row >= n) break;
+      const int v = a.free_of[row];
+#pragma unroll
+      for (int c = 0; c < K; ++c) a.x_out[(size_t)v * K + c] = a.x64[(size_t)row * K + c];
+    }
+    for (int h = row0; h < a.nh; h += R) {
+      const int v = a.handles[h];
+#pragma unroll
+      for (int c = 0; c < K; ++c)
+        a.x_out[(size_t)v * K + c] = a.mode == CN_MODE_RHS ? 0.0 : a.targets[(size_t)h * K + c];
+    }
+  }
+
+done:
+  if (team.rank() == 0 && t == 0) {
+    a.stats->status = status;
+    a.stats->iterations = total_iters;
+    a.stats->refinements = refinements;
+  }
+}
+
+// entries of a row gathered together: all of a mesh row in FP32, half of it in FP64
+template <typename T>
+constexpr int pipe_unroll() { return sizeof(T) == 4 ? 8 : 4; }
+
+// QR = 1: one row per thread, up to 1024 threads; QR = 2: two rows per
+// thread gathered together, up to 512 threads (twice the registers).
+template <typename T, int K, int QR>
+__global__ void __launch_bounds__(1024 / QR, 1) k_pipe_grid(SolveArgs a) {
+  __shared__ PipeSmem<K> s;
+  extern __shared__ __align__(16) unsigned char dyn[];
+  GridTeam team{a.ctl, a.timeout_ns, 0u};
+  pipe_body<T, K, pipe_unroll<T>(), QR>(a, team, &s, dyn);
+}
+
+template <typename T, int K>
+__global__ void __launch_bounds__(1024, 1) k_pipe_cta(SolveArgs a) {
+  __shared__ PipeSmem<K> s;
+  extern __shared__ __align__(16) unsigned char dyn[];
+  CtaTeam team;
+  pipe_body<T, K, pipe_unroll<T>(), 1>(a, team, &s, dyn);
+}
+
+template <typename T, int K>
+cudaError_t launch_pk(const SolveArgs& a, int block, int grid, int qr, cudaStream_t st) {
+  const int dyn = a.cache_bytes;
+  if (grid <= 1) {
+    SolveArgs c = a;
+    c.cache_bytes = 0;
+    k_pipe_cta<T, K><<<1, block, 0, st>>>(c);
+    return cudaGetLastError();
+  }
+  auto kern = qr == 2 ? k_pipe_grid<T, K, 2> : k_pipe_grid<T, K, 1>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+  if (e != cudaSuccess) return e;
+  SolveArgs copy = a;
+  void* args[] = {&copy};
+  return cudaLaunchCooperativeKernel((const void*)kern, dim3(grid), dim3(block), args, (size_t)dyn, st);
+}
+
+template <typename T, int K>
+int max_grid_pk(int block, int dyn, int qr) {
+  int dev = 0, sms = 0, per = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  auto kern = qr == 2 ? k_pipe_grid<T, K, 2> : k_pipe_grid<T, K, 1>;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn) != cudaSuccess) return 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, block, dyn) != cudaSuccess) return 0;
+  return sms * per;
+}
+
+}  // namespace
+
+cudaError_t launch_pipelined_solve(const SolveArgs& a, int precision, int K, int block, int grid, int qr,
+                                   cudaStream_t s) {
+  if (precision == CN_PREC_MIXED) {
+    if (K == 1) return launch_pk<float, 1>(a, block, grid, qr, s);
+    if (K == 3) return launch_pk<float, 3>(a, block, grid, qr, s);
+    if (K == 9) return launch_pk<float, 9>(a, block, grid, qr, s);
+  } else {
+    if (K == 1) return launch_pk<double, 1>(a, block, grid, qr, s);
+    if (K == 3) return launch_pk<double, 3>(a, block, grid, qr, s);
+    if (K == 9) return launch_pk<double, 9>(a, block, grid, qr, s);
+  }
+  return cudaErrorInvalidValue;
+}
+
+int pipelined_max_grid(int precision, int K, int block, int cache_bytes, int qr) {
+  if (precision == CN_PREC_MIXED) {
+    if (K == 1) return max_grid_pk<float, 1>(block, cache_bytes, qr);
+    if (K == 3) return max_grid_pk<float, 3>(block, cache_bytes, qr);
+    if (K == 9) return max_grid_pk<float, 9>(block, cache_bytes, qr);
+  } else {
+    if (K == 1) return max_grid_pk<double, 1>(block, cache_bytes, qr);
+    if (K == 3) return max_grid_pk<double, 3>(block, cache_bytes, qr);
+    if (K == 9) return max_grid_pk<double, 9>(block, cache_bytes, qr);
+  }
+  return 0;
+}
+
+void pipelined_smem_need(const int* A_ptr, int n, int grid, int block, int precision, int K, size_t* cache,
+                         size_t* full) {
+  const size_t vs = precision == CN_PREC_MIXED ? sizeof(float) : sizeof(double);
+  const long long R = (long long)grid * block;
+  size_t wc = 0, wf = 0;
+  *cache = *full = (size_t)-1;
+  for (int b = 0; b < grid; ++b) {
+    const long long blk0 = (long long)b * block;
+    if (blk0 >= n) break;
+    const long long Qb = (n - blk0 + R - 1) / R;
+    if (Qb > kPipeSlices) return;
+    size_t ents = 0;
+    for (long long q = 0; q < Qb; ++q) {
+      int w = 0;
+      for (int t = 0; t < block; ++t) {
+        const long long row = blk0 + t + q * R;
+        if (row < n) w = std::max(w, A_ptr[row + 1] - A_ptr[row]);
+      }
+      ents += (size_t)w * block;
+    }
+    const size_t c = align16(ents * sizeof(int)) + align16(ents * vs);
+    wc = std::max(wc, c);
+    wf = std::max(wf, c + (size_t)(6 * K + 1) * (size_t)Qb * (size_t)block * vs);
+  }
+  *cache = wc;
+  *full = wf;
+}
+
+}  // namespace cn

@@ -43,7 +43,7 @@ _ORDER = {"natural": L.ORDER_NATURAL, "color": L.ORDER_COLOR}
 _LAP = {"cot": L.LAPLACIAN_COT, "robust": L.LAPLACIAN_ROBUST}
 _PREC = {"fp64": L.PREC_FP64, "mixed": L.PREC_MIXED}
 _MODE = {"harmonic": L.MODE_HARMONIC, "deform": L.MODE_DEFORM, "rhs": L.MODE_RHS}
-_ALGO = {"fused": L.ALGO_FUSED, "plain": L.ALGO_PLAIN}
+_ALGO = {"fused": L.ALGO_FUSED, "plain": L.ALGO_PLAIN, "classic": L.ALGO_CLASSIC}
 
 
 def cut_mesh(n_verts, tris, loops):
