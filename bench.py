@@ -37,18 +37,58 @@ def load_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks and clock-event (throttle) reasons sampled through NVML every
+    few milliseconds during the timed region (read-only queries); nvidia-smi
+    at its 100 ms loop when NVML is not importable."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
-    def __init__(self, index):
+    def __init__(self, index, period_s=0.002):
         self.index = index
+        self.period = period_s
         self.proc = None
+        self.nvml = None
         self.lines = []
+        self.samples = []
+        self.stop_ev = threading.Event()
+
+    def _handle(self, nv):
+        try:
+            import torch
+            uuid = str(torch.cuda.get_device_properties(self.index).uuid)
+            return nv.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        except Exception:
+            return nv.nvmlDeviceGetHandleByIndex(self.index)
 
     def start(self):
+        try:
+            import pynvml as nv
+            nv.nvmlInit()
+            h = self._handle(nv)
+            bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                    "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                    "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                    "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+            self.max_mhz = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+            self.nvml = nv
+
+            def loop():
+                while not self.stop_ev.is_set():
+                    try:
+                        mhz = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                        r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                        self.samples.append((mhz, [k for k, b in bits.items() if r & b]))
+                    except Exception:
+                        pass
+                    time.sleep(self.period)
+            self.t = threading.Thread(target=loop, daemon=True)
+            self.t.start()
+            return
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
@@ -63,15 +103,21 @@ class ClockSampler:
             self.lines.append(line.strip())
 
     def stop(self):
+        if self.nvml is not None:
+            self.stop_ev.set()
+            self.t.join(timeout=2)
+            sm = [m for m, _ in self.samples]
+            reasons = sorted({r for _, rs in self.samples for r in rs})
+            return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.max_mhz,
+                    "reasons": reasons, "samples": len(sm), "source": "NVML, 2 ms period"}
         if not self.proc:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["clock query unavailable"]}
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
         except Exception:
             self.proc.kill()
         sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for ln in self.lines:
             p = [x.strip() for x in ln.split(",")]
             if len(p) < 9:
@@ -81,11 +127,11 @@ class ClockSampler:
                 mx = float(p[2])
             except ValueError:
                 continue
-            for nm, v in zip(names, p[5:9]):
+            for nm, v in zip(self.NAMES, p[5:9]):
                 if v.lower() == "active":
                     reasons.add(nm)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": "nvidia-smi, 100 ms period"}
 
 
 def algorithmic_bytes(info, stats, k, mixed):
@@ -114,6 +160,21 @@ def algorithmic_bytes_pipelined(info, stats, k, mixed):
     sv = 4 if mixed else 8
     sx = 4 if mixed else 8
     b_iter = nnz * (sv + 4) + 4 * (n + 1) + 2 * n * k * sx + 12 * n * k * sx + n * sx
+    b_res = nnz * 12 + 4 * (n + 1) + 3 * n * k * 8
+    b_rhs = info["nnz_K"] * 12 + 4 * (info["n_verts"] + 1) + n * k * 8
+    return stats.iterations * b_iter + (stats.refinements + 1) * b_res + b_rhs
+
+
+def algorithmic_bytes_classic(info, stats, k, mixed):
+    """Bytes the two-reduction Jacobi-PCG must move: per inner iteration one
+    SpMV (A's values and columns, row pointer, the gathered z and p), a read
+    and a write of the own-row vectors r, z, p, Ap, x plus 1/A_ii, and the
+    store of the [z | p] record; per FP64 residual evaluation one FP64 SpMV;
+    plus the FP64 right-hand side."""
+    n, nnz = info["n_free"], info["nnz_A"]
+    sv = 4 if mixed else 8
+    sx = 4 if mixed else 8
+    b_iter = nnz * (sv + 4) + 4 * (n + 1) + 2 * n * k * sx + 10 * n * k * sx + n * sx + 2 * n * k * sx
     b_res = nnz * 12 + 4 * (n + 1) + 3 * n * k * 8
     b_rhs = info["nnz_K"] * 12 + 4 * (info["n_verts"] + 1) + n * k * 8
     return stats.iterations * b_iter + (stats.refinements + 1) * b_res + b_rhs
@@ -298,7 +359,7 @@ def main():
     st_fp64 = one("fp64", stats=True)
     st_plain = one("fp64", "plain", stats=True)
     st_ic = one("mixed", stats=True, sv=solver_ic)
-    st_classic = one("mixed", "classic", stats=True)
+    st_classic = one("mixed", "pipelined", stats=True)
     for s in (st_mixed, st_fp64, st_plain, st_ic, st_classic):
         if s.status != 0:
             raise SystemExit(f"solve failed: status {s.status}")
@@ -331,7 +392,7 @@ def main():
     t_fp64 = timed("fp64", "fused", max(3, args.steps // 3), 2)
     t_plain = timed("fp64", "plain", 3, 1)
     t_ic = timed("mixed", "fused", max(3, args.steps // 3), 2, sv=solver_ic)
-    t_classic = timed("mixed", "classic", max(3, args.steps // 3), 2)
+    t_classic = timed("mixed", "pipelined", max(3, args.steps // 3), 2)
 
     # e2e: host (pinned) buffers through cn_solve, H2D of the targets and D2H of
     # the deformed positions inside the timed region
@@ -372,7 +433,7 @@ def main():
     ms_ic = maxred(sum(t_ic) / len(t_ic))
     ms_classic = maxred(sum(t_classic) / len(t_classic))
     peak, peak_kind = load_peaks()
-    bytes_mixed = algorithmic_bytes_pipelined(info, st_mixed, k, True)
+    bytes_mixed = algorithmic_bytes_classic(info, st_mixed, k, True)
     bytes_fp64 = algorithmic_bytes_pipelined(info, st_fp64, k, False)
     ach = bytes_mixed / (ms_mixed * 1e-3) / 1e9
     traffic = None
@@ -403,7 +464,7 @@ def main():
             "dtype": "f32 inner / f64 residual",
             "data": "synthetic (seeded torus, see tool_godot_curvenet_b200/synth.py config2)",
             "config": {"workload": WORKLOAD, "n_verts": nv, "n_free": info["n_free"], "nnz_A": info["nnz_A"],
-                       "rhs": k, "tol": 1e-8, "precond": "Jacobi, pipelined CG (one team barrier per iteration)",
+                       "rhs": k, "tol": 1e-8, "precond": "Jacobi, natural row order; two-reduction CG on the row-cached kernel (rows of A and the CG state in shared memory)",
                        "launch": f"grid {info['grid']} x block auto (2 rows per thread)", "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
                        "l2": "flushed (256 MB write) before every timed solve, outside the events"},
             "mixed": {"iterations": st_mixed.iterations, "refinements": st_mixed.refinements,
@@ -415,15 +476,15 @@ def main():
             "ic0_mixed": {"solves_per_s": 1e3 / ms_ic, "ms": ms_ic, "iterations": st_ic.iterations,
                           "n_levels": info_ic["n_levels"],
                           "note": "IC(0) in greedy-colour order, classic CG: 2 x n_levels team barriers per iteration"},
-            "jacobi_classic_mixed": {"solves_per_s": 1e3 / ms_classic, "ms": ms_classic,
-                                     "iterations": st_classic.iterations,
-                                     "note": "same preconditioner, classic CG: 2 team barriers per iteration"},
+            "jacobi_pipelined_mixed": {"solves_per_s": 1e3 / ms_classic, "ms": ms_classic,
+                                       "iterations": st_classic.iterations, "refinements": st_classic.refinements,
+                                       "note": "same kernel, pipelined CG in FP32 (one team barrier per iteration; not the default: its recurrences drift on ill-conditioned meshes)"},
             "speedup_mixed_vs_fp64_plain": ms_plain / ms_mixed,
             "speedup_mixed_vs_fp64_fused": ms_fp64 / ms_mixed,
             "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
                          "peak_kind": peak_kind, "traffic": traffic,
-                         "kernel": f"k_pipe_grid<float,3,2> (pipelined persistent solve, grid {info['grid']})",
-                         "note": "rows of A and the own-row state stay in shared memory, m in L2: DRAM traffic per launch is a small fraction of the algorithmic bytes; latency-bound (one team barrier and one L2 round trip per iteration)",
+                         "kernel": f"k_pipe_grid<float,3,2> (row-cached persistent solve, grid {info['grid']})",
+                         "note": "rows of A and the own-row state stay in shared memory, the gathered vectors in L2: DRAM traffic per launch is a small fraction of the algorithmic bytes; latency-bound (team barriers and L2 round trips)",
                          "algorithmic_bytes_per_launch": bytes_mixed,
                          "fp64_fused_achieved": bytes_fp64 / (ms_fp64 * 1e-3) / 1e9},
             "e2e": {"value": world * 1e3 / ms_e2e, "unit": "solves/s", "h2d_bytes_per_step": int(h_t.numel() * 8),

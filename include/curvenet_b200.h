@@ -54,19 +54,26 @@ typedef struct {
 } cn_mesh_desc;
 
 enum { CN_PRECOND_JACOBI = 0, CN_PRECOND_IC0 = 1, CN_PRECOND_HSC = 2 };
-enum { CN_ORDER_NATURAL = 0, CN_ORDER_COLOR = 1 };
+/* AUTO: COLOR with IC(0) (its levels), NATURAL otherwise (neighbouring
+ * vertices stay neighbouring rows, so row gathers coalesce). */
+enum { CN_ORDER_NATURAL = 0, CN_ORDER_COLOR = 1, CN_ORDER_AUTO = 2 };
 enum { CN_LAPLACIAN_COT = 0, CN_LAPLACIAN_ROBUST = 1 };
 enum { CN_PREC_FP64 = 0, CN_PREC_MIXED = 1 };
 enum { CN_MODE_HARMONIC = 0, CN_MODE_DEFORM = 1, CN_MODE_RHS = 2 };
-/* FUSED: one persistent launch; with Jacobi the pipelined CG (one team
- * barrier per iteration), otherwise the classic CG.  CLASSIC: one persistent
- * launch of the classic CG (two reductions per iteration) for every
- * preconditioner.  PLAIN: one kernel per primitive, FP64 Jacobi. */
-enum { CN_ALGO_FUSED = 0, CN_ALGO_PLAIN = 1, CN_ALGO_CLASSIC = 2 };
+/* FUSED: one persistent launch.  With Jacobi: the row-cached kernel (rows
+ * of A and each row's CG state in shared memory); in FP64 the pipelined CG
+ * (one team barrier per iteration, falling back to the two-reduction form if
+ * an inner solve stops reducing the residual), in mixed precision the
+ * two-reduction CG (two barriers per iteration; FP32 pipelined recurrences
+ * drift on ill-conditioned meshes).  With IC(0) / HSC: the level-scheduled
+ * kernel.  CLASSIC: the two-reduction CG (row-cached kernel with Jacobi).
+ * PIPELINED: the pipelined CG without fall-back, both precisions (Jacobi
+ * only).  PLAIN: one kernel per primitive, FP64 Jacobi. */
+enum { CN_ALGO_FUSED = 0, CN_ALGO_PLAIN = 1, CN_ALGO_CLASSIC = 2, CN_ALGO_PIPELINED = 3 };
 
 typedef struct {
   int32_t precond;       /* CN_PRECOND_* (default IC0) */
-  int32_t ordering;      /* CN_ORDER_* elimination order of IC(0) (default COLOR) */
+  int32_t ordering;      /* CN_ORDER_* row order of A (default AUTO) */
   int32_t laplacian;     /* CN_LAPLACIAN_* (default COT) */
   double mollify_delta;  /* delta of the robust (mollified) Laplacian */
   int32_t device;        /* CUDA device ordinal */
@@ -82,7 +89,7 @@ typedef struct {
 typedef struct {
   int32_t precision;   /* CN_PREC_FP64 or CN_PREC_MIXED */
   int32_t mode;        /* CN_MODE_HARMONIC, CN_MODE_DEFORM (targets) or CN_MODE_RHS */
-  int32_t algo;        /* CN_ALGO_FUSED, CN_ALGO_CLASSIC or CN_ALGO_PLAIN */
+  int32_t algo;        /* CN_ALGO_FUSED, CN_ALGO_CLASSIC, CN_ALGO_PIPELINED or CN_ALGO_PLAIN */
   double tol;          /* relative residual ||b - A x|| / ||b|| per column */
   int32_t max_iter;    /* inner PCG iterations per refinement step */
   int32_t max_refine;  /* FP64 residual refinements (mixed precision) */

@@ -234,10 +234,11 @@ def test_autotuner_picks_a_shape_that_solves(oracle, tmp_path):
 @pytest.mark.parametrize("k", [1, 3, 9])
 @pytest.mark.parametrize("grid,block", [(1, 1024), (8, 256), (2, 128), (148, 1024)])
 def test_jacobi_pipelined_matches_oracle_and_classic(k, grid, block, oracle):
-    """The pipelined Jacobi-PCG (one barrier per iteration; shared-memory row
-    cache with one or several row slices per thread, or global rows when a
-    block holds more slices than the cache does) against the oracle and the
-    classic two-reduction form."""
+    """The row-cached Jacobi kernel (shared-memory row cache with one or
+    several row slices per thread, or global rows when a block holds more
+    slices than the cache does): pipelined in FP64 and on request in mixed
+    precision, two-reduction in mixed precision by default; against the
+    oracle and the level-scheduled classic kernel."""
     pos, tris, h, _ = workload("torus_small")
     rng = np.random.default_rng(11 + k)
     t = rng.normal(size=(h.size, k))
@@ -247,7 +248,9 @@ def test_jacobi_pipelined_matches_oracle_and_classic(k, grid, block, oracle):
         r = s.solve(t, mode="harmonic", precision="fp64", tol=1e-13, max_iter=20000)
         rm = s.solve(t, mode="harmonic", precision="mixed", tol=1e-8, max_iter=20000)
         rc = s.solve(t, mode="harmonic", precision="fp64", tol=1e-13, max_iter=20000, algo="classic")
-    assert r.status == 0 and rm.status == 0 and rc.status == 0
+        rp = s.solve(t, mode="harmonic", precision="mixed", tol=1e-8, max_iter=20000, algo="pipelined")
+    assert r.status == 0 and rm.status == 0 and rc.status == 0 and rp.status == 0
+    assert rel_err(rp.x, xo) <= MIXED_TOL
     assert np.all(r.rel_residual <= 1e-13) and np.all(rm.rel_residual <= 1e-8)
     assert rel_err(r.x, xo) <= FP64_TOL
     assert rel_err(rm.x, xo) <= MIXED_TOL
@@ -265,3 +268,24 @@ def test_bad_algo_rejected():
                               np.empty((pos.shape[0], 3)).ctypes.data_as(L.C.POINTER(L.C.c_double)),
                               L.C.byref(o), None)
     assert st == L.CN_BAD_INPUT
+
+
+@pytest.mark.parametrize("mesh", [39, 143])
+def test_jacobi_mixed_converges_where_fp32_pipelining_drifts(mesh, oracle):
+    """Meshes of the batch workload (about 40k free rows) on which the FP32
+    pipelined recurrences lose track of the residual: the default mixed path
+    (two-reduction form) and the FP64 pipelined path converge and match the
+    oracle."""
+    from tool_godot_curvenet_b200 import cut_mesh, synth
+    m, h, t = synth.config3_mesh(mesh)
+    tris, parent = cut_mesh(m.positions.shape[0], m.tris, m.loops)
+    pos = np.ascontiguousarray(m.positions[parent])
+    t = np.ascontiguousarray(t.reshape(t.shape[0], -1)[:, :3])
+    ref = oracle.System(pos, tris, h)
+    st, xo, _, _ = ref.solve(t, mode=1, tol=1e-12)
+    with CutMeshSolver(pos, tris, h, precond="jacobi") as s:
+        rm = s.solve(t, mode="deform", precision="mixed", tol=1e-8)
+        rd = s.solve(t, mode="deform", precision="fp64", tol=1e-12, max_iter=20000)
+    assert rm.status == 0 and rd.status == 0
+    assert rel_err(rm.x, xo) <= MIXED_TOL
+    assert rel_err(rd.x, xo) <= 1e-8

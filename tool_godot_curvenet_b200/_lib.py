@@ -12,11 +12,11 @@ LIB_PATH = os.path.join(_HERE, "lib", "libcurvenet_b200.so")
 CN_OK, CN_MAX_ITER, CN_SINGULAR_COMPONENT, CN_NONPOS_PIVOT, CN_NAN = 0, 1, 2, 3, 4
 CN_BREAKDOWN, CN_TIMEOUT, CN_BAD_INPUT, CN_CUDA_ERROR, CN_NO_DEVICE = 5, 6, 7, 8, 9
 PRECOND_JACOBI, PRECOND_IC0, PRECOND_HSC = 0, 1, 2
-ORDER_NATURAL, ORDER_COLOR = 0, 1
+ORDER_NATURAL, ORDER_COLOR, ORDER_AUTO = 0, 1, 2
 LAPLACIAN_COT, LAPLACIAN_ROBUST = 0, 1
 PREC_FP64, PREC_MIXED = 0, 1
 MODE_HARMONIC, MODE_DEFORM, MODE_RHS = 0, 1, 2
-ALGO_FUSED, ALGO_PLAIN, ALGO_CLASSIC = 0, 1, 2
+ALGO_FUSED, ALGO_PLAIN, ALGO_CLASSIC, ALGO_PIPELINED = 0, 1, 2, 3
 
 
 class MeshDesc(C.Structure):

@@ -47,7 +47,7 @@ struct cn_system {
   Control* d_ctl = nullptr;
   DevStats* d_stats = nullptr;
   double *d_targets = nullptr, *d_xout = nullptr, *d_scal = nullptr;
-  double *d_pown = nullptr, *d_m[2] = {};   // pipelined solve: FP64 own-row state, two copies of m
+  double *d_pown = nullptr, *d_m[3] = {};   // row-cached solve: own-row state, gather buffers
   int* d_status = nullptr;
   // pipelined solve: shared-memory needs of the last (grid, block, precision, k)
   int pipe_grid = -1, pipe_block = -1, pipe_prec = -1, pipe_k = -1;
@@ -91,7 +91,7 @@ void layout_all(cn::Bump& b, cn_system* S) {
     S->d_w32[i] = b.take<float>(nk);
   }
   S->d_pown = b.take<double>(7 * nk);
-  for (int i = 0; i < 2; ++i) S->d_m[i] = b.take<double>((size_t)std::max(S->H.n, 1) * (S->kmax + 1));
+  for (int i = 0; i < 3; ++i) S->d_m[i] = b.take<double>((size_t)std::max(S->H.n, 1) * (2 * S->kmax + 2));
   S->d_partials = b.take<double>((size_t)cn::kSlots * S->max_grid_alloc * S->kmax);
   S->d_scal = b.take<double>(64);
   S->d_ctl = b.take<Control>(1);
@@ -208,7 +208,7 @@ extern "C" {
 void cn_default_build_opts(cn_build_opts* o) {
   std::memset(o, 0, sizeof *o);
   o->precond = CN_PRECOND_IC0;
-  o->ordering = CN_ORDER_COLOR;
+  o->ordering = CN_ORDER_AUTO;
   o->laplacian = CN_LAPLACIAN_COT;
   o->mollify_delta = 1e-4;
   o->device = 0;
@@ -448,7 +448,7 @@ cn_status cn_solve_device(cn_handle S, int32_t k, const double* d_targets, doubl
     return CN_BAD_INPUT;
   }
   if (!(o.tol > 0.0) || o.max_iter < 0 || o.max_refine < 1 || o.algo < CN_ALGO_FUSED ||
-      o.algo > CN_ALGO_CLASSIC) {
+      o.algo > CN_ALGO_PIPELINED) {
     set_err("bad solve options");
     return CN_BAD_INPUT;
   }
@@ -485,9 +485,22 @@ cn_status cn_solve_device(cn_handle S, int32_t k, const double* d_targets, doubl
   a.max_refine = o.max_refine;
   a.ctl = S->d_ctl; a.stats = S->d_stats;
   a.timeout_ns = 2000000000LL;
-  a.m0 = S->d_m[0]; a.m1 = S->d_m[1]; a.pown = S->d_pown; a.dinv64 = S->D.dinv64;
-  if (!S->hsc && S->opts.precond == CN_PRECOND_JACOBI && o.algo == CN_ALGO_FUSED) {
-    int grid = S->grid, block = S->block, qr = 1;
+  a.m0 = S->d_m[0]; a.m1 = S->d_m[1]; a.m2 = S->d_m[2]; a.pown = S->d_pown; a.dinv64 = S->D.dinv64;
+  if (o.algo == CN_ALGO_PIPELINED && (S->hsc || S->opts.precond != CN_PRECOND_JACOBI)) {
+    set_err("the pipelined form needs the Jacobi preconditioner");
+    return CN_BAD_INPUT;
+  }
+  if (!S->hsc && S->opts.precond == CN_PRECOND_JACOBI) {
+    // FP64: pipelined, falling back to the two-reduction form if an inner
+    // solve stalls; mixed: the two-reduction form (the FP32 pipelined
+    // recurrences drift on ill-conditioned meshes), pipelined on request
+    a.pipe_mode = o.algo == CN_ALGO_PIPELINED ? 1 : o.algo == CN_ALGO_CLASSIC ? 0
+                : o.precision == CN_PREC_FP64 ? 2 : 0;
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, S->device);
+    // the grid: every SM, or fewer blocks of at least 256 rows for a small mesh
+    int grid = S->opts.grid > 0 ? S->opts.grid : std::min(sms, std::max(1, (S->H.n + 255) / 256));
+    int block = S->block, qr = 1;
     a.cache_bytes = 0;
     if (grid > 1) {
       grid = std::min(grid, S->max_grid_alloc);

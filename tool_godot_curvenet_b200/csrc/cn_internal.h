@@ -75,6 +75,8 @@ struct SolveArgs {
   // that neighbouring rows gather ([rows][round_up(K, 16 B)])
   void* m0;   // T
   void* m1;   // T
+  void* m2;   // T (the classic form's first records [z | p])
+  int pipe_mode;
   double* pown;            // FP64 own-row state when it is not in shared memory: 7 x [rows][K]
   const double* dinv64;    // 1 / sqrt(A_ii), FP64
   int cache_bytes;         // dynamic shared memory (row cache, then own-row state)
@@ -117,11 +119,13 @@ cudaError_t launch_persistent_solve(const SolveArgs& a, int precision, int K, in
 // Largest co-resident grid of the persistent solve for this configuration.
 int persistent_max_grid(int precision, int K, int lanes, int block);
 
-// The pipelined Jacobi-PCG persistent solve (cn_pipe.cu): one team barrier
-// per iteration.  a.cache_bytes of dynamic shared memory hold each block's
-// rows of A.
+// The row-cached Jacobi-PCG persistent solve (cn_pipe.cu).  a.cache_bytes of
+// dynamic shared memory hold each block's rows of A and their CG state.
 // qr: rows per thread gathered together (1: up to 1024 threads per block,
-// 2: up to 512).
+// 2: up to 512).  a.pipe_mode: 0 the classic two-reduction form (two
+// barriers per iteration), 1 the pipelined form, 2 the pipelined form with a
+// fall-back to the classic one when an inner solve stops reducing the FP64
+// residual.
 cudaError_t launch_pipelined_solve(const SolveArgs& a, int precision, int K, int block, int grid, int qr,
                                    cudaStream_t s);
 int pipelined_max_grid(int precision, int K, int block, int cache_bytes, int qr);

@@ -194,7 +194,8 @@ cn_status build_host(const cn_mesh_desc* m, const cn_build_opts& o, MeshHost& H)
     }
     S->ncolors = nc;
   }
-  if (o.ordering == CN_ORDER_COLOR)
+  const bool by_color = o.ordering == CN_ORDER_COLOR || (o.ordering == CN_ORDER_AUTO && o.precond == CN_PRECOND_IC0);
+  if (by_color)
     std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return color[a] < color[b]; });
   // level of every unknown in that order; rows sorted by level
   std::vector<int> posn(n), level(n, 0);

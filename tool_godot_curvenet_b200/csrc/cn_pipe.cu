@@ -59,7 +59,8 @@ struct PipeSmem {
   Smem<K> sm;
   double red2[kMaxWarps * 2 * K];
   double psum[2 * K][kPipeSplits];
-  double tau2[K], stop[K], gprev[K], aprev[K], alpha[K], beta[K];
+  double tau2[K], stop[K], gprev[K], aprev[K], alpha[K], beta[K], rrprev[K];
+  int use_pipe;
   int act[K];
   int flag;
   int wmax[kPipeSlices];
@@ -264,11 +265,15 @@ __device__ __forceinline__ void pipe_update(const OwnRef<T, K>& o, int row, cons
   store_m<T, K>(mnext, row, m);
 }
 
-template <typename T, int K, int U, int QR, class Team>
+template <typename T, int K, int QR, class Team>
 __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, unsigned char* dyn) {
+  // entries of a row gathered together: the pipelined form gathers K values
+  // per neighbour, the classic form 2K ([z | p])
+  constexpr int UP = sizeof(T) == 4 ? 8 : 4, UC = sizeof(T) == 4 ? 4 : 2;
   const T* Aval = (const T*)a.A_val;
   T* mb0 = (T*)a.m0;
   T* mb1 = (T*)a.m1;
+  T* mb2 = (T*)a.m2;
   const int n = a.n, B = blockDim.x, t = threadIdx.x;
   const int R = team.size() * B;
   const int blk0 = team.rank() * B;
@@ -430,7 +435,7 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
                             acc);
         const OwnRef<T, K> o = own_ref(q, row);
         const T mi = o(kQminv, 0);
-        T u[K];
+        T u[2 * K];
 #pragma unroll
         for (int c = 0; c < K; ++c) {
           const double rv = a.b64[(size_t)row * K + c] - acc[c];
@@ -438,17 +443,33 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
           o(kQr, c) = rt;
           o(kQx, c) = (T)0;
           u[c] = mi * rt;
+          u[K + c] = (T)0;
+          o(kQz, c) = u[c];
           rr[c] += rv * rv;
         }
-        store_m<T, K>(mb0, row, u);
+        // both forms' first gathers: u = M^-1 r (pipelined, to m0) and the
+        // record [z | p = 0] (classic, to m2)
+        T m[K];
+#pragma unroll
+        for (int c = 0; c < K; ++c) m[c] = u[c];
+        store_m<T, K>(mb0, row, m);
+        store_m<T, 2 * K>(mb2, row, u);
       }
       block_reduce_store<K>(rr, s->sm.red, slot_ptr(kRR64) + (size_t)team.rank() * K);
       if (!team.sync()) { status = CN_TIMEOUT; goto done; }
       team_sum<K>(slot_ptr(kRR64), tsize, &s->sm);
       if (t == 0) {
         int any = 0, bad = 0;
+        // the pipelined form falls back to the classic one (for the rest of
+        // the solve) when its last inner solve cut the FP64 residual of some
+        // column by less than 10x
+        if (refine == 0) s->use_pipe = a.pipe_mode != 0;
+        if (s->use_pipe && a.pipe_mode == 2 && refine > 0)
+          for (int c = 0; c < K; ++c)
+            if (s->rrprev[c] > 0.0 && !(s->sm.sum[c] <= 1e-2 * s->rrprev[c])) s->use_pipe = 0;
         for (int c = 0; c < K; ++c) {
           const double rr64 = s->sm.sum[c], bb = s->sm.bb[c];
+          s->rrprev[c] = rr64;
           const double rel = bb > 0.0 ? sqrt(rr64 / bb) : sqrt(rr64);
           if (c < 32) a.stats->rel_residual[c] = rel;
           if (!(rel == rel)) bad = 1;
@@ -458,8 +479,9 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
           // the inner solve stops when (r, M^-1 r) has fallen by tau^2
           const double want = bb > 0.0 ? 0.5 * a.tol * sqrt(bb / (rr64 > 0.0 ? rr64 : 1.0)) : 0.0;
           double tau = fmax(a.inner_tol, want);
-          if (sizeof(T) == 4) tau = fmax(tau, kPipeInnerFloor);
+          if (s->use_pipe && sizeof(T) == 4) tau = fmax(tau, kPipeInnerFloor);
           s->tau2[c] = tau * tau;
+          s->stop[c] = tau * tau * rr64;  // the classic form tests ||r||^2
         }
         s->flag = bad ? 2 : (any ? 1 : 0);
       }
@@ -471,6 +493,8 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
       refinements = refine + 1;
     }
 
+    bool pipe_failed = false;
+    if (s->use_pipe) {
     // ---- phase I: w = A u, m = M^-1 w (to m1), gamma = (r, u), delta = (w, u)
     {
       T d2[2 * K];
@@ -480,7 +504,7 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
         const int row = row0 + q * R;
         if (row >= n) break;
         T acc[K];
-        gather_m<T, K, U>(row_ref(q, row), mb0, acc);
+        gather_m<T, K, UP>(row_ref(q, row), mb0, acc);
         const OwnRef<T, K> o = own_ref(q, row);
         const T mi = o(kQminv, 0);
         T m[K];
@@ -521,7 +545,7 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
       }
       // (2) row slices q < QR: the gathers of n = A m
       T nq[QR][K];
-      gather_rows<T, K, U, QR>(rrq, okq, mcur, nq);
+      gather_rows<T, K, UP, QR>(rrq, okq, mcur, nq);
       // (3) finish the partial sums
       auto reduce_item = [&](int item, const double (&v)[4]) {
         double x = (v[0] + v[1]) + (v[2] + v[3]);
@@ -576,7 +600,14 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
         if (lane == 0) s->flag = anybad ? 2 : (any ? 1 : 0);
       }
       __syncthreads();
-      if (s->flag == 2) { status = CN_NAN; goto done; }
+      if (s->flag == 2) {
+        if (a.pipe_mode == 2) {  // drop this inner solve, continue in the classic form
+          pipe_failed = true;
+          break;
+        }
+        status = CN_NAN;
+        goto done;
+      }
       if (s->flag == 0 || it >= a.max_iter) break;
       T alpha[K], beta[K];
 #pragma unroll
@@ -595,12 +626,180 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
         const int row = row0 + q * R;
         if (row >= n) break;
         T nn[K];
-        gather_m<T, K, U>(row_ref(q, row), mcur, nn);
+        gather_m<T, K, UP>(row_ref(q, row), mcur, nn);
         pipe_update<T, K>(own_ref(q, row), row, nn, alpha, beta, b0, mnext, d2);
       }
       block_reduce_strided<2 * K, T>(d2, s->red2, pipe_ptr(g ^ 1) + team.rank(), tsize);
       ++total_iters;
       if (!team.sync()) { status = CN_TIMEOUT; goto done; }
+    }
+    } else {
+    // ---- the classic two-reduction CG in two phases per iteration:
+    //   S: p = z + beta p' (each row gathers its neighbours' record [z | p']
+    //      and forms A p = A z + beta A p' without waiting for beta), (p, Ap)
+    //   U: alpha = (r, z) / (p, Ap); x += alpha p; r -= alpha Ap;
+    //      z = M^-1 r; the record [z | p] for the next S; (r, z), ||r||^2
+    // Partial tables [2K][blocks]: tS = (p.Ap, r.z) from S, tU = (r.z, r.r)
+    // from U (each is read in the phase after the barrier that follows its
+    // writes, and written again only after the next barrier).
+    double* tS = part + (size_t)2 * tsize * K;
+    double* tU = part + (size_t)4 * tsize * K;
+    const int ns = (tsize + 127) >> 7, items = 2 * K * ns;
+    auto load_item = [&](const double* tbl, int item, double (&v)[4]) {
+      const int fc = item / ns, sp = item - fc * ns;
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int b = sp * 128 + i * 32 + lane;
+        v[i] = b < tsize ? __ldcg(tbl + (size_t)fc * tsize + b) : 0.0;
+      }
+    };
+    auto reduce_item = [&](int item, const double (&v)[4]) {
+      double x = (v[0] + v[1]) + (v[2] + v[3]);
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) x += __shfl_xor_sync(0xffffffffu, x, off);
+      const int fc = item / ns;
+      if (lane == 0) s->psum[fc][item - fc * ns] = x;
+    };
+    for (int it = 0;; ++it) {
+      const int g = it & 1;
+      const T* rcur = g ? mb1 : mb2;
+      T* rnext = g ? mb2 : mb1;
+      const bool b0 = it == 0;
+      // ---- phase S
+      double pl[4];
+      const bool item0 = !b0 && warp < items;
+      if (item0) load_item(tU, warp, pl);
+      T accq[QR][2 * K];
+      gather_rows<T, 2 * K, UC, QR>(rrq, okq, rcur, accq);
+      if (item0) reduce_item(warp, pl);
+      if (!b0)
+        for (int item = warp + nw; item < items; item += nw) {
+          double v[4];
+          load_item(tU, item, v);
+          reduce_item(item, v);
+        }
+      __syncthreads();
+      if (warp == 0) {
+        int act = 0, bad = 0;
+        if (lane < K) {
+          const int c = lane;
+          act = s->act[c];
+          double be = 0.0;
+          if (!b0) {
+            double rzn = 0.0, rr = 0.0;
+            for (int sp = 0; sp < ns; ++sp) {
+              rzn += s->psum[c][sp];
+              rr += s->psum[K + c][sp];
+            }
+            if (!(rzn == rzn) || !(rr == rr)) bad = 1;
+            if (act && rr < s->stop[c]) act = 0;
+            be = s->gprev[c] == 0.0 ? 0.0 : rzn / s->gprev[c];
+          }
+          s->beta[c] = act ? be : 0.0;
+          s->act[c] = act;
+        }
+        const int any = __any_sync(0xffffffffu, act), anybad = __any_sync(0xffffffffu, bad);
+        if (lane == 0) s->flag = anybad ? 2 : (any ? 1 : 0);
+      }
+      __syncthreads();
+      if (s->flag == 2) { status = CN_NAN; goto done; }
+      if (s->flag == 0 || it >= a.max_iter) break;
+      {
+        T beta[K];
+#pragma unroll
+        for (int c = 0; c < K; ++c) beta[c] = (T)s->beta[c];
+        T d2[2 * K];
+#pragma unroll
+        for (int c = 0; c < 2 * K; ++c) d2[c] = (T)0;
+        auto form_p = [&](const OwnRef<T, K>& o, const T (&acc)[2 * K]) {
+#pragma unroll
+          for (int c = 0; c < K; ++c) {
+            const T z = o(kQz, c);
+            const T po = b0 ? (T)0 : o(kQp, c);
+            const T p = z + beta[c] * po;
+            const T ap = acc[c] + beta[c] * acc[K + c];
+            o(kQp, c) = p;
+            o(kQw, c) = ap;  // A p, kept for phase U
+            d2[c] += p * ap;
+            d2[K + c] += o(kQr, c) * z;
+          }
+        };
+#pragma unroll
+        for (int q = 0; q < QR; ++q)
+          if (okq[q]) form_p(ownq[q], accq[q]);
+        for (int q = QR; q < Qb; ++q) {
+          const int row = row0 + q * R;
+          if (row >= n) break;
+          RowRef<T> r1[1] = {row_ref(q, row)};
+          const bool ok1[1] = {true};
+          T acc1[1][2 * K];
+          gather_rows<T, 2 * K, UC, 1>(r1, ok1, rcur, acc1);
+          form_p(own_ref(q, row), acc1[0]);
+        }
+        block_reduce_strided<2 * K, T>(d2, s->red2, tS + team.rank(), tsize);
+      }
+      if (!team.sync()) { status = CN_TIMEOUT; goto done; }
+      // ---- phase U
+      for (int item = warp; item < items; item += nw) {
+        double v[4];
+        load_item(tS, item, v);
+        reduce_item(item, v);
+      }
+      __syncthreads();
+      if (warp == 0 && lane < K) {
+        const int c = lane;
+        double pap = 0.0, rz = 0.0;
+        for (int sp = 0; sp < ns; ++sp) {
+          pap += s->psum[c][sp];
+          rz += s->psum[K + c][sp];
+        }
+        int act = s->act[c];
+        // SparseLinAlg.lean:118 stops on pAp == 0; a non-positive value ends
+        // this column's inner solve (the next FP64 residual decides)
+        if (act && !(pap > 0.0)) act = 0;
+        s->alpha[c] = act ? rz / pap : 0.0;
+        s->gprev[c] = rz;
+        s->act[c] = act;
+      }
+      __syncthreads();
+      {
+        T alpha[K];
+#pragma unroll
+        for (int c = 0; c < K; ++c) alpha[c] = (T)s->alpha[c];
+        T d2[2 * K];
+#pragma unroll
+        for (int c = 0; c < 2 * K; ++c) d2[c] = (T)0;
+        for (int q = 0; q < Qb; ++q) {
+          const int row = row0 + q * R;
+          if (row >= n) break;
+          const OwnRef<T, K> o = own_ref(q, row);
+          const T mi = o(kQminv, 0);
+          T rec[2 * K];
+#pragma unroll
+          for (int c = 0; c < K; ++c) {
+            const T p = o(kQp, c);
+            o(kQx, c) += alpha[c] * p;
+            const T r = o(kQr, c) - alpha[c] * o(kQw, c);
+            const T z = mi * r;
+            o(kQr, c) = r;
+            o(kQz, c) = z;
+            rec[c] = z;
+            rec[K + c] = p;
+            d2[c] += r * z;
+            d2[K + c] += r * r;
+          }
+          store_m<T, 2 * K>(rnext, row, rec);
+        }
+        block_reduce_strided<2 * K, T>(d2, s->red2, tU + team.rank(), tsize);
+      }
+      ++total_iters;
+      if (!team.sync()) { status = CN_TIMEOUT; goto done; }
+    }
+    }
+    if (pipe_failed) {
+      __syncthreads();
+      if (t == 0) s->use_pipe = 0;
+      continue;  // x64 unchanged: the next residual is this one again
     }
     // ---- x64 += x (FP64 accumulation of the correction)
     for (int q = 0; q < Qb; ++q) {
@@ -649,7 +848,7 @@ __global__ void __launch_bounds__(1024 / QR, 1) k_pipe_grid(SolveArgs a) {
   __shared__ PipeSmem<K> s;
   extern __shared__ __align__(16) unsigned char dyn[];
   GridTeam team{a.ctl, a.timeout_ns, 0u};
-  pipe_body<T, K, pipe_unroll<T>(), QR>(a, team, &s, dyn);
+  pipe_body<T, K, QR>(a, team, &s, dyn);
 }
 
 template <typename T, int K>
@@ -657,7 +856,7 @@ __global__ void __launch_bounds__(1024, 1) k_pipe_cta(SolveArgs a) {
   __shared__ PipeSmem<K> s;
   extern __shared__ __align__(16) unsigned char dyn[];
   CtaTeam team;
-  pipe_body<T, K, pipe_unroll<T>(), 1>(a, team, &s, dyn);
+  pipe_body<T, K, 1>(a, team, &s, dyn);
 }
 
 template <typename T, int K>

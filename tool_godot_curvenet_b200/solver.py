@@ -39,11 +39,12 @@ def _dp(a):
 
 
 _PRECOND = {"jacobi": L.PRECOND_JACOBI, "ic0": L.PRECOND_IC0, "hsc": L.PRECOND_HSC}
-_ORDER = {"natural": L.ORDER_NATURAL, "color": L.ORDER_COLOR}
+_ORDER = {"natural": L.ORDER_NATURAL, "color": L.ORDER_COLOR, "auto": L.ORDER_AUTO}
 _LAP = {"cot": L.LAPLACIAN_COT, "robust": L.LAPLACIAN_ROBUST}
 _PREC = {"fp64": L.PREC_FP64, "mixed": L.PREC_MIXED}
 _MODE = {"harmonic": L.MODE_HARMONIC, "deform": L.MODE_DEFORM, "rhs": L.MODE_RHS}
-_ALGO = {"fused": L.ALGO_FUSED, "plain": L.ALGO_PLAIN, "classic": L.ALGO_CLASSIC}
+_ALGO = {"fused": L.ALGO_FUSED, "plain": L.ALGO_PLAIN, "classic": L.ALGO_CLASSIC,
+         "pipelined": L.ALGO_PIPELINED}
 
 
 def cut_mesh(n_verts, tris, loops):
@@ -77,7 +78,7 @@ class SolveResult:
 class CutMeshSolver:
     """Assembled and factored system of one cut mesh on one GPU."""
 
-    def __init__(self, positions, tris, handles, precond="ic0", ordering="color",
+    def __init__(self, positions, tris, handles, precond="ic0", ordering="auto",
                  laplacian="cot", mollify_delta=1e-4, max_rhs=3, device=0, lanes=0,
                  block=0, grid=0, hsc_tail_rows=0, hsc_theta=0.0):
         self.positions = _f64(positions).reshape(-1, 3)
@@ -249,7 +250,7 @@ class BatchSolver:
     launch per solve of all meshes x k right-hand sides (cn_build_batch /
     cn_solve_batch).  meshes: list of (positions, tris, handles)."""
 
-    def __init__(self, meshes, k=24, precond="ic0", ordering="color", laplacian="cot",
+    def __init__(self, meshes, k=24, precond="ic0", ordering="auto", laplacian="cot",
                  mollify_delta=1e-4, device=0, cluster_size=0, n_clusters=0, block=0):
         self.k = k
         self._keep = []
