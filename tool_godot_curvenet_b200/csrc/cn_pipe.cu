@@ -195,10 +195,10 @@ __device__ __forceinline__ void gather_rows(const RowRef<T> (&rr)[QR], const boo
   }
 }
 
-// Sum v[0..N) over the block and store sum c at out[c * stride] from thread
-// 0: warp level in A (one shuffle per value for the FP32 solve), then the
-// warp sums in FP64 in a fixed order.  The caller synchronises the block
-// before `red` is written again.
+// Sum v[0..N) over the block and store sum c at out[c * stride]: warp level
+// in A (one shuffle per value for the FP32 solve), then thread c adds the
+// warp sums of value c in FP64 in a fixed order.  The caller synchronises
+// the block before `red` is written again.
 template <int N, typename A>
 __device__ void block_reduce_strided(const A (&v)[N], double* red, double* out, int stride) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -210,14 +210,12 @@ __device__ void block_reduce_strided(const A (&v)[N], double* red, double* out, 
     if (lane == 0) red[warp * N + c] = (double)t;
   }
   __syncthreads();
-  if (warp == 0) {
-#pragma unroll
-    for (int c = 0; c < N; ++c) {
-      double t = lane < nw ? red[lane * N + c] : 0.0;
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
-      if (lane == 0) out[(size_t)c * stride] = t;
-    }
+  // thread c adds the warp sums of value c (independent shared loads)
+  if ((int)threadIdx.x < N) {
+    const int c = threadIdx.x;
+    double t = 0.0;
+    for (int w = 0; w < nw; ++w) t += red[w * N + c];
+    out[(size_t)c * stride] = t;
   }
 }
 
@@ -267,9 +265,8 @@ __device__ __forceinline__ void pipe_update(const OwnRef<T, K>& o, int row, cons
 
 template <typename T, int K, int QR, class Team>
 __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, unsigned char* dyn) {
-  // entries of a row gathered together: the pipelined form gathers K values
-  // per neighbour, the classic form 2K ([z | p])
-  constexpr int UP = sizeof(T) == 4 ? 8 : 4, UC = sizeof(T) == 4 ? 4 : 2;
+  // entries of a row gathered together (K values per neighbour in both forms)
+  constexpr int UP = sizeof(T) == 4 ? 8 : 4;
   const T* Aval = (const T*)a.A_val;
   T* mb0 = (T*)a.m0;
   T* mb1 = (T*)a.m1;
@@ -447,13 +444,13 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
           o(kQz, c) = u[c];
           rr[c] += rv * rv;
         }
-        // both forms' first gathers: u = M^-1 r (pipelined, to m0) and the
-        // record [z | p = 0] (classic, to m2)
+        // both forms' first gathers: u = M^-1 r (pipelined, to m0) and
+        // z = M^-1 r (classic, to m2)
         T m[K];
 #pragma unroll
         for (int c = 0; c < K; ++c) m[c] = u[c];
         store_m<T, K>(mb0, row, m);
-        store_m<T, 2 * K>(mb2, row, u);
+        store_m<T, K>(mb2, row, m);
       }
       block_reduce_store<K>(rr, s->sm.red, slot_ptr(kRR64) + (size_t)team.rank() * K);
       if (!team.sync()) { status = CN_TIMEOUT; goto done; }
@@ -635,10 +632,10 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
     }
     } else {
     // ---- the classic two-reduction CG in two phases per iteration:
-    //   S: p = z + beta p' (each row gathers its neighbours' record [z | p']
-    //      and forms A p = A z + beta A p' without waiting for beta), (p, Ap)
+    //   S: p = z + beta p'; A p = A z + beta A p' (each row gathers its
+    //      neighbours' z, without waiting for beta), (p, Ap)
     //   U: alpha = (r, z) / (p, Ap); x += alpha p; r -= alpha Ap;
-    //      z = M^-1 r; the record [z | p] for the next S; (r, z), ||r||^2
+    //      z = M^-1 r for the next S; (r, z), ||r||^2
     // Partial tables [2K][blocks]: tS = (p.Ap, r.z) from S, tU = (r.z, r.r)
     // from U (each is read in the phase after the barrier that follows its
     // writes, and written again only after the next barrier).
@@ -669,8 +666,8 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
       double pl[4];
       const bool item0 = !b0 && warp < items;
       if (item0) load_item(tU, warp, pl);
-      T accq[QR][2 * K];
-      gather_rows<T, 2 * K, UC, QR>(rrq, okq, rcur, accq);
+      T accq[QR][K];
+      gather_rows<T, K, UP, QR>(rrq, okq, rcur, accq);
       if (item0) reduce_item(warp, pl);
       if (!b0)
         for (int item = warp + nw; item < items; item += nw) {
@@ -693,7 +690,7 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
             }
             if (!(rzn == rzn) || !(rr == rr)) bad = 1;
             if (act && rr < s->stop[c]) act = 0;
-            be = s->gprev[c] == 0.0 ? 0.0 : rzn / s->gprev[c];
+            be = s->gprev[c] == 0.0 ? 0.0 : (double)((T)rzn / (T)s->gprev[c]);
           }
           s->beta[c] = act ? be : 0.0;
           s->act[c] = act;
@@ -711,15 +708,16 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
         T d2[2 * K];
 #pragma unroll
         for (int c = 0; c < 2 * K; ++c) d2[c] = (T)0;
-        auto form_p = [&](const OwnRef<T, K>& o, const T (&acc)[2 * K]) {
+        auto form_p = [&](const OwnRef<T, K>& o, const T (&acc)[K]) {
 #pragma unroll
           for (int c = 0; c < K; ++c) {
             const T z = o(kQz, c);
             const T po = b0 ? (T)0 : o(kQp, c);
+            const T apo = b0 ? (T)0 : o(kQw, c);
             const T p = z + beta[c] * po;
-            const T ap = acc[c] + beta[c] * acc[K + c];
+            const T ap = acc[c] + beta[c] * apo;  // A p = A z + beta A p'
             o(kQp, c) = p;
-            o(kQw, c) = ap;  // A p, kept for phase U
+            o(kQw, c) = ap;  // A p, for phase U and the next recurrence
             d2[c] += p * ap;
             d2[K + c] += o(kQr, c) * z;
           }
@@ -732,8 +730,8 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
           if (row >= n) break;
           RowRef<T> r1[1] = {row_ref(q, row)};
           const bool ok1[1] = {true};
-          T acc1[1][2 * K];
-          gather_rows<T, 2 * K, UC, 1>(r1, ok1, rcur, acc1);
+          T acc1[1][K];
+          gather_rows<T, K, UP, 1>(r1, ok1, rcur, acc1);
           form_p(own_ref(q, row), acc1[0]);
         }
         block_reduce_strided<2 * K, T>(d2, s->red2, tS + team.rank(), tsize);
@@ -757,7 +755,7 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
         // SparseLinAlg.lean:118 stops on pAp == 0; a non-positive value ends
         // this column's inner solve (the next FP64 residual decides)
         if (act && !(pap > 0.0)) act = 0;
-        s->alpha[c] = act ? rz / pap : 0.0;
+        s->alpha[c] = act ? (double)((T)rz / (T)pap) : 0.0;
         s->gprev[c] = rz;
         s->act[c] = act;
       }
@@ -774,7 +772,7 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
           if (row >= n) break;
           const OwnRef<T, K> o = own_ref(q, row);
           const T mi = o(kQminv, 0);
-          T rec[2 * K];
+          T rec[K];
 #pragma unroll
           for (int c = 0; c < K; ++c) {
             const T p = o(kQp, c);
@@ -784,11 +782,10 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
             o(kQr, c) = r;
             o(kQz, c) = z;
             rec[c] = z;
-            rec[K + c] = p;
             d2[c] += r * z;
             d2[K + c] += r * r;
           }
-          store_m<T, 2 * K>(rnext, row, rec);
+          store_m<T, K>(rnext, row, rec);
         }
         block_reduce_strided<2 * K, T>(d2, s->red2, tU + team.rank(), tsize);
       }
