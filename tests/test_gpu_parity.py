@@ -211,24 +211,25 @@ def test_max_iter_reported():
     assert r.status == L.CN_MAX_ITER
 
 
-def test_autotuner_picks_a_shape_that_solves(oracle, tmp_path):
+@pytest.mark.parametrize("precond", ["ic0", "jacobi"])
+def test_autotuner_picks_a_shape_that_solves(precond, oracle, tmp_path):
     import torch
 
     from tool_godot_curvenet_b200 import tune
     pos, tris, h, t = workload("torus_mid")
     ref = oracle.System(pos, tris, h)
     st, xo, _, _ = ref.solve(t, mode=1, tol=1e-13)
-    with CutMeshSolver(pos, tris, h) as s:
+    with CutMeshSolver(pos, tris, h, precond=precond) as s:
         d_t = torch.from_numpy(np.ascontiguousarray(t)).cuda()
-        best, table = tune.autotune(s, d_t.data_ptr(), 3, "ic0", reps=1, cache=str(tmp_path / "c.json"),
+        best, table = tune.autotune(s, d_t.data_ptr(), 3, precond, reps=1, cache=str(tmp_path / "c.json"),
                                     mode="deform", precision="mixed", tol=1e-8)
         assert len(table) >= 12 and best["ms"] == min(r["ms"] for r in table)
         i = s.info()
         assert (i["lanes"], i["block"]) == (best["lanes"], best["block"])
-        r = s.solve(t, mode="deform", precision="fp64", tol=1e-13)
+        r = s.solve(t, mode="deform", precision="fp64", tol=1e-13, max_iter=20000)
         assert rel_err(r.x, xo) <= FP64_TOL
-        with CutMeshSolver(pos, tris, h) as s2:
-            assert tune.apply_cached(s2, cache=str(tmp_path / "c.json")) == best
+        with CutMeshSolver(pos, tris, h, precond=precond) as s2:
+            assert tune.apply_cached(s2, precond=precond, cache=str(tmp_path / "c.json")) == best
 
 
 @pytest.mark.parametrize("k", [1, 3, 9])

@@ -53,6 +53,7 @@ struct cn_system {
   int pipe_grid = -1, pipe_block = -1, pipe_prec = -1, pipe_k = -1;
   size_t pipe_cache = 0, pipe_full = 0;
   int max_grid_alloc = 0;
+  bool shape_set = false;   // cn_set_launch fixed the launch shape
   bool have_solution = false;
   // HSC preconditioner tables (own allocations)
   bool hsc = false;
@@ -499,14 +500,16 @@ cn_status cn_solve_device(cn_handle S, int32_t k, const double* d_targets, doubl
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, S->device);
     // the grid: every SM, or fewer blocks of at least 256 rows for a small mesh
-    int grid = S->opts.grid > 0 ? S->opts.grid : std::min(sms, std::max(1, (S->H.n + 255) / 256));
+    int grid = S->shape_set ? S->grid
+             : S->opts.grid > 0 ? S->opts.grid : std::min(sms, std::max(1, (S->H.n + 255) / 256));
     int block = S->block, qr = 1;
     a.cache_bytes = 0;
     if (grid > 1) {
       grid = std::min(grid, S->max_grid_alloc);
       // two rows per thread, gathered together: block = n / (2 grid) rounded
       // up to a warp (an explicit block above 512 runs one row per thread)
-      if (S->opts.block <= 0) block = std::min(512, std::max(128, ((S->H.n + 2 * grid - 1) / (2 * grid) + 31) / 32 * 32));
+      if (!S->shape_set && S->opts.block <= 0)
+        block = std::min(512, std::max(128, ((S->H.n + 2 * grid - 1) / (2 * grid) + 31) / 32 * 32));
       qr = block <= 512 ? 2 : 1;
       const size_t cap = 220 * 1024;
       int level = 2;  // 2: row cache and own state in shared memory, 1: row cache only, 0: none
@@ -905,7 +908,8 @@ cn_status cn_set_launch(cn_handle S, int32_t lanes, int32_t block, int32_t grid)
     set_err("bad launch shape (lanes %d, block %d, grid %d)", lanes, block, grid);
     return CN_BAD_INPUT;
   }
-  if (grid > 1) {
+  const bool row_cached = !S->hsc && S->opts.precond == CN_PRECOND_JACOBI;  // clamps its grid per solve
+  if (grid > 1 && !row_cached) {
     const int mg = std::min(cn::persistent_max_grid(CN_PREC_MIXED, S->kmax, lanes, block),
                             cn::persistent_max_grid(CN_PREC_FP64, S->kmax, lanes, block));
     if (mg < 1) {
@@ -914,9 +918,11 @@ cn_status cn_set_launch(cn_handle S, int32_t lanes, int32_t block, int32_t grid)
     }
     grid = std::min(grid, std::min(mg, S->max_grid_alloc));
   }
+  if (row_cached) grid = std::min(grid, S->max_grid_alloc);
   S->lanes = lanes;
   S->block = block;
   S->grid = grid;
+  S->shape_set = true;
   return CN_OK;
 }
 
@@ -935,14 +941,26 @@ cn_status cn_autotune(cn_handle S, int32_t k, const double* d_targets, const cn_
   struct Cand { int lanes, block, grid; };
   std::vector<Cand> cands;
   const int lane_set[] = {1, 2, 4, 8};
-  if (S->H.n <= 65536)
-    for (int l : lane_set)
-      for (int b : {256, 512, 1024}) cands.push_back({l, b, 1});
-  if (S->H.n > 4096)
-    for (int l : lane_set)
-      for (int b : {256, 512, 1024})
-        for (int g : {sms / 2, sms, 2 * sms}) cands.push_back({l, b, g});
+  if (!S->hsc && S->opts.precond == CN_PRECOND_JACOBI) {
+    // the row-cached kernel: one lane per row; blocks of up to 512 threads
+    // take two rows per thread, larger ones one
+    for (int g : {sms / 2, (3 * sms) / 4, sms}) {
+      const int fit = std::min(512, std::max(128, ((S->H.n + 2 * g - 1) / (2 * g) + 31) / 32 * 32));
+      cands.push_back({1, fit, g});
+      for (int b : {256, 384, 512, 768, 1024})
+        if (b != fit) cands.push_back({1, b, g});
+    }
+  } else {
+    if (S->H.n <= 65536)
+      for (int l : lane_set)
+        for (int b : {256, 512, 1024}) cands.push_back({l, b, 1});
+    if (S->H.n > 4096)
+      for (int l : lane_set)
+        for (int b : {256, 512, 1024})
+          for (int g : {sms / 2, sms, 2 * sms}) cands.push_back({l, b, g});
+  }
   const int old_l = S->lanes, old_b = S->block, old_g = S->grid;
+  const bool old_set = S->shape_set;
   cn_solve_opts o;
   if (opts) o = *opts;
   else cn_default_solve_opts(&o);
@@ -977,6 +995,7 @@ cn_status cn_autotune(cn_handle S, int32_t k, const double* d_targets, const cn_
   if (nr == 0) {
     set_err("no launch shape ran");
     cn_set_launch(S, old_l, old_b, old_g);
+    S->shape_set = old_set;
     return CN_CUDA_ERROR;
   }
   return CN_OK;
