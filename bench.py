@@ -309,6 +309,58 @@ def batch_section(torch, dist, world, rank, local, steps, warmup):
     }
 
 
+def spmv_section(torch, local, peak, steps=20):
+    """SpMV / SpMM HBM bandwidth (the metric's second figure): y = A x on the
+    reduced matrix of the torus 1024 x 1024 workload (1.05M rows, 7.3M
+    nonzeros), FP32 and FP64, k = 3 and 24 columns.  The matrix and vectors
+    exceed L2 (126 MB) for k = 24, and L2 is flushed before every timed call.
+    Algorithmic bytes per call: nnz (s_v + 4) + 4 (n + 1) + 2 n k s_x (A once,
+    x once, y once)."""
+    from tool_godot_curvenet_b200 import CutMeshSolver, cut_mesh, synth
+    m, h, t = synth.config5()
+    tris, parent = cut_mesh(m.positions.shape[0], m.tris, m.loops)
+    pos = np.ascontiguousarray(m.positions[parent])
+    out = {"workload": "torus1024x1024_16seams_1pct_handles reduced matrix",
+           "l2": "flushed (256 MB read) before every call"}
+    with CutMeshSolver(pos, tris, h, device=local, precond="jacobi") as s:
+        info = s.info()
+        n, nnz = info["n_free"], info["nnz_A"]
+        out.update(n_rows=n, nnz=nnz)
+        stream = torch.cuda.ExternalStream(s.stream(), device=local)
+        # the L2 flush reads a 256 MB buffer: a flush by writing would leave
+        # dirty lines whose write-back would be charged to the timed call
+        flush = torch.ones(64 << 20, dtype=torch.float32, device=f"cuda:{local}")
+        for prec, k in [("mixed", 24), ("mixed", 3), ("fp64", 24), ("fp64", 3)]:
+            dt = torch.float32 if prec == "mixed" else torch.float64
+            sx = 4 if prec == "mixed" else 8
+            x = torch.randn((n, k), dtype=dt, device=f"cuda:{local}")
+            y = torch.empty_like(x)
+            with torch.cuda.stream(stream):
+                for _ in range(3):
+                    s.spmv_device(k, x.data_ptr(), y.data_ptr(), precision=prec)
+                ms = []
+                for _ in range(steps):
+                    flush.sum()
+                    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    a.record(stream)
+                    s.spmv_device(k, x.data_ptr(), y.data_ptr(), precision=prec)
+                    b.record(stream)
+                    b.synchronize()
+                    ms.append(a.elapsed_time(b))
+            med = statistics.median(ms)
+            byts = nnz * (sx + 4) + 4 * (n + 1) + 2 * n * k * sx
+            gbs = byts / (med * 1e-3) / 1e9
+            out[f"{prec}_k{k}"] = {"ms": med, "algorithmic_bytes": byts, "achieved_gbs": gbs, "peak_gbs": peak,
+                                   "frac": gbs / peak}
+        try:
+            with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+                out["mixed_k24"]["traffic"] = json.load(f)["cn_spmm_fp32_k24_torus1024"]["dram_bytes_per_launch"]
+        except Exception:
+            pass
+            del x, y
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -317,6 +369,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-spmv", action="store_true")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -443,6 +496,9 @@ def main():
         traffic = tj.get("cn_pipe_solve_mixed", {}).get("dram_bytes_per_launch")
     except Exception:
         pass
+    spmv = None
+    if not args.no_spmv and rank == 0:
+        spmv = spmv_section(torch, local, peak)
     batch = None
     if not args.no_batch:
         solver.close()
@@ -495,6 +551,8 @@ def main():
         }
         if batch is not None:
             line["batch"] = batch
+        if spmv is not None:
+            line["spmv"] = spmv
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(pos, tris, h, t)
         print(json.dumps(line), flush=True)

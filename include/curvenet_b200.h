@@ -167,6 +167,14 @@ cn_status cn_export_k(cn_handle h, int32_t* rowptr, int32_t* colidx, double* val
 cn_status cn_solve_deformation(cn_handle h, const double* Fc, const double* Xc, double* x_out,
                                const cn_solve_opts* opts, cn_solve_stats* stats);
 
+/* y = A x on the handle's reduced matrix A in solve order (the rows of
+ * cn_export_csr), on the handle's stream (cn_stream): the SpMV / SpMM of
+ * SparseLinAlg.lean:44-60 with the multi-RHS layout of
+ * SlangCodegen/SpmvMulti.lean:78-119.  precision CN_PREC_MIXED: FP32 values
+ * and vectors; CN_PREC_FP64: FP64.  k in {1, 3, 9, 24}; d_x, d_y: device
+ * pointers, [n_free][k] row-major, 16-byte aligned. */
+cn_status cn_spmv_device(cn_handle h, int32_t k, int32_t precision, const void* d_x, void* d_y);
+
 /* Launch shape of the persistent solve: lanes per row (1, 2, 4, 8, 16),
  * threads per block, blocks (1 = one block, __syncthreads barriers; more =
  * cooperative grid, clamped to the co-resident maximum). */

@@ -290,3 +290,36 @@ def test_jacobi_mixed_converges_where_fp32_pipelining_drifts(mesh, oracle):
     assert rm.status == 0 and rd.status == 0
     assert rel_err(rm.x, xo) <= MIXED_TOL
     assert rel_err(rd.x, xo) <= 1e-8
+
+
+@pytest.mark.parametrize("k", [1, 3, 9, 24])
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_spmv_matches_csr(k, precision):
+    """cn_spmv_device against the exported matrix applied on the host."""
+    import scipy.sparse as sp
+    import torch
+    pos, tris, h, _ = workload("torus_small")
+    with CutMeshSolver(pos, tris, h, precond="jacobi") as s:
+        free_of, ptr, col, val = s.export_csr()
+        n = ptr.size - 1
+        A = sp.csr_matrix((val, col, ptr), shape=(n, n))
+        x = np.random.default_rng(k).normal(size=(n, k))
+        dt = torch.float32 if precision == "mixed" else torch.float64
+        d_x = torch.from_numpy(x).to(dt).cuda()
+        d_y = torch.empty((n, k), dtype=dt, device="cuda")
+        s.spmv_device(k, d_x.data_ptr(), d_y.data_ptr(), precision=precision)
+        torch.cuda.synchronize()
+        y = d_y.double().cpu().numpy()
+    want = A @ x.astype(np.float32).astype(np.float64) if precision == "mixed" else A @ x
+    assert rel_err(y, want) <= (2e-6 if precision == "mixed" else 1e-14)
+
+
+def test_spmv_rejects_bad_arguments():
+    pos, tris, h, _ = workload("cyl_tiny")
+    with CutMeshSolver(pos, tris, h) as s:
+        with pytest.raises(CnError) as e:
+            s.spmv_device(5, 256, 256)
+        assert e.value.status == L.CN_BAD_INPUT
+        with pytest.raises(CnError) as e:
+            s.spmv_device(3, 260, 256)  # misaligned
+        assert e.value.status == L.CN_BAD_INPUT

@@ -902,6 +902,27 @@ cn_status cn_solve_deformation(cn_handle S, const double* Fc, const double* Xc, 
   return st;
 }
 
+// SpMV / SpMM on the handle's reduced matrix (SparseLinAlg.lean:44-60,
+// SlangCodegen/SpmvMulti.lean:78-119), on the handle's stream.
+cn_status cn_spmv_device(cn_handle S, int32_t k, int32_t precision, const void* d_x, void* d_y) {
+  if (!S || !d_x || !d_y) {
+    set_err("null argument");
+    return CN_BAD_INPUT;
+  }
+  if ((k != 1 && k != 3 && k != 9 && k != 24) || (precision != CN_PREC_MIXED && precision != CN_PREC_FP64)) {
+    set_err("cn_spmv_device: k must be 1, 3, 9 or 24 and precision CN_PREC_MIXED or CN_PREC_FP64");
+    return CN_BAD_INPUT;
+  }
+  if (((uintptr_t)d_x | (uintptr_t)d_y) & 15) {
+    set_err("cn_spmv_device: x and y must be 16-byte aligned");
+    return CN_BAD_INPUT;
+  }
+  CN_CUDA(cudaSetDevice(S->device));
+  const void* val = precision == CN_PREC_MIXED ? (const void*)S->D.A32 : (const void*)S->D.A64;
+  CN_CUDA(cn::launch_spmm(S->H.n, k, precision, S->D.A_ptr, S->D.A_col, val, d_x, d_y, S->stream));
+  return CN_OK;
+}
+
 cn_status cn_set_launch(cn_handle S, int32_t lanes, int32_t block, int32_t grid) {
   if (!S || (lanes != 1 && lanes != 2 && lanes != 4 && lanes != 8 && lanes != 16) || block < 64 ||
       block > 1024 || block % 32 != 0 || grid < 1) {

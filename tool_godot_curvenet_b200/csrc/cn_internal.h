@@ -119,6 +119,11 @@ cudaError_t launch_persistent_solve(const SolveArgs& a, int precision, int K, in
 // Largest co-resident grid of the persistent solve for this configuration.
 int persistent_max_grid(int precision, int K, int lanes, int block);
 
+// y = A x on a CSR matrix (cn_spmv.cu); k in {1, 3, 9, 24}, x and y
+// [n][k] in T = float (CN_PREC_MIXED) or double, 16-byte aligned.
+cudaError_t launch_spmm(int n, int k, int precision, const int* ptr, const int* col, const void* val,
+                        const void* x, void* y, cudaStream_t s);
+
 // The row-cached Jacobi-PCG persistent solve (cn_pipe.cu).  a.cache_bytes of
 // dynamic shared memory hold each block's rows of A and their CG state.
 // qr: rows per thread gathered together (1: up to 1024 threads per block,

@@ -217,6 +217,14 @@ class CutMeshSolver:
             raise CnError(st, "cn_solve_deformation")
         return SolveResult(x, stats)
 
+    def spmv_device(self, k, d_x, d_y, precision="mixed"):
+        """y = A x on the reduced matrix in solve order (device pointers,
+        [n_free][k], FP32 for "mixed", FP64 for "fp64"), on the handle's
+        stream."""
+        st = L.lib().cn_spmv_device(self._h, k, _PREC[precision], C.c_void_p(d_x), C.c_void_p(d_y))
+        if st != L.CN_OK:
+            raise CnError(st, "cn_spmv_device")
+
     def solve_device(self, k, d_targets, d_x_out, stats=True, **kw):
         """Device-pointer solve on the handle's stream (ints are device addresses)."""
         o = self.make_opts(**kw)
