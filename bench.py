@@ -242,12 +242,13 @@ def batch_section(torch, dist, world, rank, local, steps, warmup):
     specs = [synth.config3_mesh(i) for i in range(n_meshes)]
     costs = [mesh_cost(m.positions.shape[0] + sum(len(l) for l in m.loops), m.tris.shape[0]) for m, _, _ in specs]
     mine = rank_share(costs, world, rank)
-    meshes, targets = [], []
+    meshes, targets, sizes = [], [], []
     for i in mine:
         m, h, t = specs[i]
         tris, parent = cut_mesh(m.positions.shape[0], m.tris, m.loops)
         meshes.append((np.ascontiguousarray(m.positions[parent]), tris, h))
         targets.append(t)
+        sizes.append(reduced_sizes(parent.size, tris, h))
     t0 = time.perf_counter()
     B = BatchSolver(meshes, k=24, device=local)
     build_s = time.perf_counter() - t0
@@ -290,6 +291,17 @@ def batch_section(torch, dist, world, rank, local, steps, warmup):
     ms_m = reduce_over_ranks(dist, world, sum(tm) / len(tm), "max", dev)
     ms_f = reduce_over_ranks(dist, world, sum(tf) / len(tf), "max", dev)
     solves = n_meshes * 8  # (mesh, pose) solves of 3 RHS each, over all ranks
+    # algorithmic bytes of the inner IC(0)-PCG iterations (k = 24, FP32), per
+    # mesh from its own iteration count; the FP64 residual evaluations are
+    # left out, so this is a lower bound
+    kb = 24
+    inner = 0
+    for (n_m, nnz_m, nnzl_m), it_m in zip(sizes, its):
+        b_spmv = nnz_m * 8 + 4 * (n_m + 1) + 2 * n_m * kb * 4
+        b_ic = 2 * ((nnzl_m + n_m) * 8 + 4 * (n_m + 1) + 2 * n_m * kb * 4)
+        inner += int(it_m) * (b_spmv + b_ic + 9 * n_m * kb * 4)
+    inner = reduce_over_ranks(dist, world, float(inner), "sum", dev)
+    peak_b, _ = load_peaks()
     # algorithmic bytes of the batch (mixed): per mesh iterations x B_iter + residuals
     nnz = info["nnz_A"]
     n = info["n_free"]
@@ -304,9 +316,26 @@ def batch_section(torch, dist, world, rank, local, steps, warmup):
         "fp64_fused": {"solves_per_s": solves / (ms_f * 1e-3), "ms_per_batch": ms_f,
                        "max_rel_residual": st_fp64.max_rel_residual, "failed": st_fp64.n_failed},
         "speedup_mixed_vs_fp64_fused": ms_f / ms_m,
+        "roofline_mixed": {"bound": "hbm", "algorithmic_bytes_inner": inner,
+                           "achieved": inner / (ms_m * 1e-3) / 1e9, "peak": peak_b, "unit": "GB/s",
+                           "frac": inner / (ms_m * 1e-3) / 1e9 / peak_b,
+                           "note": "inner-iteration bytes only (SpMV + IC(0) sweeps + 9 vector passes per iteration)"},
         "build_s": build_s,
         "graph": "one cudaGraphLaunch (memset of the work counter + the persistent cluster kernel) per batch",
     }
+
+
+def reduced_sizes(nv, tris, handles):
+    """(n free rows, nnz of A, strictly-lower nnz of A) of a cut mesh: A has
+    the diagonal and one entry per direction of every free-free mesh edge."""
+    t = np.asarray(tris, dtype=np.int64).reshape(-1, 3)
+    e = np.concatenate([t[:, [0, 1]], t[:, [1, 2]], t[:, [2, 0]]])
+    e = np.unique(np.sort(e, axis=1), axis=0)
+    free = np.ones(nv, bool)
+    free[np.asarray(handles)] = False
+    ef = int(np.count_nonzero(free[e[:, 0]] & free[e[:, 1]]))
+    n = int(free.sum())
+    return n, n + 2 * ef, ef
 
 
 def spmv_section(torch, local, peak, steps=20):
@@ -361,6 +390,50 @@ def spmv_section(torch, local, peak, steps=20):
     return out
 
 
+def ddm_section(torch, local):
+    """Direct Delta Mush on the torus 512 x 256 mesh: the bind (influences of
+    every handle from its unit-target harmonic solve, nu = 2 smoothing
+    passes, top 8, FP64 solves to 1e-10) and the runtime LBS matvec (FP32,
+    one thread per vertex) timed with CUDA events."""
+    from tool_godot_curvenet_b200 import CutMeshSolver, cut_mesh, lbs_matvec_device, synth
+    m, h, t = synth.config2()
+    tris, parent = cut_mesh(m.positions.shape[0], m.tris, m.loops)
+    pos = np.ascontiguousarray(m.positions[parent])
+    with CutMeshSolver(pos, tris, h, device=local, precond="jacobi", max_rhs=9) as s:
+        t0 = time.perf_counter()
+        idx, w = s.ddm_bind(nu=2, omega=0.5, top_k=8, precision="fp64", tol=1e-10)
+        bind_s = time.perf_counter() - t0
+    nv, take = idx.shape
+    dev = f"cuda:{local}"
+    rng = np.random.default_rng(0)
+    T = np.tile(np.eye(4), (h.size, 1, 1))
+    T[:, :3, :] += 0.05 * rng.normal(size=(h.size, 3, 4))
+    d_rest = torch.from_numpy(pos).float().to(dev)
+    d_T = torch.from_numpy(T.reshape(-1, 16)).float().to(dev)
+    d_start = torch.from_numpy(np.arange(nv + 1, dtype=np.int32) * take).to(dev)
+    d_idx = torch.from_numpy(idx.reshape(-1)).to(dev)
+    d_w = torch.from_numpy(w.reshape(-1)).float().to(dev)
+    d_out = torch.empty_like(d_rest)
+    st = torch.cuda.current_stream(local)
+
+    def run():
+        lbs_matvec_device(nv, d_rest.data_ptr(), d_T.data_ptr(), d_start.data_ptr(), d_idx.data_ptr(), d_w.data_ptr(),
+                          d_out.data_ptr(), precision="mixed", stream=st.cuda_stream)
+    for _ in range(5):
+        run()
+    ms = []
+    for _ in range(50):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        run()
+        b.record(st)
+        b.synchronize()
+        ms.append(a.elapsed_time(b))
+    return {"workload": "torus512x256 cut mesh, all handles", "n_verts": nv, "n_handles": int(h.size),
+            "top_k": take, "bind_s": bind_s, "bind_solves": int((h.size + 8) // 9),
+            "runtime_lbs_us": 1e3 * statistics.median(ms), "runtime_precision": "fp32"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -370,6 +443,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-spmv", action="store_true")
+    ap.add_argument("--no-ddm", action="store_true")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -401,7 +475,9 @@ def main():
     nv, k = pos.shape[0], 3
     d_t = torch.from_numpy(t).to(f"cuda:{local}")
     d_x = torch.empty((nv, k), dtype=torch.float64, device=f"cuda:{local}")
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")  # > L2 (126 MB)
+    # L2 flush between timed solves: a 256 MB read (> L2's 126 MB; a read
+    # leaves no dirty lines whose write-back the next timed solve would pay)
+    flush = torch.ones(64 << 20, dtype=torch.float32, device=f"cuda:{local}")
 
     def one(precision, algo="fused", stats=False, sv=None):
         return (sv or solver).solve_device(k, d_t.data_ptr(), d_x.data_ptr(), stats=stats, mode="deform",
@@ -428,7 +504,7 @@ def main():
             torch.cuda.synchronize()
             st_ = torch.cuda.current_stream()
             for a, b in evs:
-                flush.fill_(1)  # L2 flush between timed solves (outside the events)
+                flush.sum()  # L2 flush between timed solves (outside the events)
                 a.record(st_)
                 one(precision, algo, sv=sv)
                 b.record(st_)
@@ -464,7 +540,7 @@ def main():
     e2e_ms = []
     with torch.cuda.stream(stream):
         for _ in range(args.steps):
-            flush.fill_(1)
+            flush.sum()
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record(stream)
             rc = e2e_one()
@@ -499,6 +575,9 @@ def main():
     spmv = None
     if not args.no_spmv and rank == 0:
         spmv = spmv_section(torch, local, peak)
+    ddm = None
+    if not args.no_ddm and rank == 0:
+        ddm = ddm_section(torch, local)
     batch = None
     if not args.no_batch:
         solver.close()
@@ -522,7 +601,7 @@ def main():
             "config": {"workload": WORKLOAD, "n_verts": nv, "n_free": info["n_free"], "nnz_A": info["nnz_A"],
                        "rhs": k, "tol": 1e-8, "precond": "Jacobi, natural row order; two-reduction CG on the row-cached kernel (rows of A and the CG state in shared memory)",
                        "launch": f"grid {info['grid']} x block auto (2 rows per thread)", "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
-                       "l2": "flushed (256 MB write) before every timed solve, outside the events"},
+                       "l2": "flushed (256 MB read) before every timed solve, outside the events"},
             "mixed": {"iterations": st_mixed.iterations, "refinements": st_mixed.refinements,
                       "max_rel_residual": st_mixed.max_rel_residual},
             "fp64_fused": {"solves_per_s": 1e3 / ms_fp64, "ms": ms_fp64, "iterations": st_fp64.iterations,
@@ -553,6 +632,8 @@ def main():
             line["batch"] = batch
         if spmv is not None:
             line["spmv"] = spmv
+        if ddm is not None:
+            line["ddm"] = ddm
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(pos, tris, h, t)
         print(json.dumps(line), flush=True)

@@ -175,6 +175,28 @@ cn_status cn_solve_deformation(cn_handle h, const double* Fc, const double* Xc, 
  * pointers, [n_free][k] row-major, 16-byte aligned. */
 cn_status cn_spmv_device(cn_handle h, int32_t k, int32_t precision, const void* d_x, void* d_y);
 
+/* ---------------------------------------------------------------------------
+ * Direct Delta Mush.  Bind (DirectDeltaMushBind.lean:6-40): the influence of
+ * handle i on every cut-mesh vertex is the harmonic solve with the unit
+ * target on handle i (HarmonicSolve.lean:51-66); the weights are smoothed nu
+ * times by w' = (1 - omega) w + omega * mean over the vertex's mesh
+ * neighbours (:72-94), each vertex keeps the top_k of largest |w| (ties: the
+ * lower handle index) and its kept weights are divided by their sum
+ * (:104-133).  Output rows of take = min(top_k, n_handles) entries:
+ * infl_idx / infl_w are n_verts x take (CSR start of vertex v = v * take).
+ * Needs a build with max_rhs = 9; runs n_handles / 9 solves. */
+cn_status cn_ddm_bind(cn_handle h, int32_t nu, double omega, int32_t top_k, const cn_solve_opts* opts,
+                      int32_t* infl_idx, double* infl_w);
+/* Runtime DDM (DirectDeltaMush.lean:84-102 lbsMatvec; the buffers of
+ * SlangCodegen/DirectDeltaMush.lean:11-22): out[v] = sum over v's
+ * influences of w * (T_i (rest[v], 1)).  Device pointers: rest and out
+ * n_verts x 3, transforms n_handles x 16 (row-major 4x4), start n_verts + 1,
+ * idx / w per influence; FP32 (CN_PREC_MIXED) or FP64; stream: a
+ * cudaStream_t (NULL: the default stream). */
+cn_status cn_lbs_matvec_device(int32_t n_verts, int32_t precision, const void* d_rest, const void* d_transforms,
+                               const int32_t* d_start, const int32_t* d_idx, const void* d_w, void* d_out,
+                               void* stream);
+
 /* Launch shape of the persistent solve: lanes per row (1, 2, 4, 8, 16),
  * threads per block, blocks (1 = one block, __syncthreads barriers; more =
  * cooperative grid, clamped to the co-resident maximum). */

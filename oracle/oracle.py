@@ -32,6 +32,11 @@ def lib():
         L = C.CDLL(LIB_PATH)
         sig = {
             "orc_cot_at_vertex": (C.c_double, [_D, _D, _D]),
+            "orc_apply_transform4x4": (None, [_D, C.c_double, C.c_double, C.c_double, _D]),
+            "orc_lbs_matvec": (None, [_D, C.c_int, _I, _D, C.c_double, C.c_double, C.c_double, _D]),
+            "orc_lbs_matvec_csr": (None, [C.c_int, _D, _D, _I, _I, _D, _D]),
+            "orc_smooth_weights": (None, [C.c_int, C.c_int, _D, _I, _I, C.c_int, C.c_double, _D]),
+            "orc_sparsify_topk": (None, [C.c_int, C.c_int, _D, C.c_int, _I, _D]),
             "orc_triangle_cot_laplacian": (None, [_D, _D, _D, _D]),
             "orc_polygon_cot_laplacian": (None, [C.c_int, _D, _D]),
             "orc_edge_lengths": (None, [_D, _D, _D, _D]),
@@ -349,3 +354,46 @@ class System:
         st = lib().orc_system_solve(self._h, k, dp(t), mode, tol, max_iter, threads,
                                     dp(f64(x0)) if x0 is not None else None, dp(x), ip(it), dp(rel))
         return st, x, it, rel
+
+
+# --------------------------------------------------------------------- Direct Delta Mush
+def lbs_matvec(transforms, infl, rest):
+    """DirectDeltaMush.lean:84-102 for one vertex; infl = [(handle, w), ...]."""
+    T = f64(transforms).reshape(-1, 16)
+    idx = i32([i for i, _ in infl]) if infl else np.zeros(1, np.int32)
+    w = f64([x for _, x in infl]) if infl else np.zeros(1)
+    out = np.empty(3)
+    lib().orc_lbs_matvec(dp(T), len(infl), ip(idx), dp(w), float(rest[0]), float(rest[1]), float(rest[2]), dp(out))
+    return out
+
+
+def lbs_matvec_csr(rest, transforms, start, idx, w):
+    rest = f64(rest).reshape(-1, 3)
+    out = np.empty_like(rest)
+    lib().orc_lbs_matvec_csr(rest.shape[0], dp(rest), dp(f64(transforms).reshape(-1, 16)), ip(i32(start)),
+                             ip(i32(idx)), dp(f64(w)), dp(out))
+    return out
+
+
+def smooth_weights(W, adj, nu, omega):
+    """DirectDeltaMushBind.lean:72-94; adj = list of neighbour lists."""
+    W = f64(W)
+    n, nh = W.shape
+    ptr = np.zeros(n + 1, np.int32)
+    for v, nb in enumerate(adj):
+        ptr[v + 1] = ptr[v] + len(nb)
+    idx = i32([u for nb in adj for u in nb]) if ptr[-1] else np.zeros(1, np.int32)
+    out = np.empty_like(W)
+    lib().orc_smooth_weights(n, nh, dp(W), ip(ptr), ip(idx), nu, omega, dp(out))
+    return out
+
+
+def sparsify_topk(W, K):
+    """DirectDeltaMushBind.lean:104-133: (idx, w) arrays of n x min(K, nh)."""
+    W = f64(W)
+    n, nh = W.shape
+    take = min(K, nh)
+    idx = np.empty((n, max(take, 1)), np.int32)
+    w = np.empty((n, max(take, 1)))
+    lib().orc_sparsify_topk(n, nh, dp(W), K, ip(idx), dp(w))
+    return idx[:, :take], w[:, :take]

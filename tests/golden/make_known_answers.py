@@ -205,6 +205,46 @@ def main():
         rec("EndToEndExample.lean:202-211", "curve_deform", P_rest=prest, P_posed=prot, t=0.5, t_fwd=0.6,
             rows={"1": [0.0, 1.0, 0.0], "2": [0.0, 0.5, 0.8660254037844386]}, eps=1e-9, **tws),
     ]
+    # ---------------------------------------------------------------- Direct Delta Mush
+    ident = [1.0, 0.0, 0.0, 0.0, 0.0, 1.0, 0.0, 0.0, 0.0, 0.0, 1.0, 0.0, 0.0, 0.0, 0.0, 1.0]
+
+    def trans(tx, ty, tz):
+        return [1.0, 0.0, 0.0, tx, 0.0, 1.0, 0.0, ty, 0.0, 0.0, 1.0, tz, 0.0, 0.0, 0.0, 1.0]
+    out += [
+        rec("DirectDeltaMush.lean:115-120", "lbs", T=[ident], infl=[[0, 1.0]], rest=[1.5, -2.0, 0.75],
+            expected=[1.5, -2.0, 0.75], eps=1e-12),
+        rec("DirectDeltaMush.lean:122-127", "lbs", T=[trans(2.0, -3.0, 1.0)], infl=[[0, 1.0]], rest=[1.0, 1.0, 1.0],
+            expected=[3.0, -2.0, 2.0], eps=1e-12),
+        rec("DirectDeltaMush.lean:129-134", "lbs", T=[ident, ident], infl=[[0, 0.5], [1, 0.5]], rest=[4.0, -1.0, 2.0],
+            expected=[4.0, -1.0, 2.0], eps=1e-12),
+        rec("DirectDeltaMush.lean:136-145", "lbs", T=[trans(1.0, 0.0, 0.0), trans(-1.0, 0.0, 0.0)],
+            infl=[[0, 0.7], [1, 0.3]], rest=[0.0, 0.0, 0.0], expected=[0.4, 0.0, 0.0], eps=1e-12),
+        rec("DirectDeltaMush.lean:147-155", "lbs", T=[ident], infl=[], rest=[1.0, 1.0, 1.0],
+            expected=[0.0, 0.0, 0.0], eps=1e-12),
+        rec("DirectDeltaMush.lean:157-165", "lbs", T=[ident] * 4, infl=[[0, 0.25], [1, 0.25], [2, 0.25], [3, 0.25]],
+            rest=[7.0, 8.0, 9.0], expected=[7.0, 8.0, 9.0], eps=1e-12),
+    ]
+    path4 = [[1], [0, 2], [1, 3], [2]]
+    idW = [[1.0 if i == v else 0.0 for i in range(4)] for v in range(4)]
+    halfW = [[0.5, 0.5, 0.0, 0.0] for _ in range(4)]
+    out += [
+        rec("DirectDeltaMushBind.lean:169", "pou", W=idW, eps=1e-12),
+        rec("DirectDeltaMushBind.lean:171-175", "smooth_entries", W=idW, adj=path4, nu=0, omega=0.5,
+            entries=[[0, 0, 1.0], [1, 1, 1.0]], eps=1e-12),
+        rec("DirectDeltaMushBind.lean:188", "pou", W=halfW, eps=1e-12),
+        rec("DirectDeltaMushBind.lean:190-192", "smooth_pou", W=halfW, adj=path4, nu=5, omega=0.5, eps=1e-12),
+        rec("DirectDeltaMushBind.lean:194-197", "smooth_entries", W=halfW, adj=path4, nu=5, omega=0.5,
+            entries=[[0, 0, 0.5], [2, 1, 0.5]], eps=1e-12),
+        rec("DirectDeltaMushBind.lean:205-207", "topk_size", W=[[0.4, 0.3, 0.2, 0.1]], K=2, size=2),
+        rec("DirectDeltaMushBind.lean:209-211", "topk_rowsum", W=[[0.4, 0.3, 0.2, 0.1]], K=2, eps=1e-12),
+        rec("DirectDeltaMushBind.lean:213-216", "topk_values", W=[[0.4, 0.3, 0.2, 0.1]], K=2,
+            values=[4.0 / 7.0, 3.0 / 7.0], eps=1e-12),
+        rec("DirectDeltaMushBind.lean:218-224", "topk_rowsum", W=idW[:1], K=4, eps=1e-12),
+        rec("DirectDeltaMushBind.lean:240-245", "smooth_topk_pou", W=idW, adj=path4, nu=2, omega=0.5, K=2, eps=1e-9),
+        rec("DirectDeltaMushBind.lean:248-253", "smooth_topk_pou", W=idW, adj=path4, nu=2, omega=0.5, K=4, eps=1e-9),
+        rec("DirectDeltaMushBind.lean:257-262", "smooth_topk_pou", W=halfW, adj=path4, nu=1,
+            omega=0.3, K=1, eps=1e-9),
+    ]
     path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "known_answers.json")
     with open(path, "w") as f:
         json.dump(out, f, indent=1)

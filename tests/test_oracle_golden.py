@@ -224,6 +224,32 @@ def test_known_answer(f, oracle):
             X = O.solve_deformation(f["nv"], f["nf"], np.array(f["he"], np.int32), f["sample_col"], f["pos"], F, pp)
             for r, want in f["rows"].items():
                 assert np.all(np.abs(X[int(r)] - want) < eps)
+    elif k == "lbs":
+        got = O.lbs_matvec(f["T"], [tuple(x) for x in f["infl"]], f["rest"])
+        assert np.all(np.abs(got - f["expected"]) < eps)
+    elif k == "pou":
+        assert np.all(np.abs(np.sum(f["W"], axis=1) - 1.0) < eps)
+    elif k in ("smooth_entries", "smooth_pou"):
+        W = O.smooth_weights(f["W"], f["adj"], f["nu"], f["omega"])
+        if k == "smooth_pou":
+            assert np.all(np.abs(W.sum(axis=1) - 1.0) < eps)
+        else:
+            for v, i, want in f["entries"]:
+                assert abs(W[v, i] - want) < eps
+    elif k in ("topk_size", "topk_rowsum", "topk_values"):
+        idx, w = O.sparsify_topk(f["W"], f["K"])
+        if k == "topk_size":
+            assert idx.shape[1] == f["size"]
+        elif k == "topk_rowsum":
+            assert abs(w[0].sum() - 1.0) < eps
+        else:
+            assert np.all(np.abs(w[0] - f["values"]) < eps)
+    elif k == "smooth_topk_pou":
+        W = O.smooth_weights(f["W"], f["adj"], f["nu"], f["omega"])
+        idx, w = O.sparsify_topk(W, f["K"])
+        dense = np.zeros_like(W)
+        np.put_along_axis(dense, idx, w, axis=1)
+        assert np.all(np.abs(dense.sum(axis=1) - 1.0) < eps)
     else:
         pytest.fail(f"unknown fixture kind {k}")
 

@@ -5,4 +5,5 @@ Public surface: `cut_mesh`, `CutMeshSolver`, `solve_multi`,
 generators (tool_godot_curvenet_b200.synth) and the C ABI in
 include/curvenet_b200.h (tool_godot_curvenet_b200._lib).
 """
-from .solver import BatchSolver, CnError, CutMeshSolver, cut_mesh, solve_deformation, solve_multi  # noqa: F401
+from .solver import (BatchSolver, CnError, CutMeshSolver, cut_mesh, lbs_matvec_device,  # noqa: F401
+                     solve_deformation, solve_multi)

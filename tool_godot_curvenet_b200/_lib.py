@@ -71,6 +71,9 @@ SIGNATURES = {
     "cn_export_factor": (C.c_int, [_P, _I32P, _I32P, _DP]),
     "cn_export_k": (C.c_int, [_P, _I32P, _I32P, _DP]),
     "cn_solve_deformation": (C.c_int, [_P, _DP, _DP, _DP, C.POINTER(SolveOpts), C.POINTER(SolveStats)]),
+    "cn_ddm_bind": (C.c_int, [_P, C.c_int32, C.c_double, C.c_int32, C.POINTER(SolveOpts), _I32P, _DP]),
+    "cn_lbs_matvec_device": (C.c_int, [C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                       C.c_void_p, C.c_void_p, C.c_void_p]),
     "cn_spmv_device": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p]),
     "cn_set_launch": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32]),
     "cn_autotune": (C.c_int, [_P, C.c_int32, _P, C.POINTER(SolveOpts), C.c_int32, _DP, _I32P]),

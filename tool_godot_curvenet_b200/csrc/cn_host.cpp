@@ -902,6 +902,100 @@ cn_status cn_solve_deformation(cn_handle S, const double* Fc, const double* Xc, 
   return st;
 }
 
+// Direct Delta Mush bind (DirectDeltaMushBind.lean:6-40): W[:, i] is the
+// harmonic solve with the unit target on handle i (chunks of 9 handles as
+// one k = 9 solve), smoothed nu times over the cut-mesh adjacency, merged
+// into each vertex's top-K list and renormalised.
+cn_status cn_ddm_bind(cn_handle S, int32_t nu, double omega, int32_t top_k, const cn_solve_opts* opts,
+                      int32_t* infl_idx, double* infl_w) {
+  if (!S || !infl_idx || !infl_w) {
+    set_err("null argument");
+    return CN_BAD_INPUT;
+  }
+  if (nu < 0 || !std::isfinite(omega) || top_k < 1 || top_k > 32) {
+    set_err("cn_ddm_bind: need nu >= 0, a finite omega and 1 <= top_k <= 32");
+    return CN_BAD_INPUT;
+  }
+  if (S->kmax < 9) {
+    set_err("cn_ddm_bind needs a build with max_rhs = 9");
+    return CN_BAD_INPUT;
+  }
+  const MeshHost& H = S->H;
+  const int nv = H.nv, nh = H.nh;
+  if (nh < 1) {
+    set_err("cn_ddm_bind: the mesh has no handles");
+    return CN_BAD_INPUT;
+  }
+  const int take = std::min(top_k, nh);
+  cn_solve_opts o;
+  if (opts) o = *opts;
+  else cn_default_solve_opts(&o);
+  o.mode = CN_MODE_HARMONIC;
+  o.warm_start = 0;
+  CN_CUDA(cudaSetDevice(S->device));
+  int *d_bidx = nullptr, *d_cnt = nullptr;
+  double *d_bw = nullptr, *d_tmp = nullptr;
+  auto release = [&]() {
+    for (void* p : {(void*)d_bidx, (void*)d_cnt, (void*)d_bw, (void*)d_tmp})
+      if (p) cudaFree(p);
+  };
+  if (cudaMalloc((void**)&d_bidx, sizeof(int) * (size_t)nv * take) != cudaSuccess ||
+      cudaMalloc((void**)&d_cnt, sizeof(int) * (size_t)nv) != cudaSuccess ||
+      cudaMalloc((void**)&d_bw, sizeof(double) * (size_t)nv * take) != cudaSuccess ||
+      cudaMalloc((void**)&d_tmp, sizeof(double) * (size_t)nv * 9) != cudaSuccess) {
+    release();
+    set_err("cn_ddm_bind: device allocation failed");
+    return CN_CUDA_ERROR;
+  }
+  cn_status st = CN_OK;
+  if (cudaMemsetAsync(d_cnt, 0, sizeof(int) * (size_t)nv, S->stream) != cudaSuccess) st = CN_CUDA_ERROR;
+  for (int c0 = 0; c0 < nh && st == CN_OK; c0 += 9) {
+    const int kc = std::min(9, nh - c0);
+    if (cn::launch_ddm_unit_targets(nh, c0, kc, S->d_targets, S->stream) != cudaSuccess) { st = CN_CUDA_ERROR; break; }
+    cn_solve_stats ss;
+    st = cn_solve_device(S, 9, S->d_targets, S->d_xout, &o, &ss);
+    if (st != CN_OK) break;
+    double* cur = S->d_xout;
+    double* nxt = d_tmp;
+    for (int pass = 0; pass < nu; ++pass) {
+      if (cn::launch_ddm_smooth(nv, S->D.K_ptr, S->D.K_col, cur, nxt, omega, S->stream) != cudaSuccess) {
+        st = CN_CUDA_ERROR;
+        break;
+      }
+      std::swap(cur, nxt);
+    }
+    if (st != CN_OK) break;
+    if (cn::launch_ddm_topk(nv, c0, kc, take, cur, d_bidx, d_bw, d_cnt, S->stream) != cudaSuccess) st = CN_CUDA_ERROR;
+  }
+  if (st == CN_OK && cn::launch_ddm_finish(nv, take, d_bw, S->stream) != cudaSuccess) st = CN_CUDA_ERROR;
+  if (st == CN_OK &&
+      (cudaMemcpyAsync(infl_idx, d_bidx, sizeof(int) * (size_t)nv * take, cudaMemcpyDeviceToHost, S->stream) !=
+           cudaSuccess ||
+       cudaMemcpyAsync(infl_w, d_bw, sizeof(double) * (size_t)nv * take, cudaMemcpyDeviceToHost, S->stream) !=
+           cudaSuccess ||
+       cudaStreamSynchronize(S->stream) != cudaSuccess))
+    st = CN_CUDA_ERROR;
+  if (st == CN_CUDA_ERROR) set_err("cn_ddm_bind: %s", cudaGetErrorString(cudaGetLastError()));
+  cudaStreamSynchronize(S->stream);
+  release();
+  S->have_solution = false;
+  return st;
+}
+
+// Runtime DDM (DirectDeltaMush.lean:84-102): one thread per vertex.
+cn_status cn_lbs_matvec_device(int32_t n_verts, int32_t precision, const void* d_rest, const void* d_transforms,
+                               const int32_t* d_start, const int32_t* d_idx, const void* d_w, void* d_out,
+                               void* stream) {
+  if (n_verts < 0 || (n_verts > 0 && (!d_rest || !d_transforms || !d_start || !d_idx || !d_w || !d_out)) ||
+      (precision != CN_PREC_MIXED && precision != CN_PREC_FP64)) {
+    set_err("cn_lbs_matvec_device: bad arguments");
+    return CN_BAD_INPUT;
+  }
+  CN_CUDA(cn::launch_lbs_matvec(n_verts, precision, d_rest, d_transforms, d_start, d_idx, d_w, d_out,
+                                (cudaStream_t)stream));
+  return CN_OK;
+}
+
 // SpMV / SpMM on the handle's reduced matrix (SparseLinAlg.lean:44-60,
 // SlangCodegen/SpmvMulti.lean:78-119), on the handle's stream.
 cn_status cn_spmv_device(cn_handle S, int32_t k, int32_t precision, const void* d_x, void* d_y) {

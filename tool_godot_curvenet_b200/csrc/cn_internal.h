@@ -119,6 +119,16 @@ cudaError_t launch_persistent_solve(const SolveArgs& a, int precision, int K, in
 // Largest co-resident grid of the persistent solve for this configuration.
 int persistent_max_grid(int precision, int K, int lanes, int block);
 
+// Direct Delta Mush (cn_ddm.cu).
+cudaError_t launch_ddm_unit_targets(int nh, int c0, int kc, double* t, cudaStream_t s);
+cudaError_t launch_ddm_smooth(int nv, const int* ptr, const int* col, const double* in, double* out, double omega,
+                              cudaStream_t s);
+cudaError_t launch_ddm_topk(int nv, int c0, int kc, int K, const double* W, int* bidx, double* bw, int* cnt,
+                            cudaStream_t s);
+cudaError_t launch_ddm_finish(int nv, int take, double* bw, cudaStream_t s);
+cudaError_t launch_lbs_matvec(int nv, int precision, const void* rest, const void* tr, const int* start,
+                              const int* idx, const void* w, void* out, cudaStream_t s);
+
 // y = A x on a CSR matrix (cn_spmv.cu); k in {1, 3, 9, 24}, x and y
 // [n][k] in T = float (CN_PREC_MIXED) or double, 16-byte aligned.
 cudaError_t launch_spmm(int n, int k, int precision, const int* ptr, const int* col, const void* val,

@@ -217,6 +217,19 @@ class CutMeshSolver:
             raise CnError(st, "cn_solve_deformation")
         return SolveResult(x, stats)
 
+    def ddm_bind(self, nu=2, omega=0.5, top_k=4, **kw):
+        """Direct Delta Mush influences (DirectDeltaMushBind.lean:6-40):
+        (idx, w), each (n_verts, min(top_k, n_handles)); row v's entries are
+        vertex v's influences, largest |w| first.  Needs max_rhs=9."""
+        take = min(top_k, self.handles.size)
+        idx = np.empty((self.n_verts, take), np.int32)
+        w = np.empty((self.n_verts, take))
+        o = self.make_opts(mode="harmonic", **kw)
+        st = L.lib().cn_ddm_bind(self._h, nu, omega, top_k, C.byref(o), _ip(idx), _dp(w))
+        if st != L.CN_OK:
+            raise CnError(st, "cn_ddm_bind")
+        return idx, w
+
     def spmv_device(self, k, d_x, d_y, precision="mixed"):
         """y = A x on the reduced matrix in solve order (device pointers,
         [n_free][k], FP32 for "mixed", FP64 for "fp64"), on the handle's
@@ -350,3 +363,14 @@ class BatchSolver:
         if st != L.CN_OK:
             raise CnError(st, "cn_solve_batch_device")
         return s if stats else None
+
+
+def lbs_matvec_device(n_verts, d_rest, d_transforms, d_start, d_idx, d_w, d_out, precision="mixed", stream=0):
+    """Runtime Direct Delta Mush (DirectDeltaMush.lean:84-102) on device
+    pointers (ints): rest/out n_verts x 3, transforms n_handles x 16,
+    CSR influences start/idx/w; FP32 for "mixed", FP64 for "fp64"."""
+    st = L.lib().cn_lbs_matvec_device(n_verts, _PREC[precision], C.c_void_p(d_rest), C.c_void_p(d_transforms),
+                                      C.c_void_p(d_start), C.c_void_p(d_idx), C.c_void_p(d_w), C.c_void_p(d_out),
+                                      C.c_void_p(stream))
+    if st != L.CN_OK:
+        raise CnError(st, "cn_lbs_matvec_device")
