@@ -104,9 +104,24 @@ __global__ void __launch_bounds__(256) k_lbs_matvec(int nv, const T* __restrict_
   out[3 * (size_t)v + 2] = z;
 }
 
+__global__ void k_copy_columns(const double* src, int rows, int ks, int s0, double* dst, int kd, int d0,
+                               int ncols) {
+  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= (long long)rows * ncols) return;
+  const int r = (int)(q / ncols), c = (int)(q - (long long)r * ncols);
+  dst[(size_t)r * kd + d0 + c] = src[(size_t)r * ks + s0 + c];
+}
+
 inline unsigned blocks_for(long long n, int t) { return (unsigned)((n + t - 1) / t); }
 
 }  // namespace
+
+cudaError_t launch_copy_columns(const double* src, int rows, int ks, int s0, double* dst, int kd, int d0, int ncols,
+                                cudaStream_t s) {
+  if (rows > 0 && ncols > 0)
+    k_copy_columns<<<blocks_for((long long)rows * ncols, 256), 256, 0, s>>>(src, rows, ks, s0, dst, kd, d0, ncols);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_ddm_unit_targets(int nh, int c0, int kc, double* t, cudaStream_t s) {
   if (nh > 0) k_unit_targets<<<blocks_for((long long)nh * 9, 256), 256, 0, s>>>(nh, c0, kc, t);

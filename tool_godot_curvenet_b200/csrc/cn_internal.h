@@ -119,6 +119,10 @@ cudaError_t launch_persistent_solve(const SolveArgs& a, int precision, int K, in
 // Largest co-resident grid of the persistent solve for this configuration.
 int persistent_max_grid(int precision, int K, int lanes, int block);
 
+// dst[r * kd + d0 + c] = src[r * ks + s0 + c] for r < rows, c < ncols (cn_ddm.cu).
+cudaError_t launch_copy_columns(const double* src, int rows, int ks, int s0, double* dst, int kd, int d0, int ncols,
+                                cudaStream_t s);
+
 // Direct Delta Mush (cn_ddm.cu).
 cudaError_t launch_ddm_unit_targets(int nh, int c0, int kc, double* t, cudaStream_t s);
 cudaError_t launch_ddm_smooth(int nv, const int* ptr, const int* col, const double* in, double* out, double omega,
