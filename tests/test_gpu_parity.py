@@ -292,13 +292,16 @@ def test_jacobi_mixed_converges_where_fp32_pipelining_drifts(mesh, oracle):
     assert rel_err(rd.x, xo) <= 1e-8
 
 
+@pytest.mark.parametrize("name", ["torus_small", "c2"])
 @pytest.mark.parametrize("k", [1, 3, 9, 24])
 @pytest.mark.parametrize("precision", ["mixed", "fp64"])
-def test_spmv_matches_csr(k, precision):
-    """cn_spmv_device against the exported matrix applied on the host."""
+def test_spmv_matches_csr(name, k, precision):
+    """cn_spmv_device against the exported matrix applied on the host (the
+    larger mesh gives every block of the staged kernel several row chunks,
+    so both shared-memory buffers are used)."""
     import scipy.sparse as sp
     import torch
-    pos, tris, h, _ = workload("torus_small")
+    pos, tris, h, _ = workload(name)
     with CutMeshSolver(pos, tris, h, precond="jacobi") as s:
         free_of, ptr, col, val = s.export_csr()
         n = ptr.size - 1
