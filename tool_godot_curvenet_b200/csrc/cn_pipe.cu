@@ -25,8 +25,8 @@
 //   decision); the own rows update, store m' = M^-1 w' into the other copy
 //   of m, and the block's partial sums of (gamma', delta', ||r'||^2) are
 //   written before the next barrier.
-// Each thread owns the rows t + q * (grid * block) of its block for the whole
-// launch, and the block keeps its rows of A (column index and T value) in
+// Each thread owns the rows b Qg B + q B + t (q < Qg) of its block b for the
+// whole launch, and the block keeps its rows of A (column index and T value) in
 // shared memory (one ELL slice per row slice, column-major, padding column
 // -1), so a row costs one L2 round trip (the gathers of m) per phase.
 // Partial sums alternate between two slot groups by phase parity (a block
@@ -272,10 +272,14 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
   T* mb1 = (T*)a.m1;
   T* mb2 = (T*)a.m2;
   const int n = a.n, B = blockDim.x, t = threadIdx.x;
-  const int R = team.size() * B;
-  const int blk0 = team.rank() * B;
+  // Block b owns the contiguous rows [b Qg B, (b + 1) Qg B): thread t the
+  // rows b Qg B + q B + t, q < Qg (consecutive threads, consecutive rows;
+  // a block's rows are neighbours on the mesh in natural order)
+  const int Qg = (int)(((long long)n + (long long)team.size() * B - 1) / ((long long)team.size() * B));
+  const int R = B;
+  const int blk0 = team.rank() * Qg * B;
   const int row0 = blk0 + t;
-  const int Qb = n > blk0 ? (n - blk0 + R - 1) / R : 0;  // row slices of this block
+  const int Qb = n > blk0 ? Qg : 0;  // row slices of this block
   const int tsize = team.size();
   const int warp = t >> 5, lane = t & 31, nw = B >> 5;
   double* part = a.partials;
@@ -818,7 +822,7 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
 #pragma unroll
       for (int c = 0; c < K; ++c) a.x_out[(size_t)v * K + c] = a.x64[(size_t)row * K + c];
     }
-    for (int h = row0; h < a.nh; h += R) {
+    for (int h = team.rank() * B + t; h < a.nh; h += team.size() * B) {
       const int v = a.handles[h];
 #pragma unroll
       for (int c = 0; c < K; ++c)
@@ -916,13 +920,14 @@ int pipelined_max_grid(int precision, int K, int block, int cache_bytes, int qr)
 void pipelined_smem_need(const int* A_ptr, int n, int grid, int block, int precision, int K, size_t* cache,
                          size_t* full) {
   const size_t vs = precision == CN_PREC_MIXED ? sizeof(float) : sizeof(double);
-  const long long R = (long long)grid * block;
+  const long long Qg = ((long long)n + (long long)grid * block - 1) / ((long long)grid * block);
+  const long long R = block;
   size_t wc = 0, wf = 0;
   *cache = *full = (size_t)-1;
   for (int b = 0; b < grid; ++b) {
-    const long long blk0 = (long long)b * block;
+    const long long blk0 = (long long)b * Qg * block;
     if (blk0 >= n) break;
-    const long long Qb = (n - blk0 + R - 1) / R;
+    const long long Qb = Qg;
     if (Qb > kPipeSlices) return;
     size_t ents = 0;
     for (long long q = 0; q < Qb; ++q) {
