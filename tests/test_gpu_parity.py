@@ -326,3 +326,46 @@ def test_spmv_rejects_bad_arguments():
         with pytest.raises(CnError) as e:
             s.spmv_device(3, 260, 256)  # misaligned
         assert e.value.status == L.CN_BAD_INPUT
+
+
+@pytest.mark.parametrize("name", ["cyl_tiny", "c1", "torus_small", "c3_0"])
+@pytest.mark.parametrize("grid,block", [(0, 0), (1, 512), (6, 256)])
+@pytest.mark.parametrize("k", [1, 3, 9])
+def test_block_ssor_matches_oracle(name, grid, block, k, oracle):
+    """Block SSOR on the row-cached kernel: colour lists in shared memory
+    (several blocks), the own rows in global memory (one block, no row
+    cache); FP64 and mixed precision against the oracle's answer."""
+    pos, tris, h, _ = workload(name)
+    rng = np.random.default_rng(5 + k)
+    t = rng.normal(size=(h.size, k))
+    ref = oracle.System(pos, tris, h)
+    st, xo, _, _ = ref.solve(t, mode=0, tol=1e-13)
+    assert st == 0
+    kw = {} if grid == 0 else {"grid": grid, "block": block}
+    with CutMeshSolver(pos, tris, h, max_rhs=k, precond="bssor", **kw) as s:
+        r = s.solve(t, mode="harmonic", precision="fp64", tol=1e-13, max_iter=20000)
+        rm = s.solve(t, mode="harmonic", precision="mixed", tol=1e-8, max_iter=20000)
+    assert r.status == 0 and rm.status == 0
+    assert np.all(r.rel_residual <= 1e-13) and np.all(rm.rel_residual <= 1e-8)
+    assert rel_err(r.x, xo) <= FP64_TOL
+    assert rel_err(rm.x, xo) <= MIXED_TOL
+
+
+def test_block_ssor_takes_fewer_iterations_than_jacobi():
+    pos, tris, h, t = workload("torus_small")
+    t = t[:, :3]
+    its = {}
+    for precond in ["jacobi", "bssor"]:
+        with CutMeshSolver(pos, tris, h, precond=precond) as s:
+            r = s.solve(t, mode="deform", precision="fp64", tol=1e-10, max_iter=20000, algo="classic")
+            assert r.status == 0
+            its[precond] = r.iterations
+    assert its["bssor"] < 0.8 * its["jacobi"], its
+
+
+def test_block_ssor_rejects_pipelined_form():
+    pos, tris, h, t = workload("cyl_tiny")
+    with CutMeshSolver(pos, tris, h, precond="bssor") as s:
+        with pytest.raises(CnError) as e:
+            s.solve(t[:, :3], mode="deform", algo="pipelined")
+        assert e.value.status == L.CN_BAD_INPUT

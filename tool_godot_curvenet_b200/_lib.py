@@ -11,7 +11,7 @@ LIB_PATH = os.path.join(_HERE, "lib", "libcurvenet_b200.so")
 
 CN_OK, CN_MAX_ITER, CN_SINGULAR_COMPONENT, CN_NONPOS_PIVOT, CN_NAN = 0, 1, 2, 3, 4
 CN_BREAKDOWN, CN_TIMEOUT, CN_BAD_INPUT, CN_CUDA_ERROR, CN_NO_DEVICE = 5, 6, 7, 8, 9
-PRECOND_JACOBI, PRECOND_IC0, PRECOND_HSC = 0, 1, 2
+PRECOND_JACOBI, PRECOND_IC0, PRECOND_HSC, PRECOND_BSSOR = 0, 1, 2, 3
 ORDER_NATURAL, ORDER_COLOR, ORDER_AUTO = 0, 1, 2
 LAPLACIAN_COT, LAPLACIAN_ROBUST = 0, 1
 PREC_FP64, PREC_MIXED = 0, 1

@@ -49,6 +49,9 @@ struct cn_system {
   double *d_targets = nullptr, *d_xout = nullptr, *d_scal = nullptr;
   double *d_pown = nullptr, *d_m[3] = {};   // row-cached solve: own-row state, gather buffers
   double *d_split_t = nullptr, *d_split_x = nullptr;  // k = 9 as three k = 3 solves
+  // block SSOR: block-local colours of the rows for blocks of bcolor_rb rows (own allocation)
+  unsigned char* d_bcolor = nullptr;
+  int bcolor_rb = -1, bncolor = 0;
   int* d_status = nullptr;
   // pipelined solve: shared-memory needs of the last (grid, block, precision, k)
   int pipe_grid = -1, pipe_block = -1, pipe_prec = -1, pipe_k = -1;
@@ -77,6 +80,11 @@ struct cn_system {
 };
 
 namespace {
+
+// Jacobi and block SSOR run on the row-cached kernel
+bool row_cached(const cn_system* S) {
+  return !S->hsc && (S->opts.precond == CN_PRECOND_JACOBI || S->opts.precond == CN_PRECOND_BSSOR);
+}
 
 const char* kStatusText[] = {"ok", "max_iter", "singular_component", "nonpositive_pivot",
                              "nan", "breakdown", "timeout", "bad_input", "cuda_error",
@@ -315,7 +323,8 @@ cn_status cn_build(const cn_mesh_desc* mesh, const cn_build_opts* opts, cn_handl
     set_err("max_rhs must be 1, 3 or 9");
     return CN_BAD_INPUT;
   }
-  if (o.precond != CN_PRECOND_IC0 && o.precond != CN_PRECOND_JACOBI && o.precond != CN_PRECOND_HSC) {
+  if (o.precond != CN_PRECOND_IC0 && o.precond != CN_PRECOND_JACOBI && o.precond != CN_PRECOND_HSC &&
+      o.precond != CN_PRECOND_BSSOR) {
     set_err("unsupported preconditioner %d", o.precond);
     return CN_BAD_INPUT;
   }
@@ -392,7 +401,7 @@ void cn_destroy(cn_handle S) {
   for (void* p : {(void*)S->d_curve_of, (void*)S->d_row_of, (void*)S->d_tau, (void*)S->d_rest_cp,
                   (void*)S->d_posed_cp, (void*)S->d_weights, (void*)S->d_dLdx, (void*)S->d_dP, (void*)S->d_dw,
                   (void*)S->d_vf_ptr, (void*)S->d_vf_face, (void*)S->d_vf_corner, (void*)S->d_contrib,
-                  (void*)S->d_Xc})
+                  (void*)S->d_Xc, (void*)S->d_bcolor})
     if (p) cudaFree(p);
   if (S->ev0) cudaEventDestroy(S->ev0);
   if (S->ev1) cudaEventDestroy(S->ev1);
@@ -456,7 +465,7 @@ cn_status cn_solve_device(cn_handle S, int32_t k, const double* d_targets, doubl
   // The row-cached Jacobi kernel runs k = 9 as three k = 3 solves on column
   // slices: its k = 9 state fits neither shared memory nor registers, and
   // three k = 3 solves take a third of the time of one k = 9 solve.
-  if (k == 9 && !S->hsc && S->opts.precond == CN_PRECOND_JACOBI && o.algo != CN_ALGO_PLAIN && S->d_split_t &&
+  if (k == 9 && row_cached(S) && o.algo != CN_ALGO_PLAIN && S->d_split_t &&
       o.tol > 0.0 && o.max_iter >= 0 && o.max_refine >= 1) {
     CN_CUDA(cudaSetDevice(S->device));
     const int rows_t = o.mode == CN_MODE_RHS ? S->H.n : S->H.nh;
@@ -531,12 +540,14 @@ cn_status cn_solve_device(cn_handle S, int32_t k, const double* d_targets, doubl
     set_err("the pipelined form needs the Jacobi preconditioner");
     return CN_BAD_INPUT;
   }
-  if (!S->hsc && S->opts.precond == CN_PRECOND_JACOBI) {
+  if (row_cached(S)) {
     // FP64: pipelined, falling back to the two-reduction form if an inner
     // solve stalls; mixed: the two-reduction form (the FP32 pipelined
     // recurrences drift on ill-conditioned meshes), pipelined on request
     a.pipe_mode = o.algo == CN_ALGO_PIPELINED ? 1 : o.algo == CN_ALGO_CLASSIC ? 0
                 : o.precision == CN_PREC_FP64 ? 2 : 0;
+    const bool bssor = S->opts.precond == CN_PRECOND_BSSOR;
+    if (bssor) a.pipe_mode = 0;  // the pipelined recurrences assume a diagonal M
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, S->device);
     // the grid: every SM, or fewer blocks of at least 256 rows for a small mesh
@@ -555,8 +566,8 @@ cn_status cn_solve_device(cn_handle S, int32_t k, const double* d_targets, doubl
       int level = 2;  // 2: row cache and own state in shared memory, 1: row cache only, 0: none
       for (int tries = 0; tries < 6; ++tries) {
         if (S->pipe_grid != grid || S->pipe_block != block || S->pipe_prec != o.precision || S->pipe_k != k) {
-          cn::pipelined_smem_need(S->H.A_ptr.data(), S->H.n, grid, block, o.precision, k, &S->pipe_cache,
-                                  &S->pipe_full);
+          cn::pipelined_smem_need(S->H.A_ptr.data(), S->H.A_col.data(), S->H.n, grid, block, o.precision, k, bssor,
+                                  &S->pipe_cache, &S->pipe_full);
           S->pipe_grid = grid; S->pipe_block = block; S->pipe_prec = o.precision; S->pipe_k = k;
         }
         if (level == 2 && S->pipe_full > cap) level = 1;
@@ -574,6 +585,22 @@ cn_status cn_solve_device(cn_handle S, int32_t k, const double* d_targets, doubl
         }
         grid = mg;
       }
+    }
+    a.bcolor = nullptr;
+    a.bncolor = 0;
+    if (bssor) {
+      // block-local colours for the blocks of this launch (rb rows each)
+      const long long tot = (long long)(grid > 1 ? grid : 1) * block;
+      const int rb = (int)(((long long)S->H.n + tot - 1) / tot * block);
+      if (S->bcolor_rb != rb) {
+        std::vector<unsigned char> col((size_t)std::max(S->H.n, 1));
+        S->bncolor = cn::block_colours(S->H.A_ptr.data(), S->H.A_col.data(), S->H.n, std::max(rb, 1), col.data());
+        if (!S->d_bcolor) CN_CUDA(cudaMalloc((void**)&S->d_bcolor, (size_t)std::max(S->H.n, 1)));
+        if (S->H.n) CN_CUDA(cudaMemcpy(S->d_bcolor, col.data(), (size_t)S->H.n, cudaMemcpyHostToDevice));
+        S->bcolor_rb = rb;
+      }
+      a.bcolor = S->d_bcolor;
+      a.bncolor = S->bncolor;
     }
     CN_CUDA(cudaMemsetAsync(S->d_ctl, 0, sizeof(Control), S->stream));
     CN_CUDA(cudaEventRecord(S->ev0, S->stream));
@@ -1063,8 +1090,8 @@ cn_status cn_set_launch(cn_handle S, int32_t lanes, int32_t block, int32_t grid)
     set_err("bad launch shape (lanes %d, block %d, grid %d)", lanes, block, grid);
     return CN_BAD_INPUT;
   }
-  const bool row_cached = !S->hsc && S->opts.precond == CN_PRECOND_JACOBI;  // clamps its grid per solve
-  if (grid > 1 && !row_cached) {
+  const bool rc = row_cached(S);  // clamps its grid per solve
+  if (grid > 1 && !rc) {
     const int mg = std::min(cn::persistent_max_grid(CN_PREC_MIXED, S->kmax, lanes, block),
                             cn::persistent_max_grid(CN_PREC_FP64, S->kmax, lanes, block));
     if (mg < 1) {
@@ -1073,7 +1100,7 @@ cn_status cn_set_launch(cn_handle S, int32_t lanes, int32_t block, int32_t grid)
     }
     grid = std::min(grid, std::min(mg, S->max_grid_alloc));
   }
-  if (row_cached) grid = std::min(grid, S->max_grid_alloc);
+  if (rc) grid = std::min(grid, S->max_grid_alloc);
   S->lanes = lanes;
   S->block = block;
   S->grid = grid;
@@ -1096,7 +1123,7 @@ cn_status cn_autotune(cn_handle S, int32_t k, const double* d_targets, const cn_
   struct Cand { int lanes, block, grid; };
   std::vector<Cand> cands;
   const int lane_set[] = {1, 2, 4, 8};
-  if (!S->hsc && S->opts.precond == CN_PRECOND_JACOBI) {
+  if (row_cached(S)) {
     // the row-cached kernel: one lane per row; blocks of up to 512 threads
     // take two rows per thread, larger ones one
     for (int g : {sms / 2, (3 * sms) / 4, sms}) {

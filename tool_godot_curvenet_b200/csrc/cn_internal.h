@@ -80,6 +80,8 @@ struct SolveArgs {
   double* pown;            // FP64 own-row state when it is not in shared memory: 7 x [rows][K]
   const double* dinv64;    // 1 / sqrt(A_ii), FP64
   int cache_bytes;         // dynamic shared memory (row cache, then own-row state)
+  const unsigned char* bcolor;  // block SSOR: block-local colour of every row (null: Jacobi)
+  int bncolor;                  // colours
   double* partials;        // [kSlots][grid][K]
   // HSC preconditioner (hsc != 0): rows are in HSC order; F_l = positions
   // [hsc_off[l], hsc_off[l + 1]); the coarse set starts at hsc_off[hsc_L];
@@ -148,12 +150,16 @@ cudaError_t launch_spmm(int n, int k, int precision, const int* ptr, const int* 
 cudaError_t launch_pipelined_solve(const SolveArgs& a, int precision, int K, int block, int grid, int qr,
                                    cudaStream_t s);
 int pipelined_max_grid(int precision, int K, int block, int cache_bytes, int qr);
-// Shared memory of the pipelined solve for this launch shape (the largest
-// block's share), given the row pointer of A: *cache = the row cache alone,
-// *full = the row cache and the FP64 own-row state; SIZE_MAX when a block
-// holds more than kPipeSlices row slices.
-void pipelined_smem_need(const int* A_ptr, int n, int grid, int block, int precision, int K, size_t* cache,
-                         size_t* full);
+// Shared memory of the row-cached solve for this launch shape (the largest
+// block's share), given A's pattern: *cache = the row cache alone, *full =
+// the row cache and the own-row state (and, for block SSOR, the colour
+// lists); SIZE_MAX when a block holds more than kPipeSlices row slices.
+void pipelined_smem_need(const int* A_ptr, const int* A_col, int n, int grid, int block, int precision, int K,
+                         bool bssor, size_t* cache, size_t* full);
+// Greedy colouring of the rows inside each block of rb consecutive rows, in
+// row order, over the couplings inside the block (at most 64 colours);
+// returns the number of colours.
+int block_colours(const int* A_ptr, const int* A_col, int n, int rb, unsigned char* col);
 
 // Build-time kernels (cn_assemble.cu).
 struct BuildArgs {

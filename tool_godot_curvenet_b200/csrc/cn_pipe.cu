@@ -34,6 +34,10 @@
 // m alternates between two buffers for the same reason.
 #include <algorithm>
 
+#include <set>
+#include <tuple>
+#include <vector>
+
 #include "cn_pcg_body.cuh"
 
 namespace cn {
@@ -49,6 +53,7 @@ struct MRow {
 };
 
 constexpr int kPipeSplits = 8;  // partial-sum read: up to 8 x 128 blocks
+constexpr int kMaxColours = 64;   // block SSOR: colours of a block (greedy: at most the row length)
 // The pipelined recurrences in FP32 lose track of the true residual below
 // about 1e-4 of the starting one, so each refinement step of the mixed solve
 // asks the inner solve for at most this much reduction.
@@ -66,6 +71,12 @@ struct PipeSmem {
   int wmax[kPipeSlices];
   int base[kPipeSlices + 1];
   int cached, own_s;
+  // block SSOR: start of each colour's rows in the slot list, the widths of
+  // the colour's lower / upper neighbour lists and where those lists start
+  int coff[kMaxColours + 1];
+  int wl[kMaxColours], wu[kMaxColours], loff[kMaxColours], uoff[kMaxColours];
+  int lents;  // entries of the neighbour lists
+  int ncb;    // colours of this block's rows
 };
 
 __host__ __device__ inline size_t align16(size_t b) { return (b + 15) & ~(size_t)15; }
@@ -290,16 +301,38 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
   auto pipe_ptr = [&](int g) { return part + ((size_t)(2 + 2 * g) * tsize) * K; };
   int status = CN_OK, total_iters = 0, refinements = 0;
 
+  const unsigned char* bcol = a.bcolor;
+  const bool bssor = bcol != nullptr;
+  const int rb_n = n - blk0 < Qg * B ? n - blk0 : Qg * B;  // rows of this block
   // ---- shared memory: the block's rows of A, then (if it fits) the own-row
-  // state
+  // state and, for block SSOR, the colour lists
   {
     if (t < kPipeSlices) s->wmax[t] = 0;
+    if (t < kMaxColours) s->wl[t] = s->wu[t] = 0;
+    if (t <= kMaxColours) s->coff[t] = 0;
     __syncthreads();
     const int qc = Qb < kPipeSlices ? Qb : kPipeSlices;
     for (int q = 0; q < qc; ++q) {
       const int row = row0 + q * R;
       if (row < n) atomicMax(&s->wmax[q], a.A_ptr[row + 1] - a.A_ptr[row]);
     }
+    if (bssor)  // rows per colour; lower / upper neighbours inside the block per row
+      for (int q = 0; q < Qb; ++q) {
+        const int row = row0 + q * R;
+        if (row >= n) break;
+        const int ci = (int)__ldg(bcol + row);
+        int nl = 0, nu = 0;
+        for (int e = a.A_ptr[row]; e < a.A_ptr[row + 1]; ++e) {
+          const int j = a.A_col[e];
+          if (j < blk0 || j >= blk0 + rb_n || j == row) continue;
+          const int cj = (int)__ldg(bcol + j);
+          nl += cj < ci;
+          nu += cj > ci;
+        }
+        atomicAdd(&s->coff[ci + 1], 1);
+        atomicMax(&s->wl[ci], nl);
+        atomicMax(&s->wu[ci], nu);
+      }
     __syncthreads();
     if (t == 0) {
       int ents = 0;
@@ -309,7 +342,25 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
       }
       s->base[qc] = ents;
       const size_t need = align16((size_t)ents * sizeof(int)) + align16((size_t)ents * sizeof(T));
-      const size_t own = (size_t)(6 * K + 1) * Qb * B * sizeof(T);
+      // own-row state, plus for block SSOR the rows' colours, the slots by
+      // colour and the colours' neighbour lists (slot, value)
+      size_t own = align16((size_t)(6 * K + 1) * Qb * B * sizeof(T));
+      int lents = 0, ncb = 0;
+      if (bssor) {
+        for (int c = 0; c < kMaxColours; ++c) {
+          const int cnt = s->coff[c + 1];
+          if (cnt > 0) ncb = c + 1;
+          s->coff[c + 1] += s->coff[c];
+          s->loff[c] = lents;
+          lents += cnt * s->wl[c];
+          s->uoff[c] = lents;
+          lents += cnt * s->wu[c];
+        }
+        own += align16((size_t)Qb * B) + align16((size_t)Qb * B * sizeof(short)) +
+               align16((size_t)lents * sizeof(short)) + align16((size_t)lents * sizeof(T));
+      }
+      s->lents = lents;
+      s->ncb = ncb;
       s->cached = (qc == Qb && Qb > 0 && need <= (size_t)a.cache_bytes) ? 1 : 0;
       s->own_s = (s->cached && need + own <= (size_t)a.cache_bytes) ? 1 : 0;
     }
@@ -320,6 +371,16 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
   int* ccol = (int*)dyn;
   T* cval = (T*)(dyn + align16((size_t)ents * sizeof(int)));
   T* os = (T*)(dyn + align16((size_t)ents * sizeof(int)) + align16((size_t)ents * sizeof(T)));
+  // block SSOR, own state in shared memory: per own row its colour, the
+  // block's slots ordered by colour, and per colour the lower- and
+  // higher-colour neighbours of its rows inside the block (neighbour slot,
+  // -1 padding; value), entry e of the colour's p-th row at
+  // off + e * rows of the colour + p
+  unsigned char* srowc = (unsigned char*)os + align16((size_t)(6 * K + 1) * Qb * B * sizeof(T));
+  short* slist = (short*)(srowc + align16((size_t)Qb * B));
+  const int lents = s->lents;
+  short* lslot = (short*)((unsigned char*)slist + align16((size_t)Qb * B * sizeof(short)));
+  T* lval = (T*)((unsigned char*)lslot + align16((size_t)lents * sizeof(short)));
   T* pown = (T*)a.pown;
   auto own_ref = [&](int q, int row) {
     OwnRef<T, K> o;
@@ -363,6 +424,165 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
     }
     return rr;
   };
+  // ---- block SSOR (a.bcolor != null): M = (D + L) D^-1 (D + U) over the
+  // block's own rows (the couplings to other blocks dropped), L / U in the
+  // order of the block-local colours a.bcolor (rows of one colour are not
+  // coupled).  z = M^-1 r: y = (D + L)^-1 r colour by colour upwards, then
+  // z = y - D^-1 U z colour by colour downwards; one block barrier per
+  // colour step.
+  //
+  // Own state in shared memory: a step runs over the colour's slot list,
+  // one row per thread, its neighbours from the colour's lists (consecutive
+  // rows of the list read consecutive entries).  The colour-0 rows (no lower
+  // neighbours) have y = M_ii^-1 r_i; with c0done their owners have set it
+  // before the barrier ahead of the sweeps.  The top colour's z = y is
+  // written by the last upward step.
+  auto ssor_fast = [&](bool c0done) {
+    constexpr int UE = 4;
+    const int nc = s->ncb;
+    for (int pass = 0; pass < 2; ++pass) {
+      const bool fwd = pass == 0;
+      for (int step = fwd ? (c0done ? 1 : 0) : 1; step < nc; ++step) {
+        const int c = fwd ? step : nc - 1 - step;
+        const int beg = s->coff[c], cnt = s->coff[c + 1] - beg;
+        const int w = fwd ? s->wl[c] : s->wu[c];
+        const int lo = fwd ? s->loff[c] : s->uoff[c];
+        const bool top = fwd && c == nc - 1;
+        for (int p = t; p < cnt; p += B) {
+          T* o = os + (size_t)slist[beg + p] * OwnRef<T, K>::kLen;
+          T acc[K];
+#pragma unroll
+          for (int cc = 0; cc < K; ++cc) acc[cc] = (T)0;
+          for (int e0 = 0; e0 < w; e0 += UE) {
+            int sl[UE];
+            T v[UE];
+#pragma unroll
+            for (int u = 0; u < UE; ++u) {
+              const int ix = lo + (e0 + u) * cnt + p;
+              sl[u] = e0 + u < w ? (int)lslot[ix] : -1;
+              v[u] = e0 + u < w ? lval[ix] : (T)0;
+            }
+#pragma unroll
+            for (int u = 0; u < UE; ++u)
+              if (sl[u] >= 0) {
+                const T* oj = os + (size_t)sl[u] * OwnRef<T, K>::kLen + (fwd ? kQs : kQz) * K;
+#pragma unroll
+                for (int cc = 0; cc < K; ++cc) acc[cc] += v[u] * oj[cc];
+              }
+          }
+          const T mi = o[kQminv * K];
+#pragma unroll
+          for (int cc = 0; cc < K; ++cc) {
+            if (fwd) {
+              const T y = (o[kQr * K + cc] - acc[cc]) * mi;
+              o[kQs * K + cc] = y;
+              if (top) o[kQz * K + cc] = y;
+            } else {
+              o[kQz * K + cc] = o[kQs * K + cc] - mi * acc[cc];
+            }
+          }
+        }
+        __syncthreads();
+      }
+    }
+  };
+  // Own state in global memory: each thread its own rows, colour by colour,
+  // the neighbours from the row of A.
+  auto ssor_generic = [&]() {
+    for (int pass = 0; pass < 2; ++pass) {
+      const bool fwd = pass == 0;
+      for (int step = 0; step < s->ncb; ++step) {
+        const int c = fwd ? step : s->ncb - 1 - step;
+        for (int q = 0; q < Qb; ++q) {
+          const int row = row0 + q * R;
+          if (row >= n) break;
+          if ((int)__ldg(bcol + row) != c) continue;
+          const OwnRef<T, K> o = own_ref(q, row);
+          const RowRef<T> rr = row_ref(q, row);
+          T acc[K];
+#pragma unroll
+          for (int cc = 0; cc < K; ++cc) acc[cc] = (T)0;
+          for (int e = 0; e < rr.len; ++e) {
+            const int j = rr.c[e * rr.stride];
+            if (j < blk0 || j >= blk0 + rb_n || j == row) continue;  // padding (-1) or another block's row
+            const int cj = (int)__ldg(bcol + j);
+            if (fwd ? cj >= c : cj <= c) continue;
+            const T v = rr.v[e * rr.stride];
+            const T* oj = pown + (size_t)j * OwnRef<T, K>::kLen + (fwd ? kQs : kQz) * K;
+#pragma unroll
+            for (int cc = 0; cc < K; ++cc) acc[cc] += v * oj[cc];
+          }
+          const T mi = o(kQminv, 0);
+#pragma unroll
+          for (int cc = 0; cc < K; ++cc) {
+            if (fwd) o(kQs, cc) = (o(kQr, cc) - acc[cc]) * mi;
+            else o(kQz, cc) = o(kQs, cc) - mi * acc[cc];
+          }
+        }
+        __syncthreads();
+      }
+    }
+  };
+  const bool fast_ssor = bssor && own_s;
+  auto ssor_apply = [&](bool c0done) {
+    if (fast_ssor) ssor_fast(c0done);
+    else ssor_generic();
+  };
+  if (fast_ssor) {
+    for (int q = 0; q < Qb; ++q) {
+      const int row = row0 + q * R;
+      srowc[q * B + t] = row < n ? __ldg(bcol + row) : (unsigned char)255;
+    }
+    __syncthreads();
+    // slot lists in slot order (warp w scans the block's slots for the
+    // colours w, w + warps, ...; ballots give the positions) and each row's
+    // column of its colour's lists
+    const int nslots = Qb * B;
+    for (int c = warp; c < s->ncb; c += nw) {
+      int pos0 = s->coff[c];
+      const int cnt = s->coff[c + 1] - pos0;
+      const int lo = s->loff[c], uo = s->uoff[c], wl = s->wl[c], wu = s->wu[c];
+      for (int s0 = 0; s0 < nslots; s0 += 32) {
+        const int slot = s0 + lane;
+        const bool hit = slot < nslots && srowc[slot] == c;
+        const unsigned m = __ballot_sync(0xffffffffu, hit);
+        if (hit) {
+          const int pos = pos0 + __popc(m & ((1u << lane) - 1u));
+          slist[pos] = (short)slot;
+          const int p = pos - s->coff[c];
+          const int q = slot / B, tt = slot - q * B, row = blk0 + slot;
+          const int wq = s->wmax[q], bq = s->base[q] + tt;
+          int nl = 0, nu = 0;
+          for (int e = 0; e < wq; ++e) {
+            const int ix = bq + e * B;
+            const int j = ccol[ix];
+            if (j < blk0 || j >= blk0 + rb_n || j == row) continue;
+            const int cj = srowc[j - blk0];
+            if (cj < c) {
+              lslot[lo + nl * cnt + p] = (short)(j - blk0);
+              lval[lo + nl * cnt + p] = cval[ix];
+              ++nl;
+            } else if (cj > c) {
+              lslot[uo + nu * cnt + p] = (short)(j - blk0);
+              lval[uo + nu * cnt + p] = cval[ix];
+              ++nu;
+            }
+          }
+          for (; nl < wl; ++nl) {
+            lslot[lo + nl * cnt + p] = -1;
+            lval[lo + nl * cnt + p] = (T)0;
+          }
+          for (; nu < wu; ++nu) {
+            lslot[uo + nu * cnt + p] = -1;
+            lval[uo + nu * cnt + p] = (T)0;
+          }
+        }
+        pos0 += __popc(m);
+      }
+    }
+    __syncthreads();
+  }
+
   // row slices q < QR: gathered together before the partial sums are needed
   bool okq[QR];
   RowRef<T> rrq[QR];
@@ -449,12 +669,28 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
           rr[c] += rv * rv;
         }
         // both forms' first gathers: u = M^-1 r (pipelined, to m0) and
-        // z = M^-1 r (classic, to m2)
-        T m[K];
+        // z = M^-1 r (classic, to m2; after the block sweeps with block SSOR)
+        if (!bssor) {
+          T m[K];
 #pragma unroll
-        for (int c = 0; c < K; ++c) m[c] = u[c];
-        store_m<T, K>(mb0, row, m);
-        store_m<T, K>(mb2, row, m);
+          for (int c = 0; c < K; ++c) m[c] = u[c];
+          store_m<T, K>(mb0, row, m);
+          store_m<T, K>(mb2, row, m);
+        }
+      }
+      if (bssor) {
+        __syncthreads();
+        ssor_apply(false);
+        for (int q = 0; q < Qb; ++q) {
+          const int row = row0 + q * R;
+          if (row >= n) break;
+          const OwnRef<T, K> o = own_ref(q, row);
+          T m[K];
+#pragma unroll
+          for (int c = 0; c < K; ++c) m[c] = o(kQz, c);
+          store_m<T, K>(mb0, row, m);
+          store_m<T, K>(mb2, row, m);
+        }
       }
       block_reduce_store<K>(rr, s->sm.red, slot_ptr(kRR64) + (size_t)team.rank() * K);
       if (!team.sync()) { status = CN_TIMEOUT; goto done; }
@@ -776,20 +1012,45 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
           if (row >= n) break;
           const OwnRef<T, K> o = own_ref(q, row);
           const T mi = o(kQminv, 0);
+          // block SSOR: a colour-0 row's y (and z, with one colour) needs no neighbour
+          const bool y0 = fast_ssor && srowc[q * B + t] == 0;
           T rec[K];
 #pragma unroll
           for (int c = 0; c < K; ++c) {
             const T p = o(kQp, c);
             o(kQx, c) += alpha[c] * p;
             const T r = o(kQr, c) - alpha[c] * o(kQw, c);
-            const T z = mi * r;
             o(kQr, c) = r;
-            o(kQz, c) = z;
-            rec[c] = z;
-            d2[c] += r * z;
-            d2[K + c] += r * r;
+            if (!bssor) {
+              const T z = mi * r;
+              o(kQz, c) = z;
+              rec[c] = z;
+              d2[c] += r * z;
+              d2[K + c] += r * r;
+            } else if (y0) {
+              o(kQs, c) = mi * r;
+              if (s->ncb == 1) o(kQz, c) = mi * r;
+            }
           }
-          store_m<T, K>(rnext, row, rec);
+          if (!bssor) store_m<T, K>(rnext, row, rec);
+        }
+        if (bssor) {  // z = M^-1 r by the block sweeps, then the records and the dots
+          __syncthreads();
+          ssor_apply(true);
+          for (int q = 0; q < Qb; ++q) {
+            const int row = row0 + q * R;
+            if (row >= n) break;
+            const OwnRef<T, K> o = own_ref(q, row);
+            T rec[K];
+#pragma unroll
+            for (int c = 0; c < K; ++c) {
+              const T r = o(kQr, c), z = o(kQz, c);
+              rec[c] = z;
+              d2[c] += r * z;
+              d2[K + c] += r * r;
+            }
+            store_m<T, K>(rnext, row, rec);
+          }
         }
         block_reduce_strided<2 * K, T>(d2, s->red2, tU + team.rank(), tsize);
       }
@@ -917,18 +1178,68 @@ int pipelined_max_grid(int precision, int K, int block, int cache_bytes, int qr)
   return 0;
 }
 
-void pipelined_smem_need(const int* A_ptr, int n, int grid, int block, int precision, int K, size_t* cache,
-                         size_t* full) {
+int block_colours(const int* A_ptr, const int* A_col, int n, int rb, unsigned char* col) {
+  // DSatur inside each block: the next row is the uncoloured one with the
+  // most distinct colours among its coloured neighbours (then the most
+  // uncoloured neighbours, then the lowest index); it takes the lowest
+  // colour none of them has.
+  int maxc = 0;
+  std::vector<unsigned long long> used;
+  std::vector<int> deg;
+  for (int lo = 0; lo < n; lo += rb) {
+    const int hi = std::min(n, lo + rb), m = hi - lo;
+    used.assign((size_t)m, 0ull);
+    deg.assign((size_t)m, 0);
+    for (int i = lo; i < hi; ++i)
+      for (int e = A_ptr[i]; e < A_ptr[i + 1]; ++e) {
+        const int j = A_col[e];
+        if (j >= lo && j < hi && j != i) ++deg[i - lo];
+      }
+    // key: (saturation, uncoloured neighbours, -index), largest first
+    std::set<std::tuple<int, int, int>> pq;
+    for (int r = 0; r < m; ++r) pq.insert({0, deg[r], -r});
+    std::vector<char> done((size_t)m, 0);
+    while (!pq.empty()) {
+      const auto top = *pq.rbegin();
+      pq.erase(std::prev(pq.end()));
+      const int r = -std::get<2>(top), i = lo + r;
+      int c = 0;
+      while (c < kMaxColours - 1 && (used[r] >> c & 1ull)) ++c;
+      col[i] = (unsigned char)c;
+      done[r] = 1;
+      maxc = std::max(maxc, c + 1);
+      for (int e = A_ptr[i]; e < A_ptr[i + 1]; ++e) {
+        const int j = A_col[e];
+        if (j < lo || j >= hi || j == i || done[j - lo]) continue;
+        const int q = j - lo;
+        pq.erase({__builtin_popcountll(used[q]), deg[q], -q});
+        used[q] |= 1ull << c;
+        --deg[q];
+        pq.insert({__builtin_popcountll(used[q]), deg[q], -q});
+      }
+    }
+  }
+  return maxc;
+}
+
+void pipelined_smem_need(const int* A_ptr, const int* A_col, int n, int grid, int block, int precision, int K,
+                         bool bssor, size_t* cache, size_t* full) {
   const size_t vs = precision == CN_PREC_MIXED ? sizeof(float) : sizeof(double);
   const long long Qg = ((long long)n + (long long)grid * block - 1) / ((long long)grid * block);
   const long long R = block;
   size_t wc = 0, wf = 0;
   *cache = *full = (size_t)-1;
+  if (Qg > kPipeSlices) return;
+  std::vector<unsigned char> col;
+  if (bssor && n > 0) {  // the colours the solve will use for blocks of Qg x block rows
+    col.resize((size_t)n);
+    block_colours(A_ptr, A_col, n, (int)(Qg * block), col.data());
+  }
   for (int b = 0; b < grid; ++b) {
     const long long blk0 = (long long)b * Qg * block;
     if (blk0 >= n) break;
     const long long Qb = Qg;
-    if (Qb > kPipeSlices) return;
+    const long long rb_n = std::min<long long>(n - blk0, Qg * block);
     size_t ents = 0;
     for (long long q = 0; q < Qb; ++q) {
       int w = 0;
@@ -940,7 +1251,28 @@ void pipelined_smem_need(const int* A_ptr, int n, int grid, int block, int preci
     }
     const size_t c = align16(ents * sizeof(int)) + align16(ents * vs);
     wc = std::max(wc, c);
-    wf = std::max(wf, c + (size_t)(6 * K + 1) * (size_t)Qb * (size_t)block * vs);
+    size_t extra = 0;
+    if (bssor) {  // the kernel's colour lists: rows per colour x (lower + upper width)
+      int cnt[kMaxColours] = {}, wl[kMaxColours] = {}, wu[kMaxColours] = {};
+      for (long long row = blk0; row < blk0 + rb_n; ++row) {
+        const int ci = col[row];
+        int nl = 0, nu = 0;
+        for (int e = A_ptr[row]; e < A_ptr[row + 1]; ++e) {
+          const int j = A_col[e];
+          if (j < blk0 || j >= blk0 + rb_n || j == row) continue;
+          nl += col[j] < ci;
+          nu += col[j] > ci;
+        }
+        ++cnt[ci];
+        wl[ci] = std::max(wl[ci], nl);
+        wu[ci] = std::max(wu[ci], nu);
+      }
+      size_t lents = 0;
+      for (int k = 0; k < kMaxColours; ++k) lents += (size_t)cnt[k] * (wl[k] + wu[k]);
+      extra = align16((size_t)Qb * block) + align16((size_t)Qb * block * sizeof(short)) +
+              align16(lents * sizeof(short)) + align16(lents * vs);
+    }
+    wf = std::max(wf, c + align16((size_t)(6 * K + 1) * (size_t)Qb * (size_t)block * vs) + extra);
   }
   *cache = wc;
   *full = wf;

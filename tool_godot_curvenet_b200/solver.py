@@ -38,7 +38,7 @@ def _dp(a):
     return a.ctypes.data_as(C.POINTER(C.c_double))
 
 
-_PRECOND = {"jacobi": L.PRECOND_JACOBI, "ic0": L.PRECOND_IC0, "hsc": L.PRECOND_HSC}
+_PRECOND = {"jacobi": L.PRECOND_JACOBI, "ic0": L.PRECOND_IC0, "hsc": L.PRECOND_HSC, "bssor": L.PRECOND_BSSOR}
 _ORDER = {"natural": L.ORDER_NATURAL, "color": L.ORDER_COLOR, "auto": L.ORDER_AUTO}
 _LAP = {"cot": L.LAPLACIAN_COT, "robust": L.LAPLACIAN_ROBUST}
 _PREC = {"fp64": L.PREC_FP64, "mixed": L.PREC_MIXED}
