@@ -81,6 +81,14 @@ struct PipeSmem {
 
 __host__ __device__ inline size_t align16(size_t b) { return (b + 15) & ~(size_t)15; }
 
+// Block SSOR list entry: a neighbour's list position (-1: padding) and its
+// coefficient scaled by the row's 1 / A_ii (one 8- or 16-byte load)
+template <typename T>
+struct alignas(2 * sizeof(T)) LEnt {
+  int j;
+  T v;
+};
+
 template <typename T, int K>
 __device__ __forceinline__ void load_m(const T* __restrict__ m, int j, T (&x)[K]) {
   constexpr int W = MRow<T, K>::W, NC = MRow<T, K>::NC;
@@ -342,8 +350,9 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
       }
       s->base[qc] = ents;
       const size_t need = align16((size_t)ents * sizeof(int)) + align16((size_t)ents * sizeof(T));
-      // own-row state, plus for block SSOR the rows' colours, the slots by
-      // colour and the colours' neighbour lists (slot, value)
+      // own-row state, plus for block SSOR the rows' colours and list
+      // positions, the colours' neighbour lists and the sweep vector in
+      // list order
       size_t own = align16((size_t)(6 * K + 1) * Qb * B * sizeof(T));
       int lents = 0, ncb = 0;
       if (bssor) {
@@ -357,7 +366,7 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
           lents += cnt * s->wu[c];
         }
         own += align16((size_t)Qb * B) + align16((size_t)Qb * B * sizeof(short)) +
-               align16((size_t)lents * sizeof(short)) + align16((size_t)lents * sizeof(T));
+               align16((size_t)lents * sizeof(LEnt<T>)) + (size_t)Qb * B * MRow<T, K>::W * sizeof(T);
       }
       s->lents = lents;
       s->ncb = ncb;
@@ -371,16 +380,19 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
   int* ccol = (int*)dyn;
   T* cval = (T*)(dyn + align16((size_t)ents * sizeof(int)));
   T* os = (T*)(dyn + align16((size_t)ents * sizeof(int)) + align16((size_t)ents * sizeof(T)));
-  // block SSOR, own state in shared memory: per own row its colour, the
-  // block's slots ordered by colour, and per colour the lower- and
-  // higher-colour neighbours of its rows inside the block (neighbour slot,
-  // -1 padding; value), entry e of the colour's p-th row at
-  // off + e * rows of the colour + p
-  unsigned char* srowc = (unsigned char*)os + align16((size_t)(6 * K + 1) * Qb * B * sizeof(T));
-  short* slist = (short*)(srowc + align16((size_t)Qb * B));
+  // block SSOR, own state in shared memory: the block's rows are listed by
+  // colour (in row order inside a colour); per slot (q B + t) its colour and
+  // list position; per colour the lower- and higher-colour neighbours of its
+  // rows inside the block, entry e of the colour's p-th row at
+  // off + e * rows of the colour + p; the sweep vector v in list order, one
+  // 16-byte-padded row per position (consecutive threads of a step touch
+  // consecutive rows)
+  const int nsl = Qb * B;
+  unsigned char* srowc = (unsigned char*)os + align16((size_t)(6 * K + 1) * nsl * sizeof(T));
+  short* spos = (short*)(srowc + align16((size_t)nsl));
   const int lents = s->lents;
-  short* lslot = (short*)((unsigned char*)slist + align16((size_t)Qb * B * sizeof(short)));
-  T* lval = (T*)((unsigned char*)lslot + align16((size_t)lents * sizeof(short)));
+  LEnt<T>* lent = (LEnt<T>*)((unsigned char*)spos + align16((size_t)nsl * sizeof(short)));
+  T* sv = (T*)((unsigned char*)lent + align16((size_t)lents * sizeof(LEnt<T>)));  // 16-byte rows
   T* pown = (T*)a.pown;
   auto own_ref = [&](int q, int row) {
     OwnRef<T, K> o;
@@ -431,56 +443,41 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
   // z = y - D^-1 U z colour by colour downwards; one block barrier per
   // colour step.
   //
-  // Own state in shared memory: a step runs over the colour's slot list,
-  // one row per thread, its neighbours from the colour's lists (consecutive
-  // rows of the list read consecutive entries).  The colour-0 rows (no lower
-  // neighbours) have y = M_ii^-1 r_i; with c0done their owners have set it
-  // before the barrier ahead of the sweeps.  The top colour's z = y is
-  // written by the last upward step.
-  auto ssor_fast = [&](bool c0done) {
-    constexpr int UE = 4;
+  // Own state in shared memory: the owners set v = M_ii^-1 r_i before the
+  // barrier ahead of the sweeps; going up, v_i -= sum over lower neighbours
+  // of (a_ij / a_ii) v_j turns v into y colour by colour (colour 0 has no
+  // lower neighbour); going down, v_i -= sum over higher neighbours of
+  // (a_ij / a_ii) v_j turns it into z (the top colour's z is its y).  A step
+  // runs over the colour's list, one row per thread.
+  auto ssor_fast = [&]() {
     const int nc = s->ncb;
     for (int pass = 0; pass < 2; ++pass) {
       const bool fwd = pass == 0;
-      for (int step = fwd ? (c0done ? 1 : 0) : 1; step < nc; ++step) {
+      for (int step = 1; step < nc; ++step) {
         const int c = fwd ? step : nc - 1 - step;
         const int beg = s->coff[c], cnt = s->coff[c + 1] - beg;
         const int w = fwd ? s->wl[c] : s->wu[c];
-        const int lo = fwd ? s->loff[c] : s->uoff[c];
-        const bool top = fwd && c == nc - 1;
+        const LEnt<T>* le = lent + (fwd ? s->loff[c] : s->uoff[c]);
         for (int p = t; p < cnt; p += B) {
-          T* o = os + (size_t)slist[beg + p] * OwnRef<T, K>::kLen;
-          T acc[K];
+          T x[K];
+          load_m<T, K>(sv, beg + p, x);
+          int e = 0;
+          for (; e + 1 < w; e += 2) {
+            const LEnt<T> e0 = le[e * cnt + p], e1 = le[(e + 1) * cnt + p];
+            T y0[K], y1[K];
+            load_m<T, K>(sv, e0.j, y0);
+            load_m<T, K>(sv, e1.j, y1);
 #pragma unroll
-          for (int cc = 0; cc < K; ++cc) acc[cc] = (T)0;
-          for (int e0 = 0; e0 < w; e0 += UE) {
-            int sl[UE];
-            T v[UE];
-#pragma unroll
-            for (int u = 0; u < UE; ++u) {
-              const int ix = lo + (e0 + u) * cnt + p;
-              sl[u] = e0 + u < w ? (int)lslot[ix] : -1;
-              v[u] = e0 + u < w ? lval[ix] : (T)0;
-            }
-#pragma unroll
-            for (int u = 0; u < UE; ++u)
-              if (sl[u] >= 0) {
-                const T* oj = os + (size_t)sl[u] * OwnRef<T, K>::kLen + (fwd ? kQs : kQz) * K;
-#pragma unroll
-                for (int cc = 0; cc < K; ++cc) acc[cc] += v[u] * oj[cc];
-              }
+            for (int cc = 0; cc < K; ++cc) x[cc] -= e0.v * y0[cc] + e1.v * y1[cc];
           }
-          const T mi = o[kQminv * K];
+          if (e < w) {
+            const LEnt<T> e0 = le[e * cnt + p];
+            T y0[K];
+            load_m<T, K>(sv, e0.j, y0);
 #pragma unroll
-          for (int cc = 0; cc < K; ++cc) {
-            if (fwd) {
-              const T y = (o[kQr * K + cc] - acc[cc]) * mi;
-              o[kQs * K + cc] = y;
-              if (top) o[kQz * K + cc] = y;
-            } else {
-              o[kQz * K + cc] = o[kQs * K + cc] - mi * acc[cc];
-            }
+            for (int cc = 0; cc < K; ++cc) x[cc] -= e0.v * y0[cc];
           }
+          store_m<T, K>(sv, beg + p, x);
         }
         __syncthreads();
       }
@@ -524,8 +521,8 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
     }
   };
   const bool fast_ssor = bssor && own_s;
-  auto ssor_apply = [&](bool c0done) {
-    if (fast_ssor) ssor_fast(c0done);
+  auto ssor_apply = [&]() {
+    if (fast_ssor) ssor_fast();
     else ssor_generic();
   };
   if (fast_ssor) {
@@ -534,51 +531,45 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
       srowc[q * B + t] = row < n ? __ldg(bcol + row) : (unsigned char)255;
     }
     __syncthreads();
-    // slot lists in slot order (warp w scans the block's slots for the
-    // colours w, w + warps, ...; ballots give the positions) and each row's
-    // column of its colour's lists
-    const int nslots = Qb * B;
+    // list positions in row order (warp w scans the block's slots for the
+    // colours w, w + warps, ...; ballots give the positions) and the list
+    // order's 1 / A_ii
     for (int c = warp; c < s->ncb; c += nw) {
       int pos0 = s->coff[c];
-      const int cnt = s->coff[c + 1] - pos0;
-      const int lo = s->loff[c], uo = s->uoff[c], wl = s->wl[c], wu = s->wu[c];
-      for (int s0 = 0; s0 < nslots; s0 += 32) {
+      for (int s0 = 0; s0 < nsl; s0 += 32) {
         const int slot = s0 + lane;
-        const bool hit = slot < nslots && srowc[slot] == c;
+        const bool hit = slot < nsl && srowc[slot] == c;
         const unsigned m = __ballot_sync(0xffffffffu, hit);
         if (hit) {
           const int pos = pos0 + __popc(m & ((1u << lane) - 1u));
-          slist[pos] = (short)slot;
-          const int p = pos - s->coff[c];
-          const int q = slot / B, tt = slot - q * B, row = blk0 + slot;
-          const int wq = s->wmax[q], bq = s->base[q] + tt;
-          int nl = 0, nu = 0;
-          for (int e = 0; e < wq; ++e) {
-            const int ix = bq + e * B;
-            const int j = ccol[ix];
-            if (j < blk0 || j >= blk0 + rb_n || j == row) continue;
-            const int cj = srowc[j - blk0];
-            if (cj < c) {
-              lslot[lo + nl * cnt + p] = (short)(j - blk0);
-              lval[lo + nl * cnt + p] = cval[ix];
-              ++nl;
-            } else if (cj > c) {
-              lslot[uo + nu * cnt + p] = (short)(j - blk0);
-              lval[uo + nu * cnt + p] = cval[ix];
-              ++nu;
-            }
-          }
-          for (; nl < wl; ++nl) {
-            lslot[lo + nl * cnt + p] = -1;
-            lval[lo + nl * cnt + p] = (T)0;
-          }
-          for (; nu < wu; ++nu) {
-            lslot[uo + nu * cnt + p] = -1;
-            lval[uo + nu * cnt + p] = (T)0;
-          }
+          spos[slot] = (short)pos;
         }
         pos0 += __popc(m);
       }
+    }
+    __syncthreads();
+    // each row's column of its colour's lists
+    for (int q = 0; q < Qb; ++q) {
+      const int row = row0 + q * R;
+      if (row >= n) break;
+      const int slot = q * B + t, ci = srowc[slot];
+      const int p = spos[slot] - s->coff[ci], cnt = s->coff[ci + 1] - s->coff[ci];
+      LEnt<T>* ll = lent + s->loff[ci] + p;
+      LEnt<T>* lu = lent + s->uoff[ci] + p;
+      const T mi = os[(size_t)slot * OwnRef<T, K>::kLen + kQminv * K];
+      const int wq = s->wmax[q], bq = s->base[q] + t;
+      int nl = 0, nu = 0;
+      for (int e = 0; e < wq; ++e) {
+        const int ix = bq + e * B;
+        const int j = ccol[ix];
+        if (j < blk0 || j >= blk0 + rb_n || j == row) continue;
+        const int cj = srowc[j - blk0];
+        const LEnt<T> en{(int)spos[j - blk0], mi * cval[ix]};
+        if (cj < ci) ll[(size_t)nl++ * cnt] = en;
+        else if (cj > ci) lu[(size_t)nu++ * cnt] = en;
+      }
+      for (; nl < s->wl[ci]; ++nl) ll[(size_t)nl * cnt] = LEnt<T>{-1, (T)0};
+      for (; nu < s->wu[ci]; ++nu) lu[(size_t)nu * cnt] = LEnt<T>{-1, (T)0};
     }
     __syncthreads();
   }
@@ -668,6 +659,12 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
           o(kQz, c) = u[c];
           rr[c] += rv * rv;
         }
+        if (fast_ssor) {  // the block sweeps start from M^-1 r
+          T v[K];
+#pragma unroll
+          for (int c = 0; c < K; ++c) v[c] = u[c];
+          store_m<T, K>(sv, spos[q * B + t], v);
+        }
         // both forms' first gathers: u = M^-1 r (pipelined, to m0) and
         // z = M^-1 r (classic, to m2; after the block sweeps with block SSOR)
         if (!bssor) {
@@ -680,14 +677,20 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
       }
       if (bssor) {
         __syncthreads();
-        ssor_apply(false);
+        ssor_apply();
         for (int q = 0; q < Qb; ++q) {
           const int row = row0 + q * R;
           if (row >= n) break;
           const OwnRef<T, K> o = own_ref(q, row);
           T m[K];
+          if (fast_ssor) {
+            load_m<T, K>(sv, spos[q * B + t], m);
 #pragma unroll
-          for (int c = 0; c < K; ++c) m[c] = o(kQz, c);
+            for (int c = 0; c < K; ++c) o(kQz, c) = m[c];
+          } else {
+#pragma unroll
+            for (int c = 0; c < K; ++c) m[c] = o(kQz, c);
+          }
           store_m<T, K>(mb0, row, m);
           store_m<T, K>(mb2, row, m);
         }
@@ -1012,8 +1015,6 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
           if (row >= n) break;
           const OwnRef<T, K> o = own_ref(q, row);
           const T mi = o(kQminv, 0);
-          // block SSOR: a colour-0 row's y (and z, with one colour) needs no neighbour
-          const bool y0 = fast_ssor && srowc[q * B + t] == 0;
           T rec[K];
 #pragma unroll
           for (int c = 0; c < K; ++c) {
@@ -1027,24 +1028,28 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
               rec[c] = z;
               d2[c] += r * z;
               d2[K + c] += r * r;
-            } else if (y0) {
-              o(kQs, c) = mi * r;
-              if (s->ncb == 1) o(kQz, c) = mi * r;
+            } else {
+              rec[c] = mi * r;  // block SSOR: the sweeps start from M^-1 r
             }
           }
           if (!bssor) store_m<T, K>(rnext, row, rec);
+          else if (fast_ssor) store_m<T, K>(sv, spos[q * B + t], rec);
         }
         if (bssor) {  // z = M^-1 r by the block sweeps, then the records and the dots
           __syncthreads();
-          ssor_apply(true);
+          ssor_apply();
           for (int q = 0; q < Qb; ++q) {
             const int row = row0 + q * R;
             if (row >= n) break;
             const OwnRef<T, K> o = own_ref(q, row);
+            T zf[K];
+            if (fast_ssor) load_m<T, K>(sv, spos[q * B + t], zf);
             T rec[K];
 #pragma unroll
             for (int c = 0; c < K; ++c) {
-              const T r = o(kQr, c), z = o(kQz, c);
+              const T r = o(kQr, c);
+              if (fast_ssor) o(kQz, c) = zf[c];
+              const T z = o(kQz, c);
               rec[c] = z;
               d2[c] += r * z;
               d2[K + c] += r * r;
@@ -1269,8 +1274,10 @@ void pipelined_smem_need(const int* A_ptr, const int* A_col, int n, int grid, in
       }
       size_t lents = 0;
       for (int k = 0; k < kMaxColours; ++k) lents += (size_t)cnt[k] * (wl[k] + wu[k]);
-      extra = align16((size_t)Qb * block) + align16((size_t)Qb * block * sizeof(short)) +
-              align16(lents * sizeof(short)) + align16(lents * vs);
+      // (LEnt: 8 bytes in FP32, 16 in FP64; the sweep vector padded to 16 bytes a row)
+      const size_t wpad = ((size_t)K * vs + 15) / 16 * 16;
+      extra = align16((size_t)Qb * block) + align16((size_t)Qb * block * sizeof(short)) + align16(lents * 2 * vs) +
+              (size_t)Qb * (size_t)block * wpad;
     }
     wf = std::max(wf, c + align16((size_t)(6 * K + 1) * (size_t)Qb * (size_t)block * vs) + extra);
   }
