@@ -180,6 +180,17 @@ def algorithmic_bytes_classic(info, stats, k, mixed):
     return stats.iterations * b_iter + (stats.refinements + 1) * b_res + b_rhs
 
 
+def algorithmic_bytes_bssor(info, stats, k, mixed):
+    """The two-reduction PCG with block SSOR: the Jacobi form's bytes plus,
+    per inner iteration, the two triangular sweeps over the off-diagonal
+    entries (scaled value and neighbour index) with a read and a write of the
+    sweep vector in each."""
+    n, nnz = info["n_free"], info["nnz_A"]
+    sv = 4 if mixed else 8
+    sweeps = (nnz - n) * (sv + 4) + 4 * n * k * sv
+    return algorithmic_bytes_classic(info, stats, k, mixed) + stats.iterations * sweeps
+
+
 def cpu_baseline(pos, tris, h, t, seconds=12.0):
     """The oracle's FP64 IC(0)-PCG (the reference's CPU path restated), columns
     on parallel threads; bounded sample of whole solves."""
@@ -465,9 +476,12 @@ def main():
     m, h, t = synth.config2()
     tris, parent = cut_mesh(m.positions.shape[0], m.tris, m.loops)
     pos = np.ascontiguousarray(m.positions[parent])
-    # the headline path: Jacobi preconditioner, pipelined CG (one team barrier
-    # per iteration, rows of A and the own-row state in shared memory)
-    solver = CutMeshSolver(pos, tris, h, device=local, precond="jacobi")
+    # the headline path: block SSOR preconditioner, two-reduction CG on the
+    # row-cached kernel (rows of A, the CG state and the colour lists in
+    # shared memory), mixed precision; Jacobi (FP64 pipelined, FP64 plain,
+    # mixed) and IC(0) beside it
+    solver = CutMeshSolver(pos, tris, h, device=local, precond="bssor")
+    solver_j = CutMeshSolver(pos, tris, h, device=local, precond="jacobi")
     solver_ic = CutMeshSolver(pos, tris, h, device=local, precond="ic0")
     info = solver.info()
     info_ic = solver_ic.info()
@@ -485,11 +499,12 @@ def main():
 
     # reference statistics of each variant (same inputs, cold start)
     st_mixed = one("mixed", stats=True)
-    st_fp64 = one("fp64", stats=True)
-    st_plain = one("fp64", "plain", stats=True)
+    st_fp64 = one("fp64", stats=True, sv=solver_j)
+    st_plain = one("fp64", "plain", stats=True, sv=solver_j)
     st_ic = one("mixed", stats=True, sv=solver_ic)
-    st_classic = one("mixed", "pipelined", stats=True)
-    for s in (st_mixed, st_fp64, st_plain, st_ic, st_classic):
+    st_jac = one("mixed", stats=True, sv=solver_j)
+    st_classic = one("mixed", "pipelined", stats=True, sv=solver_j)
+    for s in (st_mixed, st_fp64, st_plain, st_ic, st_jac, st_classic):
         if s.status != 0:
             raise SystemExit(f"solve failed: status {s.status}")
 
@@ -518,10 +533,11 @@ def main():
     clocks.start()
     t_mixed = timed("mixed", "fused", args.steps, args.warmup)
     clk = clocks.stop()
-    t_fp64 = timed("fp64", "fused", max(3, args.steps // 3), 2)
-    t_plain = timed("fp64", "plain", 3, 1)
+    t_fp64 = timed("fp64", "fused", max(3, args.steps // 3), 2, sv=solver_j)
+    t_plain = timed("fp64", "plain", 3, 1, sv=solver_j)
     t_ic = timed("mixed", "fused", max(3, args.steps // 3), 2, sv=solver_ic)
-    t_classic = timed("mixed", "pipelined", max(3, args.steps // 3), 2)
+    t_jac = timed("mixed", "fused", max(3, args.steps // 3), 2, sv=solver_j)
+    t_classic = timed("mixed", "pipelined", max(3, args.steps // 3), 2, sv=solver_j)
 
     # e2e: host (pinned) buffers through cn_solve, H2D of the targets and D2H of
     # the deformed positions inside the timed region
@@ -560,16 +576,17 @@ def main():
     ms_plain = maxred(sum(t_plain) / len(t_plain))
     ms_e2e = maxred(sum(e2e_ms) / len(e2e_ms))
     ms_ic = maxred(sum(t_ic) / len(t_ic))
+    ms_jac = maxred(sum(t_jac) / len(t_jac))
     ms_classic = maxred(sum(t_classic) / len(t_classic))
     peak, peak_kind = load_peaks()
-    bytes_mixed = algorithmic_bytes_classic(info, st_mixed, k, True)
+    bytes_mixed = algorithmic_bytes_bssor(info, st_mixed, k, True)
     bytes_fp64 = algorithmic_bytes_pipelined(info, st_fp64, k, False)
     ach = bytes_mixed / (ms_mixed * 1e-3) / 1e9
     traffic = None
     try:
         with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
             tj = json.load(f)
-        traffic = tj.get("cn_pipe_solve_mixed", {}).get("dram_bytes_per_launch")
+        traffic = tj.get("cn_pipe_solve_bssor_mixed", {}).get("dram_bytes_per_launch")
     except Exception:
         pass
     spmv = None
@@ -581,6 +598,7 @@ def main():
     batch = None
     if not args.no_batch:
         solver.close()
+        solver_j.close()
         solver_ic.close()
         batch = batch_section(torch, dist, world, rank, local, max(3, args.steps // 6), 2)
     if rank == 0:
@@ -599,13 +617,17 @@ def main():
             "dtype": "f32 inner / f64 residual",
             "data": "synthetic (seeded torus, see tool_godot_curvenet_b200/synth.py config2)",
             "config": {"workload": WORKLOAD, "n_verts": nv, "n_free": info["n_free"], "nnz_A": info["nnz_A"],
-                       "rhs": k, "tol": 1e-8, "precond": "Jacobi, natural row order; two-reduction CG on the row-cached kernel (rows of A and the CG state in shared memory)",
+                       "rhs": k, "tol": 1e-8, "precond": "block SSOR (blocks = the rows each CTA owns, DSatur colours inside a block), natural row order; two-reduction CG on the row-cached kernel (rows of A, the CG state and the colour lists in shared memory)",
                        "launch": f"grid {info['grid']} x block auto (2 rows per thread)", "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
                        "l2": "flushed (256 MB read) before every timed solve, outside the events"},
             "mixed": {"iterations": st_mixed.iterations, "refinements": st_mixed.refinements,
                       "max_rel_residual": st_mixed.max_rel_residual},
             "fp64_fused": {"solves_per_s": 1e3 / ms_fp64, "ms": ms_fp64, "iterations": st_fp64.iterations,
-                           "max_rel_residual": st_fp64.max_rel_residual},
+                           "max_rel_residual": st_fp64.max_rel_residual,
+                           "note": "Jacobi, pipelined CG in FP64 on the row-cached kernel"},
+            "jacobi_mixed": {"solves_per_s": 1e3 / ms_jac, "ms": ms_jac, "iterations": st_jac.iterations,
+                             "refinements": st_jac.refinements,
+                             "note": "Jacobi, two-reduction CG on the same kernel"},
             "fp64_plain": {"solves_per_s": 1e3 / ms_plain, "ms": ms_plain, "iterations": st_plain.iterations,
                            "note": "Jacobi-PCG, one kernel per primitive, dots folded on the host each iteration"},
             "ic0_mixed": {"solves_per_s": 1e3 / ms_ic, "ms": ms_ic, "iterations": st_ic.iterations,
@@ -618,7 +640,7 @@ def main():
             "speedup_mixed_vs_fp64_fused": ms_fp64 / ms_mixed,
             "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
                          "peak_kind": peak_kind, "traffic": traffic,
-                         "kernel": f"k_pipe_grid<float,3,2> (row-cached persistent solve, grid {info['grid']})",
+                         "kernel": f"k_pipe_grid<float,3,2> (row-cached persistent solve, block SSOR, grid {info['grid']})",
                          "note": "rows of A and the own-row state stay in shared memory, the gathered vectors in L2: DRAM traffic per launch is a small fraction of the algorithmic bytes; latency-bound (team barriers and L2 round trips)",
                          "algorithmic_bytes_per_launch": bytes_mixed,
                          "fp64_fused_achieved": bytes_fp64 / (ms_fp64 * 1e-3) / 1e9},
@@ -638,6 +660,7 @@ def main():
             line["cpu_baseline"] = cpu_baseline(pos, tris, h, t)
         print(json.dumps(line), flush=True)
     solver.close()
+    solver_j.close()
     solver_ic.close()
     if world > 1:
         dist.destroy_process_group()
