@@ -241,11 +241,13 @@ __device__ void solve_body_wide(const SolveArgs& a, const ClusterTeam& team, Sme
                                    },
                                    acc);
           } else {
+            // A p = A z + beta A p_old: only z is gathered, A p_old is this
+            // row's own entry of Ap
             gather_row<CPL, 1, UW>(a.A_ptr[row], a.A_ptr[row + 1], 0, a.A_col, Aval,
                                    [&](int j, T* x) {
                                      const size_t jb = (size_t)j * K + c0;
 #pragma unroll
-                                     for (int c = 0; c < CPL; ++c) x[c] = z[jb + c] + beta[c] * pold[jb + c];
+                                     for (int c = 0; c < CPL; ++c) x[c] = z[jb + c];
                                    },
                                    acc);
           }
@@ -253,9 +255,10 @@ __device__ void solve_body_wide(const SolveArgs& a, const ClusterTeam& team, Sme
           for (int c = 0; c < CPL; ++c) {
             const size_t ix = (size_t)row * K + c0 + c;
             const T pi = b0 ? z[ix] : z[ix] + beta[c] * pold[ix];
+            const T api = b0 ? acc[c] : acc[c] + beta[c] * Ap[ix];
             pnew[ix] = pi;
-            Ap[ix] = acc[c];
-            pap[c] += (double)pi * (double)acc[c];
+            Ap[ix] = api;
+            pap[c] += (double)pi * (double)api;
           }
         }
         block_reduce_wide<K, C>(pap, s->red, s->part[kPAP]);
@@ -304,11 +307,10 @@ __device__ void solve_body_wide(const SolveArgs& a, const ClusterTeam& team, Sme
             const T yv = (rv - acc[c]) * di;
             y[ix] = yv;
             rrp[c] += (double)rv * (double)rv;
-            if (last) {
-              const T zv = yv * di;
-              z[ix] = zv;
-              rzp[c] += (double)rv * (double)zv;
-            }
+            // (r, M^-1 r) = (L y, L^-T y) = ||y||^2 with M = L L^T, y = L^-1 r:
+            // the backward sweep need not read r again
+            rzp[c] += (double)yv * (double)yv;
+            if (last) z[ix] = yv * di;
           }
         }
         if (!last) team.sync();
@@ -331,9 +333,7 @@ __device__ void solve_body_wide(const SolveArgs& a, const ClusterTeam& team, Sme
 #pragma unroll
           for (int c = 0; c < CPL; ++c) {
             const size_t ix = (size_t)row * K + c0 + c;
-            const T zv = (y[ix] - acc[c]) * di;
-            z[ix] = zv;
-            rzp[c] += (double)r[ix] * (double)zv;
+            z[ix] = (y[ix] - acc[c]) * di;
           }
         }
       }
