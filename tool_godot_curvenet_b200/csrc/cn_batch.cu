@@ -215,6 +215,10 @@ __device__ void solve_body_wide(const SolveArgs& a, const ClusterTeam& team, Sme
 
     int it = 0;
     bool first = true;
+    // x += alpha p of an iteration is applied where that p is read next: in
+    // the following iteration's SpMV pass, or after the loop for the last one
+    const T* plast = nullptr;
+    T alast[CPL];
     for (;;) {
       if (!first) {
         double pap[CPL];
@@ -228,6 +232,9 @@ __device__ void solve_body_wide(const SolveArgs& a, const ClusterTeam& team, Sme
         const bool b0 = it == 0;
         const T* pold = (it & 1) ? pb : pa;
         T* pnew = (it & 1) ? pa : pb;
+        T aprev[CPL];
+#pragma unroll
+        for (int c = 0; c < CPL; ++c) aprev[c] = (T)s->alpha[c0 + c];
         for (int row = row0; row < n; row += rstride) {
           T acc[CPL];
 #pragma unroll
@@ -254,7 +261,12 @@ __device__ void solve_body_wide(const SolveArgs& a, const ClusterTeam& team, Sme
 #pragma unroll
           for (int c = 0; c < CPL; ++c) {
             const size_t ix = (size_t)row * K + c0 + c;
-            const T pi = b0 ? z[ix] : z[ix] + beta[c] * pold[ix];
+            T pi = z[ix];
+            if (!b0) {
+              const T po = pold[ix];
+              xin[ix] += aprev[c] * po;  // the previous iteration's x update
+              pi += beta[c] * po;
+            }
             const T api = b0 ? acc[c] : acc[c] + beta[c] * Ap[ix];
             pnew[ix] = pi;
             Ap[ix] = api;
@@ -300,7 +312,6 @@ __device__ void solve_body_wide(const SolveArgs& a, const ClusterTeam& team, Sme
             const size_t ix = (size_t)row * K + c0 + c;
             T rv = r[ix];
             if (!first) {
-              xin[ix] += alpha[c] * pcur[ix];
               rv -= alpha[c] * Ap[ix];
               r[ix] = rv;
             }
@@ -363,6 +374,9 @@ __device__ void solve_body_wide(const SolveArgs& a, const ClusterTeam& team, Sme
       }
       __syncthreads();
       if (!first) {
+        plast = pcur;
+#pragma unroll
+        for (int c = 0; c < CPL; ++c) alast[c] = alpha[c];
         ++it;
         ++total_iters;
       }
@@ -374,7 +388,9 @@ __device__ void solve_body_wide(const SolveArgs& a, const ClusterTeam& team, Sme
 #pragma unroll
       for (int c = 0; c < CPL; ++c) {
         const size_t ix = (size_t)row * K + c0 + c;
-        a.x64[ix] += (double)xin[ix];
+        T xv = xin[ix];
+        if (plast) xv += alast[c] * plast[ix];  // the last iteration's x update
+        a.x64[ix] += (double)xv;
       }
     }
     team.sync();
