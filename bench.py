@@ -241,7 +241,7 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-def batch_section(torch, dist, world, rank, local, steps, warmup):
+def batch_section(torch, dist, world, rank, local, steps, warmup, n_meshes=512):
     """The batched workload (512 meshes, cylinder or torus, n_v log-uniform in
     [2k, 60k], 1-4 seams, 8 poses x 3 RHS, mixed precision to 1e-8) in one
     persistent CUDA-graph launch per batch; with N ranks the meshes are
@@ -249,7 +249,6 @@ def batch_section(torch, dist, world, rank, local, steps, warmup):
     share."""
     from tool_godot_curvenet_b200 import BatchSolver, cut_mesh, synth
     from tool_godot_curvenet_b200.shard import mesh_cost, rank_share, reduce_over_ranks
-    n_meshes = 512
     specs = [synth.config3_mesh(i) for i in range(n_meshes)]
     costs = [mesh_cost(m.positions.shape[0] + sum(len(l) for l in m.loops), m.tris.shape[0]) for m, _, _ in specs]
     mine = rank_share(costs, world, rank)
@@ -317,7 +316,7 @@ def batch_section(torch, dist, world, rank, local, steps, warmup):
     nnz = info["nnz_A"]
     n = info["n_free"]
     return {
-        "workload": "512 meshes (cylinder|torus, n_v log-uniform [2k,60k], 1-4 seams, 2% handles) x 8 poses x 3 RHS",
+        "workload": f"{n_meshes} meshes (cylinder|torus, n_v log-uniform [2k,60k], 1-4 seams, 2% handles) x 8 poses x 3 RHS",
         "n_meshes": n_meshes, "meshes_this_rank": len(mine), "n_verts_rank0": info["n_verts"],
         "nnz_A_rank0": nnz, "n_free_rank0": n,
         "cluster_size": info["cluster_size"], "n_clusters": info["n_clusters"], "block": info["block"],
@@ -455,6 +454,8 @@ def main():
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-spmv", action="store_true")
     ap.add_argument("--no-ddm", action="store_true")
+    ap.add_argument("--batch-meshes", type=int, default=512,
+                    help="meshes of the batched workload (the first N of the 512-mesh set; 512 is the benchmark)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -600,7 +601,7 @@ def main():
         solver.close()
         solver_j.close()
         solver_ic.close()
-        batch = batch_section(torch, dist, world, rank, local, max(3, args.steps // 6), 2)
+        batch = batch_section(torch, dist, world, rank, local, max(3, args.steps // 6), 2, args.batch_meshes)
     if rank == 0:
         x = d_x.cpu().numpy()
         line = {

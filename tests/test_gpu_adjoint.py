@@ -122,3 +122,19 @@ def test_identity_curves_give_rest_pose():
     d = deformer()
     x = d.deform(rest_cp, np.ones(rest_cp.shape[0]), tol=TOL)
     assert np.abs(x - pos).max() < 1e-9
+
+
+def test_adjoint_with_block_ssor_matches_default():
+    """The adjoint solve of a block-SSOR handle (a different preconditioner,
+    the same A) gives the gradient of the default handle."""
+    from tool_godot_curvenet_b200.autograd import CurveDeformer
+    pos, tris, h, cof, tau, rest_cp, P, w, _, _ = problem()
+    loss, dP, dw = loss_and_grad(P, w)
+    d2 = CurveDeformer(pos, tris, h, cof, tau, rest_cp, precond="bssor")
+    xt = target()
+    x = d2.deform(P, w, tol=TOL)
+    g = x - xt
+    dP2, dw2 = d2.adjoint(g, tol=TOL)
+    a = np.concatenate([dP.ravel(), dw])
+    b = np.concatenate([dP2.ravel(), dw2])
+    assert np.linalg.norm(a - b) <= 1e-8 * np.linalg.norm(a)

@@ -88,3 +88,22 @@ def test_batch_matches_single_mesh_solver():
             for p in range(8):
                 r = s.solve(t[:, 3 * p:3 * p + 3], precision="fp64", tol=1e-12)
                 assert rel_err(xb[:, 3 * p:3 * p + 3], r.x) <= 1e-9
+
+
+@pytest.mark.parametrize("precond", ["jacobi", "ic0"])
+def test_batch_preconditioners_converge_to_oracle(precond):
+    """Both batch preconditioners (the inner dot (r, M^-1 r) is taken as
+    ||L^-1 r||^2 from the forward sweep; A p by the recurrence A z + beta A p';
+    x += alpha p one pass late) reach the oracle's solution in FP64 and mixed
+    precision, including a run with too few iterations that must report
+    max_iter rather than a wrong answer."""
+    meshes = small_batch()
+    ref = oracle_solutions()
+    with BatchSolver([(p, t, h) for p, t, h, _ in meshes], k=24, precond=precond) as B:
+        for precision, tol, bar in [("fp64", 1e-13, FP64_TOL), ("mixed", 1e-8, MIXED_TOL)]:
+            xs, st = B.solve([m[3] for m in meshes], precision=precision, tol=tol, max_iter=20000)
+            assert st.status == 0 and st.max_rel_residual <= tol
+            for x, xo in zip(xs, ref):
+                assert rel_err(x, xo) <= bar
+        xs, st = B.solve([m[3] for m in meshes], precision="fp64", tol=1e-13, max_iter=3, check=False)
+        assert st.n_failed > 0

@@ -211,7 +211,7 @@ def test_max_iter_reported():
     assert r.status == L.CN_MAX_ITER
 
 
-@pytest.mark.parametrize("precond", ["ic0", "jacobi"])
+@pytest.mark.parametrize("precond", ["ic0", "jacobi", "bssor"])
 def test_autotuner_picks_a_shape_that_solves(precond, oracle, tmp_path):
     import torch
 
