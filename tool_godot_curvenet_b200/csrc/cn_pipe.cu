@@ -1,10 +1,17 @@
-// cn_pipe.cu -- the pipelined Jacobi-PCG persistent solve (sm_100a).
+// cn_pipe.cu -- the row-cached persistent PCG solve (sm_100a): Jacobi or
+// block SSOR, two CG forms.
 //
 // Same problem, right-hand sides, FP64 residual refinement and output as the
-// classic persistent solve (cn_pcg.cu); the inner solve is the pipelined
-// preconditioned CG of Ghysels & Vanroose ("Hiding global synchronization
-// latency in the preconditioned Conjugate Gradient algorithm", Parallel
-// Computing 40, 2014, Alg. 4) with the Jacobi preconditioner M = diag(A):
+// level-scheduled persistent solve (cn_pcg.cu).  Each thread owns the rows
+// b Qg B + q B + t (q < Qg) of its block b for the whole launch, and the
+// block keeps its rows of A (column index and T value) in shared memory (one
+// ELL slice per row slice, column-major, padding column -1) and, when it
+// fits, their CG state, so a row costs one L2 round trip (the gathers of the
+// vector its neighbours need) per phase.
+//
+// Pipelined form (Jacobi only): the preconditioned CG of Ghysels & Vanroose
+// ("Hiding global synchronization latency in the preconditioned Conjugate
+// Gradient algorithm", Parallel Computing 40, 2014, Alg. 4) with M = diag(A):
 //
 //   gamma = (r, u), delta = (w, u)               one reduction per iteration
 //   m = M^-1 w ; n = A m                         overlaps that reduction
@@ -13,27 +20,24 @@
 //   x += alpha p ; r -= alpha s ; w -= alpha z ; u = M^-1 r
 //
 // (with a diagonal M the recurrences u -= alpha q, q = m + beta q of the
-// general form reduce to u = M^-1 r, so q is not kept).  The classic form
-// needs two reductions per iteration (p.Ap before the update, r.z after it),
-// hence two team barriers; here an iteration is ONE phase between two
-// barriers:
-//   after the barrier a block issues the gathers of m (its rows' neighbours,
-//   written by their owners in the previous phase) and the loads of its own
-//   rows' state, and, in the same memory round trip, three warps sum the
-//   previous phase's partials (gamma, delta, ||r||^2 per column, a fixed
-//   order, so every block derives the same alpha, beta and stopping
-//   decision); the own rows update, store m' = M^-1 w' into the other copy
-//   of m, and the block's partial sums of (gamma', delta', ||r'||^2) are
-//   written before the next barrier.
-// Each thread owns the rows b Qg B + q B + t (q < Qg) of its block b for the
-// whole launch, and the block keeps its rows of A (column index and T value) in
-// shared memory (one ELL slice per row slice, column-major, padding column
-// -1), so a row costs one L2 round trip (the gathers of m) per phase.
+// general form reduce to u = M^-1 r, so q is not kept).  An iteration is ONE
+// phase between two team barriers: after the barrier a block issues the
+// gathers of m (its rows' neighbours, written by their owners in the
+// previous phase) and, in the same memory round trip, three warps sum the
+// previous phase's partials (gamma, delta, ||r||^2 per column, a fixed
+// order, so every block derives the same alpha, beta and stopping decision);
+// the own rows update, store m' = M^-1 w' into the other copy of m, and the
+// block's partial sums are written before the next barrier.
+//
+// Two-reduction form (Jacobi or block SSOR): phase S gathers z, forms
+// p = z + beta p' and A p = A z + beta A p', (p, Ap); phase U updates x and
+// r, applies z = M^-1 r (inline for Jacobi, by the block's colour sweeps in
+// shared memory for block SSOR), (r, z) and ||r||^2.
+//
 // Partial sums alternate between two slot groups by phase parity (a block
 // may write phase i+1's partials while a slower block still reads phase i's);
-// m alternates between two buffers for the same reason.
+// the gathered vectors alternate between two buffers for the same reason.
 #include <algorithm>
-
 #include <set>
 #include <tuple>
 #include <vector>
