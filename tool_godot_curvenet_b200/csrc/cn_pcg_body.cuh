@@ -328,32 +328,26 @@ __device__ void solve_body(const SolveArgs& a, const Team& team, Smem<K>* s) {
           T acc[K];
 #pragma unroll
           for (int c = 0; c < K; ++c) acc[c] = (T)0;
-          if (b0) {
-            gather_row<K, G, UR>(a.A_ptr[row], a.A_ptr[row + 1], sub, a.A_col, Aval,
-                                 [&](int j, T* x) {
+          // A p = A z + beta A p_old: only z is gathered, A p_old is the
+          // row's own entry of Ap
+          gather_row<K, G, UR>(a.A_ptr[row], a.A_ptr[row + 1], sub, a.A_col, Aval,
+                               [&](int j, T* x) {
 #pragma unroll
-                                   for (int c = 0; c < K; ++c) x[c] = z[(size_t)j * K + c];
-                                 },
-                                 acc);
-          } else {
-            gather_row<K, G, UR>(a.A_ptr[row], a.A_ptr[row + 1], sub, a.A_col, Aval,
-                                 [&](int j, T* x) {
-#pragma unroll
-                                   for (int c = 0; c < K; ++c)
-                                     x[c] = z[(size_t)j * K + c] + beta[c] * pold[(size_t)j * K + c];
-                                 },
-                                 acc);
-          }
+                                 for (int c = 0; c < K; ++c) x[c] = z[(size_t)j * K + c];
+                               },
+                               acc);
 #pragma unroll
           for (int c = 0; c < K; ++c) acc[c] = group_sum<G>(acc[c], gmask);
           if (sub == 0) {
 #pragma unroll
             for (int c = 0; c < K; ++c) {
-              T pi = z[(size_t)row * K + c];
-              if (!b0) pi += beta[c] * pold[(size_t)row * K + c];
-              pnew[(size_t)row * K + c] = pi;
-              Ap[(size_t)row * K + c] = acc[c];
-              pap[c] += (double)pi * (double)acc[c];
+              const size_t ix = (size_t)row * K + c;
+              T pi = z[ix];
+              if (!b0) pi += beta[c] * pold[ix];
+              const T api = b0 ? acc[c] : acc[c] + beta[c] * Ap[ix];
+              pnew[ix] = pi;
+              Ap[ix] = api;
+              pap[c] += (double)pi * (double)api;
             }
           }
         }
@@ -529,11 +523,10 @@ __device__ void solve_body(const SolveArgs& a, const Team& team, Smem<K>* s) {
               const T yv = (rv - acc[c]) * di;
               y[ix] = yv;
               rrp[c] += (double)rv * (double)rv;
-              if (last) {
-                const T zv = yv * di;
-                z[ix] = zv;
-                rzp[c] += (double)rv * (double)zv;
-              }
+              // (r, M^-1 r) = (L y, L^-T y) = ||y||^2 with M = L L^T, y = L^-1 r:
+              // the backward sweep need not read r again
+              rzp[c] += (double)yv * (double)yv;
+              if (last) z[ix] = yv * di;
             }
           }
         }
@@ -562,9 +555,7 @@ __device__ void solve_body(const SolveArgs& a, const Team& team, Smem<K>* s) {
 #pragma unroll
             for (int c = 0; c < K; ++c) {
               const size_t ix = (size_t)row * K + c;
-              const T zv = (y[ix] - acc[c]) * di;
-              z[ix] = zv;
-              rzp[c] += (double)r[ix] * (double)zv;
+              z[ix] = (y[ix] - acc[c]) * di;
             }
           }
         }
