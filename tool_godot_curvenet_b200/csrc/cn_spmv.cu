@@ -3,13 +3,17 @@
 // SlangCodegen/SpmvMulti.lean:78-119 (X row-major n x k).
 //
 // Work item: one 16-byte chunk of one output row (4 FP32 or 2 FP64 columns)
-// when k is a multiple of the chunk, else one whole row.  Consecutive threads
+// when k is a multiple of the chunk, else one whole row; the grid holds the
+// blocks resident on the device at once and walks the items grid-stride
+// (one wave: about 17 % faster than one thread per item at k = 24 in FP64).  Consecutive threads
 // take consecutive chunks, so the store of Y and the gather of a neighbour
 // row of X are contiguous across the threads of a row; the row's column
 // indices and values are the same addresses for those threads (one L1
 // transaction).  Eight entries are in flight per thread (indices and values
 // first, then the eight gathers, then the multiply-adds), so a warp keeps
 // enough loads outstanding to stream HBM.
+#include <algorithm>
+
 #include "cn_internal.h"
 
 namespace cn {
@@ -53,60 +57,61 @@ __global__ void __launch_bounds__(256) k_spmm_vec(int n, const int* __restrict__
   constexpr int C = K / V16<T>::W;  // chunks per row
   const long long items = (long long)n * C;
   const long long H = (items + RPT - 1) / RPT;
-  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (tid >= H) return;
   const V* __restrict__ xv = reinterpret_cast<const V*>(x);
-  int row[RPT], ch[RPT], e0[RPT], e1[RPT];
-  bool ok[RPT];
+  for (long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x; tid < H;
+       tid += (long long)gridDim.x * blockDim.x) {
+    int row[RPT], ch[RPT], e0[RPT], e1[RPT];
+    bool ok[RPT];
 #pragma unroll
-  for (int q = 0; q < RPT; ++q) {
-    const long long it = tid + q * H;
-    ok[q] = it < items;
-    row[q] = ok[q] ? (int)(it / C) : 0;
-    ch[q] = ok[q] ? (int)(it - (long long)row[q] * C) : 0;
-  }
+    for (int q = 0; q < RPT; ++q) {
+      const long long it = tid + q * H;
+      ok[q] = it < items;
+      row[q] = ok[q] ? (int)(it / C) : 0;
+      ch[q] = ok[q] ? (int)(it - (long long)row[q] * C) : 0;
+    }
 #pragma unroll
-  for (int q = 0; q < RPT; ++q) {
-    e0[q] = ok[q] ? __ldg(ptr + row[q]) : 0;
-    e1[q] = ok[q] ? __ldg(ptr + row[q] + 1) : 0;
-  }
-  V acc[RPT];
+    for (int q = 0; q < RPT; ++q) {
+      e0[q] = ok[q] ? __ldg(ptr + row[q]) : 0;
+      e1[q] = ok[q] ? __ldg(ptr + row[q] + 1) : 0;
+    }
+    V acc[RPT];
 #pragma unroll
-  for (int q = 0; q < RPT; ++q) {
-    if constexpr (sizeof(T) == 4) acc[q] = make_float4(0.f, 0.f, 0.f, 0.f);
-    else acc[q] = make_double2(0.0, 0.0);
-  }
-  int len = 0;
+    for (int q = 0; q < RPT; ++q) {
+      if constexpr (sizeof(T) == 4) acc[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+      else acc[q] = make_double2(0.0, 0.0);
+    }
+    int len = 0;
 #pragma unroll
-  for (int q = 0; q < RPT; ++q) len = max(len, e1[q] - e0[q]);
-  for (int e = 0; e < len; e += kU) {
-    int j[RPT][kU];
-    T a[RPT][kU];
+    for (int q = 0; q < RPT; ++q) len = max(len, e1[q] - e0[q]);
+    for (int e = 0; e < len; e += kU) {
+      int j[RPT][kU];
+      T a[RPT][kU];
+#pragma unroll
+      for (int q = 0; q < RPT; ++q)
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+          const bool g = e0[q] + e + u < e1[q];
+          j[q][u] = g ? __ldg(col + e0[q] + e + u) : -1;
+          a[q][u] = g ? __ldg(val + e0[q] + e + u) : (T)0;
+        }
+      V xs[RPT][kU];
+#pragma unroll
+      for (int q = 0; q < RPT; ++q)
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+          if (j[q][u] >= 0) xs[q][u] = __ldg(xv + (size_t)j[q][u] * C + ch[q]);
+          else if constexpr (sizeof(T) == 4) xs[q][u] = make_float4(0.f, 0.f, 0.f, 0.f);
+          else xs[q][u] = make_double2(0.0, 0.0);
+        }
+#pragma unroll
+      for (int q = 0; q < RPT; ++q)
+#pragma unroll
+        for (int u = 0; u < kU; ++u) fma16(acc[q], a[q][u], xs[q][u]);
+    }
 #pragma unroll
     for (int q = 0; q < RPT; ++q)
-#pragma unroll
-      for (int u = 0; u < kU; ++u) {
-        const bool g = e0[q] + e + u < e1[q];
-        j[q][u] = g ? __ldg(col + e0[q] + e + u) : -1;
-        a[q][u] = g ? __ldg(val + e0[q] + e + u) : (T)0;
-      }
-    V xs[RPT][kU];
-#pragma unroll
-    for (int q = 0; q < RPT; ++q)
-#pragma unroll
-      for (int u = 0; u < kU; ++u) {
-        if (j[q][u] >= 0) xs[q][u] = __ldg(xv + (size_t)j[q][u] * C + ch[q]);
-        else if constexpr (sizeof(T) == 4) xs[q][u] = make_float4(0.f, 0.f, 0.f, 0.f);
-        else xs[q][u] = make_double2(0.0, 0.0);
-      }
-#pragma unroll
-    for (int q = 0; q < RPT; ++q)
-#pragma unroll
-      for (int u = 0; u < kU; ++u) fma16(acc[q], a[q][u], xs[q][u]);
+      if (ok[q]) reinterpret_cast<V*>(y)[(size_t)row[q] * C + ch[q]] = acc[q];
   }
-#pragma unroll
-  for (int q = 0; q < RPT; ++q)
-    if (ok[q]) reinterpret_cast<V*>(y)[(size_t)row[q] * C + ch[q]] = acc[q];
 }
 
 // Any K: thread = row.
@@ -114,33 +119,44 @@ template <typename T, int K>
 __global__ void __launch_bounds__(256) k_spmm_row(int n, const int* __restrict__ ptr, const int* __restrict__ col,
                                                   const T* __restrict__ val, const T* __restrict__ x,
                                                   T* __restrict__ y) {
-  const int row = blockIdx.x * blockDim.x + threadIdx.x;
-  if (row >= n) return;
-  T acc[K];
+  for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < n; row += gridDim.x * blockDim.x) {
+    T acc[K];
 #pragma unroll
-  for (int c = 0; c < K; ++c) acc[c] = (T)0;
-  const int e0 = ptr[row], e1 = ptr[row + 1];
-  for (int e = e0; e < e1; e += kU) {
-    int j[kU];
-    T a[kU];
+    for (int c = 0; c < K; ++c) acc[c] = (T)0;
+    const int e0 = ptr[row], e1 = ptr[row + 1];
+    for (int e = e0; e < e1; e += kU) {
+      int j[kU];
+      T a[kU];
 #pragma unroll
-    for (int u = 0; u < kU; ++u) {
-      const bool ok = e + u < e1;
-      j[u] = ok ? __ldg(col + e + u) : -1;
-      a[u] = ok ? __ldg(val + e + u) : (T)0;
+      for (int u = 0; u < kU; ++u) {
+        const bool ok = e + u < e1;
+        j[u] = ok ? __ldg(col + e + u) : -1;
+        a[u] = ok ? __ldg(val + e + u) : (T)0;
+      }
+      T xs[kU][K];
+#pragma unroll
+      for (int u = 0; u < kU; ++u)
+#pragma unroll
+        for (int c = 0; c < K; ++c) xs[u][c] = j[u] >= 0 ? __ldg(x + (size_t)j[u] * K + c) : (T)0;
+#pragma unroll
+      for (int u = 0; u < kU; ++u)
+#pragma unroll
+        for (int c = 0; c < K; ++c) acc[c] += a[u] * xs[u][c];
     }
-    T xs[kU][K];
 #pragma unroll
-    for (int u = 0; u < kU; ++u)
-#pragma unroll
-      for (int c = 0; c < K; ++c) xs[u][c] = j[u] >= 0 ? __ldg(x + (size_t)j[u] * K + c) : (T)0;
-#pragma unroll
-    for (int u = 0; u < kU; ++u)
-#pragma unroll
-      for (int c = 0; c < K; ++c) acc[c] += a[u] * xs[u][c];
+    for (int c = 0; c < K; ++c) y[(size_t)row * K + c] = acc[c];
   }
-#pragma unroll
-  for (int c = 0; c < K; ++c) y[(size_t)row * K + c] = acc[c];
+}
+
+// Blocks of 256 threads resident on the whole device at once: the grid of
+// the grid-stride kernels (one wave, no tail of partly filled waves).
+template <typename F>
+int resident_blocks(F kern) {
+  int dev = 0, sms = 148, per = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, 256, 0) != cudaSuccess || per < 1) per = 1;
+  return sms * per;
 }
 
 template <typename T, int K>
@@ -150,9 +166,13 @@ cudaError_t launch_k(int n, const int* ptr, const int* col, const T* val, const 
     constexpr int RPT = 1;
     const long long items = (long long)n * (K / V16<T>::W);
     const long long threads = (items + RPT - 1) / RPT;
-    k_spmm_vec<T, K, RPT><<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(n, ptr, col, val, x, y);
+    static const int slots = resident_blocks(k_spmm_vec<T, K, RPT>);
+    const long long nb = std::min<long long>((threads + 255) / 256, slots);
+    k_spmm_vec<T, K, RPT><<<(unsigned)nb, 256, 0, s>>>(n, ptr, col, val, x, y);
   } else {
-    k_spmm_row<T, K><<<(n + 255) / 256, 256, 0, s>>>(n, ptr, col, val, x, y);
+    static const int slots = resident_blocks(k_spmm_row<T, K>);
+    const long long nb = std::min<long long>((n + 255) / 256, slots);
+    k_spmm_row<T, K><<<(unsigned)nb, 256, 0, s>>>(n, ptr, col, val, x, y);
   }
   return cudaGetLastError();
 }
