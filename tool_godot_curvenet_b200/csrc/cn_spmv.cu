@@ -9,9 +9,11 @@
 // take consecutive chunks, so the store of Y and the gather of a neighbour
 // row of X are contiguous across the threads of a row; the row's column
 // indices and values are the same addresses for those threads (one L1
-// transaction).  Eight entries are in flight per thread (indices and values
-// first, then the eight gathers, then the multiply-adds), so a warp keeps
-// enough loads outstanding to stream HBM.
+// transaction).  Four entries are in flight per thread (indices and values
+// first, then the four gathers, then the multiply-adds): the kernel then fits
+// in 32 registers, so every SM holds 2048 threads, which keeps more loads
+// outstanding than eight entries per thread at 40-48 registers did
+// (k = 24: 46 % -> 56 % of the copy bandwidth).
 #include <algorithm>
 
 #include "cn_internal.h"
@@ -43,7 +45,7 @@ __device__ __forceinline__ void fma16(double2& acc, double a, const double2& x) 
   acc.y += a * x.y;
 }
 
-constexpr int kU = 8;
+constexpr int kU = 4;
 
 // K a multiple of the chunk width: thread = (row, chunk) for RPT items
 // h, h + H, ... (H = items / RPT rounded up), all of whose loads are issued
