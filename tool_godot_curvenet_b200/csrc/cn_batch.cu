@@ -117,7 +117,10 @@ __device__ void solve_body_wide(const SolveArgs& a, const ClusterTeam& team, Sme
   const int row0 = team.rank() * gpb + grp, rstride = team.size() * gpb;
   const int csize = team.size();
   int status = CN_OK, total_iters = 0, refinements = 0;
-  constexpr int UW = 4;  // entries of a row gathered together
+  // entries of a row gathered together: FP32 runs three 512-thread CTAs per
+  // SM (40 registers; more clusters in flight hide more of the HBM latency
+  // than wider gathers), FP64 two (64 registers)
+  constexpr int UW = sizeof(T) == 4 ? 2 : 4;
 
   // ---- right-hand side (HarmonicSolve.lean:51-66 / DeformSolve.lean:123-135)
   {
@@ -421,7 +424,7 @@ done:
 }
 
 template <typename T, int K, int C>
-__global__ void __launch_bounds__(512, 2) k_batch(BatchArgs ba) {
+__global__ void __launch_bounds__(512, sizeof(T) == 4 ? 3 : 2) k_batch(BatchArgs ba) {
   __shared__ SmemW<K> s;
   __shared__ int s_mesh;
   cg::cluster_group cl = cg::this_cluster();

@@ -35,6 +35,7 @@ struct cn_batch {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   cn_build_opts opts{};
   int K = 24, csize = 4, nclusters = 0, block = 512, max_n = 0, nm = 0;
+  int ncl_prec[2] = {0, 0};  // clusters launched per precision (CN_PREC_*), <= nclusters (the scratch)
   std::vector<MeshHost> H;
   std::vector<MeshDev> D;
   std::vector<long long> tgt_off, out_off;
@@ -165,13 +166,17 @@ cn_status cn_build_batch(const cn_mesh_desc* meshes, int32_t n_meshes, const cn_
   // launch shape: clusters of csize blocks, as many as are co-resident
   B->block = o.block > 0 ? o.block : 512;
   B->csize = cluster_size > 0 ? cluster_size : 4;
-  const int mc = std::min(cn::batch_max_clusters(CN_PREC_MIXED, k, B->csize, B->block),
-                          cn::batch_max_clusters(CN_PREC_FP64, k, B->csize, B->block));
-  if (mc <= 0) {
+  // each precision launches as many clusters as are co-resident for its kernel
+  // (FP32 fits more per SM); the per-cluster scratch is sized for the larger
+  const int mc64 = cn::batch_max_clusters(CN_PREC_FP64, k, B->csize, B->block);
+  const int mc32 = cn::batch_max_clusters(CN_PREC_MIXED, k, B->csize, B->block);
+  if (mc64 <= 0 || mc32 <= 0) {
     set_err("no co-resident cluster of %d x %d threads fits this device", B->csize, B->block);
     return fail(CN_CUDA_ERROR);
   }
-  B->nclusters = n_clusters > 0 ? std::min(n_clusters, mc) : mc;
+  B->ncl_prec[CN_PREC_FP64] = n_clusters > 0 ? std::min(n_clusters, mc64) : mc64;
+  B->ncl_prec[CN_PREC_MIXED] = n_clusters > 0 ? std::min(n_clusters, mc32) : mc32;
+  B->nclusters = std::max(B->ncl_prec[CN_PREC_FP64], B->ncl_prec[CN_PREC_MIXED]);
   if (cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreate(&B->ev0) != cudaSuccess || cudaEventCreate(&B->ev1) != cudaSuccess) {
     set_err("stream/event creation failed");
@@ -320,7 +325,8 @@ cn_status cn_solve_batch_device(cn_batch_handle B, const double* d_targets, doub
     cudaGraph_t g = nullptr;
     CN_CUDA(cudaStreamBeginCapture(B->stream, cudaStreamCaptureModeThreadLocal));
     cudaError_t e1 = cudaMemsetAsync(B->d_queue, 0, sizeof(int), B->stream);
-    cudaError_t e2 = cn::launch_batch(ba, o.precision, B->K, B->csize, B->nclusters, B->block, B->stream);
+    cudaError_t e2 = cn::launch_batch(ba, o.precision, B->K, B->csize, B->ncl_prec[o.precision == CN_PREC_MIXED],
+                                      B->block, B->stream);
     cudaError_t e3 = cudaStreamEndCapture(B->stream, &g);
     if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess) {
       set_err("graph capture failed: %s / %s / %s", cudaGetErrorString(e1), cudaGetErrorString(e2),
