@@ -52,6 +52,15 @@ struct cn_system {
   // block SSOR: block-local colours of the rows for blocks of bcolor_rb rows (own allocation)
   unsigned char* d_bcolor = nullptr;
   int bcolor_rb = -1, bncolor = 0;
+  std::vector<unsigned char> h_bcolor;
+  // block SSOR tables in global memory (own allocations): list positions,
+  // sweep vector, lists and each block's first entry, for (bss_rb, bss_grid)
+  int* d_bss_pos = nullptr;
+  void* d_bss_v = nullptr;
+  void* d_bss_lent = nullptr;
+  long long* d_bss_loff = nullptr;
+  long long bss_lent_cap = 0;
+  int bss_loff_cap = 0, bss_rb = -1, bss_grid = -1;
   int* d_status = nullptr;
   // pipelined solve: shared-memory needs of the last (grid, block, precision, k)
   int pipe_grid = -1, pipe_block = -1, pipe_prec = -1, pipe_k = -1;
@@ -401,7 +410,8 @@ void cn_destroy(cn_handle S) {
   for (void* p : {(void*)S->d_curve_of, (void*)S->d_row_of, (void*)S->d_tau, (void*)S->d_rest_cp,
                   (void*)S->d_posed_cp, (void*)S->d_weights, (void*)S->d_dLdx, (void*)S->d_dP, (void*)S->d_dw,
                   (void*)S->d_vf_ptr, (void*)S->d_vf_face, (void*)S->d_vf_corner, (void*)S->d_contrib,
-                  (void*)S->d_Xc, (void*)S->d_bcolor})
+                  (void*)S->d_Xc, (void*)S->d_bcolor, (void*)S->d_bss_pos, S->d_bss_v, S->d_bss_lent,
+                  (void*)S->d_bss_loff})
     if (p) cudaFree(p);
   if (S->ev0) cudaEventDestroy(S->ev0);
   if (S->ev1) cudaEventDestroy(S->ev1);
@@ -592,15 +602,52 @@ cn_status cn_solve_device(cn_handle S, int32_t k, const double* d_targets, doubl
       // block-local colours for the blocks of this launch (rb rows each)
       const long long tot = (long long)(grid > 1 ? grid : 1) * block;
       const int rb = (int)(((long long)S->H.n + tot - 1) / tot * block);
+      const int n = S->H.n;
       if (S->bcolor_rb != rb) {
-        std::vector<unsigned char> col((size_t)std::max(S->H.n, 1));
-        S->bncolor = cn::block_colours(S->H.A_ptr.data(), S->H.A_col.data(), S->H.n, std::max(rb, 1), col.data());
-        if (!S->d_bcolor) CN_CUDA(cudaMalloc((void**)&S->d_bcolor, (size_t)std::max(S->H.n, 1)));
-        if (S->H.n) CN_CUDA(cudaMemcpy(S->d_bcolor, col.data(), (size_t)S->H.n, cudaMemcpyHostToDevice));
+        S->h_bcolor.assign((size_t)std::max(n, 1), 0);
+        S->bncolor = cn::block_colours(S->H.A_ptr.data(), S->H.A_col.data(), n, std::max(rb, 1), S->h_bcolor.data());
+        if (!S->d_bcolor) CN_CUDA(cudaMalloc((void**)&S->d_bcolor, (size_t)std::max(n, 1)));
+        if (n) CN_CUDA(cudaMemcpy(S->d_bcolor, S->h_bcolor.data(), (size_t)n, cudaMemcpyHostToDevice));
         S->bcolor_rb = rb;
       }
       a.bcolor = S->d_bcolor;
       a.bncolor = S->bncolor;
+      // the global tables (used by the blocks whose shared memory cannot hold
+      // them): each block's list entries, prefix-summed
+      const int nb = grid > 1 ? grid : 1;
+      if (S->bss_rb != rb || S->bss_grid != nb) {
+        std::vector<long long> off((size_t)nb + 1, 0);
+        for (int b = 0; b < nb; ++b) {
+          const long long blk0 = (long long)b * rb;
+          const long long rb_n = blk0 < n ? std::min<long long>(n - blk0, rb) : 0;
+          off[b + 1] = off[b] + (rb_n > 0 ? cn::block_list_entries(S->H.A_ptr.data(), S->H.A_col.data(),
+                                                                     S->h_bcolor.data(), blk0, rb_n)
+                                          : 0);
+        }
+        if (!S->d_bss_pos) {
+          CN_CUDA(cudaMalloc((void**)&S->d_bss_pos, sizeof(int) * (size_t)std::max(n, 1)));
+          CN_CUDA(cudaMalloc(&S->d_bss_v, 32 * (size_t)std::max(n, 1)));
+        }
+        if (off[nb] > S->bss_lent_cap || !S->d_bss_lent) {
+          if (S->d_bss_lent) CN_CUDA(cudaFree(S->d_bss_lent));
+          S->d_bss_lent = nullptr;
+          CN_CUDA(cudaMalloc(&S->d_bss_lent, 16 * (size_t)std::max<long long>(off[nb], 1)));
+          S->bss_lent_cap = off[nb];
+        }
+        if (nb + 1 > S->bss_loff_cap) {
+          if (S->d_bss_loff) CN_CUDA(cudaFree(S->d_bss_loff));
+          S->d_bss_loff = nullptr;
+          CN_CUDA(cudaMalloc((void**)&S->d_bss_loff, sizeof(long long) * (size_t)(nb + 1)));
+          S->bss_loff_cap = nb + 1;
+        }
+        CN_CUDA(cudaMemcpy(S->d_bss_loff, off.data(), sizeof(long long) * (size_t)(nb + 1), cudaMemcpyHostToDevice));
+        S->bss_rb = rb;
+        S->bss_grid = nb;
+      }
+      a.bss_pos = S->d_bss_pos;
+      a.bss_v = S->d_bss_v;
+      a.bss_lent = S->d_bss_lent;
+      a.bss_loff = S->d_bss_loff;
     }
     CN_CUDA(cudaMemsetAsync(S->d_ctl, 0, sizeof(Control), S->stream));
     CN_CUDA(cudaEventRecord(S->ev0, S->stream));

@@ -82,6 +82,14 @@ struct SolveArgs {
   int cache_bytes;         // dynamic shared memory (row cache, then own-row state)
   const unsigned char* bcolor;  // block SSOR: block-local colour of every row (null: Jacobi)
   int bncolor;                  // colours
+  // block SSOR tables in global memory, for the blocks whose shared memory
+  // cannot hold them (provided with every block-SSOR launch): list position
+  // per row, the sweep vector (32 bytes a row), the neighbour lists (16 bytes
+  // an entry) and each block's first entry in them
+  int* bss_pos;
+  void* bss_v;
+  void* bss_lent;
+  const long long* bss_loff;
   double* partials;        // [kSlots][grid][K]
   // HSC preconditioner (hsc != 0): rows are in HSC order; F_l = positions
   // [hsc_off[l], hsc_off[l + 1]); the coarse set starts at hsc_off[hsc_L];
@@ -160,6 +168,10 @@ void pipelined_smem_need(const int* A_ptr, const int* A_col, int n, int grid, in
 // row order, over the couplings inside the block (at most 64 colours);
 // returns the number of colours.
 int block_colours(const int* A_ptr, const int* A_col, int n, int rb, unsigned char* col);
+// Entries of the block-SSOR lists of the block of rows [blk0, blk0 + rb_n)
+// (per colour: rows x (widest lower + widest upper in-block neighbour count)).
+long long block_list_entries(const int* A_ptr, const int* A_col, const unsigned char* col, long long blk0,
+                             long long rb_n);
 
 // Build-time kernels (cn_assemble.cu).
 struct BuildArgs {

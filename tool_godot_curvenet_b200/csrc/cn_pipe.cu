@@ -58,6 +58,7 @@ struct MRow {
 
 constexpr int kPipeSplits = 8;  // partial-sum read: up to 8 x 128 blocks
 constexpr int kMaxColours = 64;   // block SSOR: colours of a block (greedy: at most the row length)
+constexpr int kSweepRows = 4;     // block SSOR, tables in global memory: rows a thread sweeps at a time
 // The pipelined recurrences in FP32 lose track of the true residual below
 // about 1e-4 of the starting one, so each refinement step of the mixed solve
 // asks the inner solve for at most this much reduction.
@@ -286,6 +287,58 @@ __device__ __forceinline__ void pipe_update(const OwnRef<T, K>& o, int row, cons
   store_m<T, K>(mnext, row, m);
 }
 
+// The block-SSOR sweeps over a block's colour lists when they live in global
+// memory (a block whose shared memory cannot hold them): the same steps as
+// the shared-memory sweeps of pipe_body, NR rows per thread at a time with
+// their loads issued together (rows of one colour are not coupled, and a
+// thread has several rows per step when a block holds many row slices).
+// Kept out of line, so the kernel body holds the hot shared-memory loop only.
+template <typename T, int K, int NR>
+__device__ __noinline__ void ssor_sweeps_global(const PipeSmem<K>* s, const LEnt<T>* lent, T* sv, int t, int B) {
+  const int nc = s->ncb;
+  for (int pass = 0; pass < 2; ++pass) {
+    const bool fwd = pass == 0;
+    for (int step = 1; step < nc; ++step) {
+      const int c = fwd ? step : nc - 1 - step;
+      const int beg = s->coff[c], cnt = s->coff[c + 1] - beg;
+      const int w = fwd ? s->wl[c] : s->wu[c];
+      const LEnt<T>* le = lent + (fwd ? s->loff[c] : s->uoff[c]);
+      for (int p0 = t; p0 < cnt; p0 += NR * B) {
+        T x[NR][K];
+        bool okr[NR];
+#pragma unroll
+        for (int r = 0; r < NR; ++r) {
+          okr[r] = p0 + r * B < cnt;
+          load_m<T, K>(sv, okr[r] ? beg + p0 + r * B : -1, x[r]);
+        }
+        for (int e = 0; e < w; e += 2) {
+          LEnt<T> e0[NR], e1[NR];
+#pragma unroll
+          for (int r = 0; r < NR; ++r) {
+            const int p = p0 + r * B;
+            e0[r] = okr[r] ? le[e * cnt + p] : LEnt<T>{-1, (T)0};
+            e1[r] = okr[r] && e + 1 < w ? le[(e + 1) * cnt + p] : LEnt<T>{-1, (T)0};
+          }
+          T y0[NR][K], y1[NR][K];
+#pragma unroll
+          for (int r = 0; r < NR; ++r) {
+            load_m<T, K>(sv, e0[r].j, y0[r]);
+            load_m<T, K>(sv, e1[r].j, y1[r]);
+          }
+#pragma unroll
+          for (int r = 0; r < NR; ++r)
+#pragma unroll
+            for (int cc = 0; cc < K; ++cc) x[r][cc] -= e0[r].v * y0[r][cc] + e1[r].v * y1[r][cc];
+        }
+#pragma unroll
+        for (int r = 0; r < NR; ++r)
+          if (okr[r]) store_m<T, K>(sv, beg + p0 + r * B, x[r]);
+      }
+      __syncthreads();
+    }
+  }
+}
+
 template <typename T, int K, int QR, class Team>
 __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, unsigned char* dyn) {
   // entries of a row gathered together (K values per neighbour in both forms)
@@ -395,8 +448,12 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
   unsigned char* srowc = (unsigned char*)os + align16((size_t)(6 * K + 1) * nsl * sizeof(T));
   short* spos = (short*)(srowc + align16((size_t)nsl));
   const int lents = s->lents;
-  LEnt<T>* lent = (LEnt<T>*)((unsigned char*)spos + align16((size_t)nsl * sizeof(short)));
-  T* sv = (T*)((unsigned char*)lent + align16((size_t)lents * sizeof(LEnt<T>)));  // 16-byte rows
+  LEnt<T>* const lent = (LEnt<T>*)((unsigned char*)spos + align16((size_t)nsl * sizeof(short)));
+  T* const sv = (T*)((unsigned char*)lent + align16((size_t)lents * sizeof(LEnt<T>)));  // 16-byte rows
+  // the same tables in the global scratch a.bss_* (this block's share), for
+  // blocks whose shared memory cannot hold them
+  LEnt<T>* const lent_g = bssor ? (LEnt<T>*)a.bss_lent + a.bss_loff[team.rank()] : nullptr;
+  T* const sv_g = bssor ? (T*)a.bss_v + (size_t)blk0 * MRow<T, K>::W : nullptr;
   T* pown = (T*)a.pown;
   auto own_ref = [&](int q, int row) {
     OwnRef<T, K> o;
@@ -487,53 +544,36 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
       }
     }
   };
-  // Own state in global memory: each thread its own rows, colour by colour,
-  // the neighbours from the row of A.
-  auto ssor_generic = [&]() {
-    for (int pass = 0; pass < 2; ++pass) {
-      const bool fwd = pass == 0;
-      for (int step = 0; step < s->ncb; ++step) {
-        const int c = fwd ? step : s->ncb - 1 - step;
-        for (int q = 0; q < Qb; ++q) {
-          const int row = row0 + q * R;
-          if (row >= n) break;
-          if ((int)__ldg(bcol + row) != c) continue;
-          const OwnRef<T, K> o = own_ref(q, row);
-          const RowRef<T> rr = row_ref(q, row);
-          T acc[K];
-#pragma unroll
-          for (int cc = 0; cc < K; ++cc) acc[cc] = (T)0;
-          for (int e = 0; e < rr.len; ++e) {
-            const int j = rr.c[e * rr.stride];
-            if (j < blk0 || j >= blk0 + rb_n || j == row) continue;  // padding (-1) or another block's row
-            const int cj = (int)__ldg(bcol + j);
-            if (fwd ? cj >= c : cj <= c) continue;
-            const T v = rr.v[e * rr.stride];
-            const T* oj = pown + (size_t)j * OwnRef<T, K>::kLen + (fwd ? kQs : kQz) * K;
-#pragma unroll
-            for (int cc = 0; cc < K; ++cc) acc[cc] += v * oj[cc];
-          }
-          const T mi = o(kQminv, 0);
-#pragma unroll
-          for (int cc = 0; cc < K; ++cc) {
-            if (fwd) o(kQs, cc) = (o(kQr, cc) - acc[cc]) * mi;
-            else o(kQz, cc) = o(kQs, cc) - mi * acc[cc];
-          }
-        }
-        __syncthreads();
-      }
-    }
+  // The tables in shared memory (beside the own state, when everything fits
+  // there) or in the global scratch; the colours of the global case come
+  // from a.bcolor, the list positions from a.bss_pos.
+  const bool sm_ssor = bssor && own_s;
+  int* const gpos = a.bss_pos;
+  auto colour_of = [&](int slot) -> int {
+    if (sm_ssor) return srowc[slot];
+    return slot < rb_n ? (int)__ldg(bcol + blk0 + slot) : 255;
   };
-  const bool fast_ssor = bssor && own_s;
+  auto pos_of = [&](int slot) -> int { return sm_ssor ? (int)spos[slot] : gpos[blk0 + slot]; };
   auto ssor_apply = [&]() {
-    if (fast_ssor) ssor_fast();
-    else ssor_generic();
+    if (sm_ssor) ssor_fast();
+    else if (Qb <= 2) ssor_sweeps_global<T, K, 1>(s, lent_g, sv_g, t, B);
+    else ssor_sweeps_global<T, K, kSweepRows>(s, lent_g, sv_g, t, B);
   };
-  if (fast_ssor) {
-    for (int q = 0; q < Qb; ++q) {
-      const int row = row0 + q * R;
-      srowc[q * B + t] = row < n ? __ldg(bcol + row) : (unsigned char)255;
-    }
+  // a row's entry of the sweep vector, by slot
+  auto sv_store = [&](int slot, const T (&x)[K]) {
+    if (sm_ssor) store_m<T, K>(sv, spos[slot], x);
+    else store_m<T, K>(sv_g, gpos[blk0 + slot], x);
+  };
+  auto sv_load = [&](int slot, T (&x)[K]) {
+    if (sm_ssor) load_m<T, K>(sv, spos[slot], x);
+    else load_m<T, K>(sv_g, gpos[blk0 + slot], x);
+  };
+  if (bssor) {
+    if (sm_ssor)
+      for (int q = 0; q < Qb; ++q) {
+        const int row = row0 + q * R;
+        srowc[q * B + t] = row < n ? __ldg(bcol + row) : (unsigned char)255;
+      }
     __syncthreads();
     // list positions in row order (warp w scans the block's slots for the
     // colours w, w + warps, ...; ballots give the positions) and the list
@@ -542,11 +582,12 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
       int pos0 = s->coff[c];
       for (int s0 = 0; s0 < nsl; s0 += 32) {
         const int slot = s0 + lane;
-        const bool hit = slot < nsl && srowc[slot] == c;
+        const bool hit = slot < nsl && colour_of(slot) == c;
         const unsigned m = __ballot_sync(0xffffffffu, hit);
         if (hit) {
           const int pos = pos0 + __popc(m & ((1u << lane) - 1u));
-          spos[slot] = (short)pos;
+          if (sm_ssor) spos[slot] = (short)pos;
+          else gpos[blk0 + slot] = pos;
         }
         pos0 += __popc(m);
       }
@@ -556,19 +597,19 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
     for (int q = 0; q < Qb; ++q) {
       const int row = row0 + q * R;
       if (row >= n) break;
-      const int slot = q * B + t, ci = srowc[slot];
-      const int p = spos[slot] - s->coff[ci], cnt = s->coff[ci + 1] - s->coff[ci];
-      LEnt<T>* ll = lent + s->loff[ci] + p;
-      LEnt<T>* lu = lent + s->uoff[ci] + p;
-      const T mi = os[(size_t)slot * OwnRef<T, K>::kLen + kQminv * K];
-      const int wq = s->wmax[q], bq = s->base[q] + t;
+      const int slot = q * B + t, ci = colour_of(slot);
+      const int p = pos_of(slot) - s->coff[ci], cnt = s->coff[ci + 1] - s->coff[ci];
+      LEnt<T>* const lbase = sm_ssor ? lent : lent_g;
+      LEnt<T>* ll = lbase + s->loff[ci] + p;
+      LEnt<T>* lu = lbase + s->uoff[ci] + p;
+      const T mi = own_ref(q, row)(kQminv, 0);
+      const RowRef<T> rr = row_ref(q, row);
       int nl = 0, nu = 0;
-      for (int e = 0; e < wq; ++e) {
-        const int ix = bq + e * B;
-        const int j = ccol[ix];
+      for (int e = 0; e < rr.len; ++e) {
+        const int j = rr.c[e * rr.stride];
         if (j < blk0 || j >= blk0 + rb_n || j == row) continue;
-        const int cj = srowc[j - blk0];
-        const LEnt<T> en{(int)spos[j - blk0], mi * cval[ix]};
+        const int cj = colour_of(j - blk0);
+        const LEnt<T> en{pos_of(j - blk0), mi * rr.v[e * rr.stride]};
         if (cj < ci) ll[(size_t)nl++ * cnt] = en;
         else if (cj > ci) lu[(size_t)nu++ * cnt] = en;
       }
@@ -663,11 +704,11 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
           o(kQz, c) = u[c];
           rr[c] += rv * rv;
         }
-        if (fast_ssor) {  // the block sweeps start from M^-1 r
+        if (bssor) {  // the block sweeps start from M^-1 r
           T v[K];
 #pragma unroll
           for (int c = 0; c < K; ++c) v[c] = u[c];
-          store_m<T, K>(sv, spos[q * B + t], v);
+          sv_store(q * B + t, v);
         }
         // both forms' first gathers: u = M^-1 r (pipelined, to m0) and
         // z = M^-1 r (classic, to m2; after the block sweeps with block SSOR)
@@ -687,8 +728,8 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
           if (row >= n) break;
           const OwnRef<T, K> o = own_ref(q, row);
           T m[K];
-          if (fast_ssor) {
-            load_m<T, K>(sv, spos[q * B + t], m);
+          if (bssor) {
+            sv_load(q * B + t, m);
 #pragma unroll
             for (int c = 0; c < K; ++c) o(kQz, c) = m[c];
           } else {
@@ -1037,7 +1078,7 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
             }
           }
           if (!bssor) store_m<T, K>(rnext, row, rec);
-          else if (fast_ssor) store_m<T, K>(sv, spos[q * B + t], rec);
+          else sv_store(q * B + t, rec);
         }
         if (bssor) {  // z = M^-1 r by the block sweeps, then the records and the dots
           __syncthreads();
@@ -1047,12 +1088,12 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
             if (row >= n) break;
             const OwnRef<T, K> o = own_ref(q, row);
             T zf[K];
-            if (fast_ssor) load_m<T, K>(sv, spos[q * B + t], zf);
+            if (bssor) sv_load(q * B + t, zf);
             T rec[K];
 #pragma unroll
             for (int c = 0; c < K; ++c) {
               const T r = o(kQr, c);
-              if (fast_ssor) o(kQz, c) = zf[c];
+              if (bssor) o(kQz, c) = zf[c];
               const T z = o(kQz, c);
               rec[c] = z;
               d2[c] += r * z;
@@ -1231,6 +1272,27 @@ int block_colours(const int* A_ptr, const int* A_col, int n, int rb, unsigned ch
   return maxc;
 }
 
+long long block_list_entries(const int* A_ptr, const int* A_col, const unsigned char* col, long long blk0,
+                             long long rb_n) {
+  int cnt[kMaxColours] = {}, wl[kMaxColours] = {}, wu[kMaxColours] = {};
+  for (long long row = blk0; row < blk0 + rb_n; ++row) {
+    const int ci = col[row];
+    int nl = 0, nu = 0;
+    for (int e = A_ptr[row]; e < A_ptr[row + 1]; ++e) {
+      const int j = A_col[e];
+      if (j < blk0 || j >= blk0 + rb_n || j == row) continue;
+      nl += col[j] < ci;
+      nu += col[j] > ci;
+    }
+    ++cnt[ci];
+    wl[ci] = std::max(wl[ci], nl);
+    wu[ci] = std::max(wu[ci], nu);
+  }
+  long long lents = 0;
+  for (int k = 0; k < kMaxColours; ++k) lents += (long long)cnt[k] * (wl[k] + wu[k]);
+  return lents;
+}
+
 void pipelined_smem_need(const int* A_ptr, const int* A_col, int n, int grid, int block, int precision, int K,
                          bool bssor, size_t* cache, size_t* full) {
   const size_t vs = precision == CN_PREC_MIXED ? sizeof(float) : sizeof(double);
@@ -1262,22 +1324,7 @@ void pipelined_smem_need(const int* A_ptr, const int* A_col, int n, int grid, in
     wc = std::max(wc, c);
     size_t extra = 0;
     if (bssor) {  // the kernel's colour lists: rows per colour x (lower + upper width)
-      int cnt[kMaxColours] = {}, wl[kMaxColours] = {}, wu[kMaxColours] = {};
-      for (long long row = blk0; row < blk0 + rb_n; ++row) {
-        const int ci = col[row];
-        int nl = 0, nu = 0;
-        for (int e = A_ptr[row]; e < A_ptr[row + 1]; ++e) {
-          const int j = A_col[e];
-          if (j < blk0 || j >= blk0 + rb_n || j == row) continue;
-          nl += col[j] < ci;
-          nu += col[j] > ci;
-        }
-        ++cnt[ci];
-        wl[ci] = std::max(wl[ci], nl);
-        wu[ci] = std::max(wu[ci], nu);
-      }
-      size_t lents = 0;
-      for (int k = 0; k < kMaxColours; ++k) lents += (size_t)cnt[k] * (wl[k] + wu[k]);
+      const size_t lents = (size_t)block_list_entries(A_ptr, A_col, col.data(), blk0, rb_n);
       // (LEnt: 8 bytes in FP32, 16 in FP64; the sweep vector padded to 16 bytes a row)
       const size_t wpad = ((size_t)K * vs + 15) / 16 * 16;
       extra = align16((size_t)Qb * block) + align16((size_t)Qb * block * sizeof(short)) + align16(lents * 2 * vs) +
