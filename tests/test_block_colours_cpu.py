@@ -1,6 +1,7 @@
 """CPU checks of the host logic behind block SSOR: the DSatur colouring of
 the rows inside each block of the row-cached kernel (cn::block_colours) is a
-proper colouring of the couplings inside the block, uses few colours, and the
+proper colouring of the couplings inside the block up to a few folded rows,
+uses few colours, and the
 list sizing the kernel and the host agree on (cn::block_list_entries) covers
 every in-block coupling of the block exactly once."""
 import ctypes as C
@@ -38,11 +39,17 @@ def test_dsatur_block_colouring_is_proper(name, rb, oracle):
                                col.ctypes.data_as(C.c_void_p))
     assert 1 <= nc <= 64 and col.max() + 1 == nc
     maxdeg = int(np.diff(ap).max())
+    same = {}
     for i in range(n):
         lo = i // rb * rb
         nb = ac[ap[i]:ap[i + 1]]
         nb = nb[(nb != i) & (nb >= lo) & (nb < lo + rb)]
-        assert not np.any(col[nb] == col[i]), (i, nb)
+        same[lo] = same.get(lo, 0) + int(np.sum(col[nb] == col[i]))
+    # proper, except where a tiny fourth colour (at most 8 rows) was folded
+    # into the lower colours: those rows' couplings to same-colour neighbours
+    # are the only ones the sweeps drop
+    assert all(v <= 2 * 8 * maxdeg for v in same.values())
+    assert sum(same.values()) <= 0.01 * ap[-1]
     # a triangulated surface needs 3 colours; DSatur stays well below the degree bound
     assert nc <= min(maxdeg, 6)
 

@@ -1233,6 +1233,16 @@ int block_colours(const int* A_ptr, const int* A_col, int n, int rb, unsigned ch
   // most distinct colours among its coloured neighbours (then the most
   // uncoloured neighbours, then the lowest index); it takes the lowest
   // colour none of them has.
+  //
+  // Then a top colour (beyond the third) of at most kFoldRows rows, which
+  // would cost every sweep two block barriers (and, through the grid
+  // barrier, every block) for a handful of rows, is folded into the lower
+  // colour holding the fewest of each row's neighbours.  The couplings
+  // between rows of one colour are left out of the block's L and U on both
+  // sides (the kernel's list build skips them), so M = (D + L) D^-1 (D + L)^T
+  // stays symmetric positive definite; a few of a block's thousands of
+  // couplings are dropped.
+  constexpr int kFoldRows = 8;
   int maxc = 0;
   std::vector<unsigned long long> used;
   std::vector<int> deg;
@@ -1268,7 +1278,27 @@ int block_colours(const int* A_ptr, const int* A_col, int n, int rb, unsigned ch
         pq.insert({__builtin_popcountll(used[q]), deg[q], -q});
       }
     }
+    for (;;) {
+      int top = 0, ntop = 0;
+      for (int i = lo; i < hi; ++i) top = std::max(top, (int)col[i]);
+      for (int i = lo; i < hi; ++i) ntop += col[i] == top;
+      if (top < 3 || ntop > kFoldRows) break;
+      for (int i = lo; i < hi; ++i) {
+        if (col[i] != top) continue;
+        int cnt[kMaxColours] = {};
+        for (int e = A_ptr[i]; e < A_ptr[i + 1]; ++e) {
+          const int j = A_col[e];
+          if (j >= lo && j < hi && j != i) ++cnt[col[j]];
+        }
+        int best = 0;
+        for (int c = 1; c < top; ++c)
+          if (cnt[c] < cnt[best]) best = c;
+        col[i] = (unsigned char)best;
+      }
+    }
   }
+  maxc = 0;
+  for (int i = 0; i < n; ++i) maxc = std::max(maxc, (int)col[i] + 1);
   return maxc;
 }
 
