@@ -422,7 +422,7 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
           s->uoff[c] = lents;
           lents += cnt * s->wu[c];
         }
-        own += align16((size_t)Qb * B) + align16((size_t)Qb * B * sizeof(short)) +
+        own += align16((size_t)Qb * B) + 2 * align16((size_t)Qb * B * sizeof(short)) +
                align16((size_t)lents * sizeof(LEnt<T>)) + (size_t)Qb * B * MRow<T, K>::W * sizeof(T);
       }
       s->lents = lents;
@@ -448,7 +448,8 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
   unsigned char* srowc = (unsigned char*)os + align16((size_t)(6 * K + 1) * nsl * sizeof(T));
   short* spos = (short*)(srowc + align16((size_t)nsl));
   const int lents = s->lents;
-  LEnt<T>* const lent = (LEnt<T>*)((unsigned char*)spos + align16((size_t)nsl * sizeof(short)));
+  short* const slist = (short*)((unsigned char*)spos + align16((size_t)nsl * sizeof(short)));  // position -> slot
+  LEnt<T>* const lent = (LEnt<T>*)((unsigned char*)slist + align16((size_t)nsl * sizeof(short)));
   T* const sv = (T*)((unsigned char*)lent + align16((size_t)lents * sizeof(LEnt<T>)));  // 16-byte rows
   // the same tables in the global scratch a.bss_* (this block's share), for
   // blocks whose shared memory cannot hold them
@@ -510,7 +511,11 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
   // lower neighbour); going down, v_i -= sum over higher neighbours of
   // (a_ij / a_ii) v_j turns it into z (the top colour's z is its y).  A step
   // runs over the colour's list, one row per thread.
-  auto ssor_fast = [&]() {
+  // With fin (the inner iterations, at least two colours), the thread that
+  // makes a row's z final (the top colour going up, the others going down)
+  // also writes it to the row's record and to the gathered copy zn, and adds
+  // the row's (r, z) and ||r||^2 to d2: no pass over the own rows afterwards.
+  auto ssor_fast_fin = [&](bool fin, T* zn, T* d2) {
     const int nc = s->ncb;
     for (int pass = 0; pass < 2; ++pass) {
       const bool fwd = pass == 0;
@@ -539,11 +544,24 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
             for (int cc = 0; cc < K; ++cc) x[cc] -= e0.v * y0[cc];
           }
           store_m<T, K>(sv, beg + p, x);
+          if (fin && (!fwd || c == nc - 1)) {
+            const int slot = slist[beg + p];
+            T* o = os + (size_t)slot * OwnRef<T, K>::kLen;
+#pragma unroll
+            for (int cc = 0; cc < K; ++cc) {
+              const T r = o[kQr * K + cc];
+              o[kQz * K + cc] = x[cc];
+              d2[cc] += r * x[cc];
+              d2[K + cc] += r * r;
+            }
+            store_m<T, K>(zn, blk0 + slot, x);
+          }
         }
         __syncthreads();
       }
     }
   };
+  auto ssor_fast = [&]() { ssor_fast_fin(false, nullptr, nullptr); };
   // The tables in shared memory (beside the own state, when everything fits
   // there) or in the global scratch; the colours of the global case come
   // from a.bcolor, the list positions from a.bss_pos.
@@ -586,7 +604,10 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
         const unsigned m = __ballot_sync(0xffffffffu, hit);
         if (hit) {
           const int pos = pos0 + __popc(m & ((1u << lane) - 1u));
-          if (sm_ssor) spos[slot] = (short)pos;
+          if (sm_ssor) {
+            spos[slot] = (short)pos;
+            slist[pos] = (short)slot;
+          }
           else gpos[blk0 + slot] = pos;
         }
         pos0 += __popc(m);
@@ -1080,7 +1101,10 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
           if (!bssor) store_m<T, K>(rnext, row, rec);
           else sv_store(q * B + t, rec);
         }
-        if (bssor) {  // z = M^-1 r by the block sweeps, then the records and the dots
+        if (bssor && sm_ssor && s->ncb >= 2) {  // the sweeps also write the records and the dots
+          __syncthreads();
+          ssor_fast_fin(true, rnext, d2);
+        } else if (bssor) {  // z = M^-1 r by the block sweeps, then the records and the dots
           __syncthreads();
           ssor_apply();
           for (int q = 0; q < Qb; ++q) {
@@ -1357,7 +1381,7 @@ void pipelined_smem_need(const int* A_ptr, const int* A_col, int n, int grid, in
       const size_t lents = (size_t)block_list_entries(A_ptr, A_col, col.data(), blk0, rb_n);
       // (LEnt: 8 bytes in FP32, 16 in FP64; the sweep vector padded to 16 bytes a row)
       const size_t wpad = ((size_t)K * vs + 15) / 16 * 16;
-      extra = align16((size_t)Qb * block) + align16((size_t)Qb * block * sizeof(short)) + align16(lents * 2 * vs) +
+      extra = align16((size_t)Qb * block) + 2 * align16((size_t)Qb * block * sizeof(short)) + align16(lents * 2 * vs) +
               (size_t)Qb * (size_t)block * wpad;
     }
     wf = std::max(wf, c + align16((size_t)(6 * K + 1) * (size_t)Qb * (size_t)block * vs) + extra);
