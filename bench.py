@@ -25,6 +25,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 WORKLOAD = "torus512x256_8seams_2pct_handles_3rhs"
+METRIC = "solves/sec at 1e-8 rel. residual"
 
 
 def load_peaks():
@@ -191,52 +192,82 @@ def algorithmic_bytes_bssor(info, stats, k, mixed):
     return algorithmic_bytes_classic(info, stats, k, mixed) + stats.iterations * sweeps
 
 
-def cpu_baseline(pos, tris, h, t, seconds=12.0):
-    """The oracle's FP64 IC(0)-PCG (the reference's CPU path restated), columns
-    on parallel threads; bounded sample of whole solves."""
-    from oracle import oracle as O
-    ref = O.System(pos, tris, h)
-    threads = min(3, os.cpu_count() or 1)
-    n = 0
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def oracle_round(ref, t, threads, tol=1e-8):
+    """`threads` whole FP64 IC(0)-PCG solves of the same targets at once, one
+    per host thread (each solves its 3 columns in turn); returns the wall
+    time of the round.  ctypes releases the GIL inside the oracle."""
+    from concurrent.futures import ThreadPoolExecutor
     t0 = time.perf_counter()
-    while True:
-        st, x, it, rel = ref.solve(t, mode=1, tol=1e-8, threads=threads)
-        n += 1
-        el = time.perf_counter() - t0
-        if el > seconds or n >= 200:
-            break
-    return {"value": n / el, "unit": "solves/s", "cores": threads, "kind": "port",
-            "sample": f"{n} whole FP64 IC(0)-PCG solves of the workload to 1e-8 ({el:.1f} s)"}
+    if threads == 1:
+        st, *_ = ref.solve(t, mode=1, tol=tol, threads=1)
+        assert st == 0
+    else:
+        with ThreadPoolExecutor(max_workers=threads) as ex:
+            for st, *_ in ex.map(lambda _: ref.solve(t, mode=1, tol=tol, threads=1), range(threads)):
+                assert st == 0
+    return time.perf_counter() - t0
+
+
+def oracle_system(pos, tris, h):
+    from oracle import oracle as O
+    return O.System(pos, tris, h)
+
+
+def cpu_baseline(pos, tris, h, t, seconds=10.0):
+    """The oracle's FP64 IC(0)-PCG (the reference's CPU path restated) on the
+    host: rounds of independent whole solves, one per core, for about
+    `seconds`, then single-threaded for about half that."""
+    ref = oracle_system(pos, tris, h)
+    cores = host_cores()
+    n_all, el_all = 0, 0.0
+    while el_all < seconds:
+        el_all += oracle_round(ref, t, cores)
+        n_all += cores
+    n_one, el_one = 0, 0.0
+    while el_one < seconds / 2 or n_one < 2:
+        el_one += oracle_round(ref, t, 1)
+        n_one += 1
+    return {"value": n_all / el_all, "unit": "solves/s", "cores": cores, "kind": "port",
+            "sample": f"{n_all} whole FP64 IC(0)-PCG solves of the workload to 1e-8, {cores} at a time "
+                      f"on {cores} host threads ({el_all:.1f} s)",
+            "single_thread": {"value": n_one / el_one, "unit": "solves/s", "cores": 1,
+                              "sample": f"{n_one} solves one after another ({el_one:.1f} s)"}}
 
 
 def run_reference(args, rank, world):
     """--impl reference: the oracle (the reference's CPU path restated; the
-    reference's own C++ runtime is not in its snapshot) on the host cores."""
+    reference's own C++ runtime is not in its snapshot) on all host cores:
+    each step is one round of independent whole solves, one per core; the
+    seam cut is the oracle's own (no product library is loaded)."""
     if rank != 0:
         return
-    from tool_godot_curvenet_b200 import cut_mesh, synth
-    m, h, t = synth.config2()
-    tris, parent = cut_mesh(m.positions.shape[0], m.tris, m.loops)
-    pos = m.positions[parent]
     from oracle import oracle as O
+    from tool_godot_curvenet_b200 import synth
+    m, h, t = synth.config2()
+    tris, parent = O.cut_mesh(m.positions.shape[0], m.tris, m.loops)
+    pos = np.ascontiguousarray(m.positions[parent])
     ref = O.System(pos, tris, h)
-    threads = min(3, os.cpu_count() or 1)
+    cores = host_cores()
     for _ in range(args.warmup):
-        ref.solve(t, mode=1, tol=1e-8, threads=threads)
-    times = []
-    for _ in range(args.steps):
-        t0 = time.perf_counter()
-        ref.solve(t, mode=1, tol=1e-8, threads=threads)
-        times.append(time.perf_counter() - t0)
+        oracle_round(ref, t, cores)
+    times = [oracle_round(ref, t, cores) for _ in range(args.steps)]
     ms = 1e3 * sum(times) / len(times)
-    v = 1e3 / ms
-    line = {"impl": "reference", "metric": "solves/sec at 1e-8 rel. residual (mixed FP32+FP64 refinement)",
+    v = cores * 1e3 / ms
+    line = {"impl": "reference", "metric": METRIC,
             "value": v, "unit": "solves/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic (seeded torus, see synth.config2)",
-            "config": {"workload": WORKLOAD, "parallelism": "host threads over RHS columns"},
-            "cpu_baseline": {"value": v, "unit": "solves/s", "cores": threads, "kind": "port",
-                             "sample": f"{args.steps} whole FP64 IC(0)-PCG solves"},
+            "config": {"workload": WORKLOAD, "parallelism": f"{cores} host threads, one whole solve each per step",
+                       "solver": "FP64 IC(0)-PCG (oracle restatement of the reference's CPU solve)"},
+            "cpu_baseline": {"value": v, "unit": "solves/s", "cores": cores, "kind": "port",
+                             "sample": f"{args.steps} rounds of {cores} concurrent whole FP64 IC(0)-PCG solves"},
             "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -268,7 +299,7 @@ def batch_section(torch, dist, world, rank, local, steps, warmup, n_meshes=512):
     d_x = torch.empty(int(B.out_off[-1]), dtype=torch.float64, device=f"cuda:{local}")
     stream = torch.cuda.ExternalStream(B.stream(), device=local)
     st_mixed = B.solve_device(d_t.data_ptr(), d_x.data_ptr(), precision="mixed", tol=1e-8)
-    sts, its, rel = B.mesh_stats()
+    sts, its, rel, refs = B.mesh_stats(refinements=True)
     st_fp64 = B.solve_device(d_t.data_ptr(), d_x.data_ptr(), precision="fp64", tol=1e-8)
 
     def timed(precision, k_steps):
@@ -301,18 +332,21 @@ def batch_section(torch, dist, world, rank, local, steps, warmup, n_meshes=512):
     ms_m = reduce_over_ranks(dist, world, sum(tm) / len(tm), "max", dev)
     ms_f = reduce_over_ranks(dist, world, sum(tf) / len(tf), "max", dev)
     solves = n_meshes * 8  # (mesh, pose) solves of 3 RHS each, over all ranks
-    # algorithmic bytes of the inner IC(0)-PCG iterations (k = 24, FP32), per
-    # mesh from its own iteration count; the FP64 residual evaluations are
-    # left out, so this is a lower bound
+    # algorithmic bytes of the mixed solve, per mesh from its own iteration and
+    # refinement counts: inner IC(0)-PCG iterations (k = 24, FP32: SpMV, the two
+    # sweeps, 9 vector passes) plus the FP64 residual evaluations (FP64 SpMV of
+    # the 24 columns, b and x read, r written) and the FP64 right-hand side
     kb = 24
-    inner = 0
-    for (n_m, nnz_m, nnzl_m), it_m in zip(sizes, its):
+    inner, resid = 0, 0
+    for (n_m, nnz_m, nnzl_m), it_m, rf_m in zip(sizes, its, refs):
         b_spmv = nnz_m * 8 + 4 * (n_m + 1) + 2 * n_m * kb * 4
         b_ic = 2 * ((nnzl_m + n_m) * 8 + 4 * (n_m + 1) + 2 * n_m * kb * 4)
         inner += int(it_m) * (b_spmv + b_ic + 9 * n_m * kb * 4)
+        resid += (int(rf_m) + 1) * (nnz_m * 12 + 4 * (n_m + 1) + 3 * n_m * kb * 8)
     inner = reduce_over_ranks(dist, world, float(inner), "sum", dev)
+    resid = reduce_over_ranks(dist, world, float(resid), "sum", dev)
     peak_b, _ = load_peaks()
-    # algorithmic bytes of the batch (mixed): per mesh iterations x B_iter + residuals
+    plain = plain_batch_estimate(specs, mine, torch, local) if rank == 0 else None
     nnz = info["nnz_A"]
     n = info["n_free"]
     return {
@@ -326,13 +360,44 @@ def batch_section(torch, dist, world, rank, local, steps, warmup, n_meshes=512):
         "fp64_fused": {"solves_per_s": solves / (ms_f * 1e-3), "ms_per_batch": ms_f,
                        "max_rel_residual": st_fp64.max_rel_residual, "failed": st_fp64.n_failed},
         "speedup_mixed_vs_fp64_fused": ms_f / ms_m,
-        "roofline_mixed": {"bound": "hbm", "algorithmic_bytes_inner": inner,
-                           "achieved": inner / (ms_m * 1e-3) / 1e9, "peak": peak_b, "unit": "GB/s",
-                           "frac": inner / (ms_m * 1e-3) / 1e9 / peak_b,
-                           "note": "inner-iteration bytes only (SpMV + IC(0) sweeps + 9 vector passes per iteration)"},
+        "fp64_plain_extrapolated": plain,
+        "speedup_mixed_vs_fp64_plain": (plain["ms_per_batch"] / ms_m) if plain else None,
+        "roofline_mixed": {"bound": "hbm", "algorithmic_bytes": inner + resid, "algorithmic_bytes_inner": inner,
+                           "algorithmic_bytes_fp64_residuals": resid,
+                           "achieved": (inner + resid) / (ms_m * 1e-3) / 1e9, "peak": peak_b, "unit": "GB/s",
+                           "frac": (inner + resid) / (ms_m * 1e-3) / 1e9 / peak_b,
+                           "note": "per mesh: iterations x (SpMV + IC(0) sweeps + 9 vector passes) + (refinements + 1) x FP64 residual"},
         "build_s": build_s,
         "graph": "one cudaGraphLaunch (memset of the work counter + the persistent cluster kernel) per batch",
     }
+
+
+def plain_batch_estimate(specs, mine, torch, local, sample=16):
+    """Plain FP64 GPU PCG (Jacobi, one kernel per primitive, dots folded on the
+    host every iteration) over the batch workload, extrapolated from a timed
+    sample: the meshes of this rank in size order, every (len / sample)-th
+    one solved pose by pose (k = 3) to 1e-8 on its own handle; each sampled
+    mesh stands for the meshes of its size stratum."""
+    from tool_godot_curvenet_b200 import CutMeshSolver, cut_mesh
+    order = sorted(mine, key=lambda i: specs[i][0].positions.shape[0])
+    step = max(1, len(order) // sample)
+    picked = order[step // 2::step][:sample]
+    total_ms, solves = 0.0, 0
+    for i in picked:
+        m, h, t = specs[i]
+        tris, parent = cut_mesh(m.positions.shape[0], m.tris, m.loops)
+        pos = np.ascontiguousarray(m.positions[parent])
+        with CutMeshSolver(pos, tris, h, device=local, precond="jacobi") as s:
+            s.solve(t[:, :3], mode="deform", precision="fp64", algo="plain", tol=1e-8, max_iter=100000)
+            for p in range(t.shape[1] // 3):
+                r = s.solve(t[:, 3 * p:3 * p + 3], mode="deform", precision="fp64", algo="plain", tol=1e-8,
+                            max_iter=100000)
+                total_ms += r.device_ms
+                solves += 1
+    scale = len(order) / len(picked)
+    return {"ms_per_batch": total_ms * scale, "solves_per_s": solves * scale / (total_ms * scale * 1e-3),
+            "sample": f"{len(picked)} of {len(order)} meshes (every {step}-th in size order), "
+                      f"{solves} pose solves of 3 RHS, device time x {scale:.1f}"}
 
 
 def reduced_sizes(nv, tris, handles):
@@ -391,12 +456,14 @@ def spmv_section(torch, local, peak, steps=20):
             gbs = byts / (med * 1e-3) / 1e9
             out[f"{prec}_k{k}"] = {"ms": med, "algorithmic_bytes": byts, "achieved_gbs": gbs, "peak_gbs": peak,
                                    "frac": gbs / peak}
+            del x, y
         try:
             with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
-                out["mixed_k24"]["traffic"] = json.load(f)["cn_spmm_fp32_k24_torus1024"]["dram_bytes_per_launch"]
+                e = json.load(f)["cn_spmm_fp32_k24_torus1024"]
+            out["mixed_k24"]["traffic"] = e["dram_bytes_per_launch"]
+            out["mixed_k24"]["traffic_capture"] = {k: e.get(k) for k in ("workload", "kernel", "source")}
         except Exception:
             pass
-            del x, y
     return out
 
 
@@ -444,6 +511,164 @@ def ddm_section(torch, local):
             "runtime_lbs_us": 1e3 * statistics.median(ms), "runtime_precision": "fp32"}
 
 
+def capture_traffic(key, workload, info, stats):
+    """DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of
+    the ncu capture recorded in profiles/traffic.json under `key`, used only
+    when the capture's workload, launch grid and inner-iteration count match
+    this run's (otherwise the figure belongs to another kernel or workload
+    and None is reported)."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            e = json.load(f)[key]
+    except Exception:
+        return None, None
+    src = {k: e.get(k) for k in ("workload", "kernel", "grid", "iterations", "source")}
+    same = (e.get("workload") == workload and e.get("grid") == info["grid"]
+            and e.get("iterations") == stats.iterations)
+    src["matches_this_run"] = bool(same)
+    return (e["dram_bytes_per_launch"] if same else None), src
+
+
+def time_device_solves(torch, s, local, k, d_t, d_x, steps, warmup, flush=None, **kw):
+    """Statistics of one solve, then `warmup` untimed and `steps` timed
+    device-pointer solves on the handle's stream (CUDA events; optional L2
+    flush outside the events)."""
+    st = s.solve_device(k, d_t, d_x, stats=True, **kw)
+    if st.status != 0:
+        raise SystemExit(f"solve failed: status {st.status}")
+    stream = torch.cuda.ExternalStream(s.stream(), device=local)
+    with torch.cuda.stream(stream):
+        for _ in range(warmup):
+            s.solve_device(k, d_t, d_x, stats=False, **kw)
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        for a, b in evs:
+            if flush is not None:
+                flush.sum()
+            a.record(stream)
+            s.solve_device(k, d_t, d_x, stats=False, **kw)
+            b.record(stream)
+        torch.cuda.synchronize()
+    return st, [a.elapsed_time(b) for a, b in evs]
+
+
+def c1_section(torch, local, steps=20):
+    """The small plain-method workload (cylinder 64 x 32, one seam, bottom
+    ring fixed, top ring under a rigid transform, 3 RHS): FP64 IC(0)-PCG to
+    1e-10 (the configuration's solver and tolerance) on the GPU, mixed
+    precision and block SSOR beside it, and the oracle's FP64 IC(0)-PCG on one
+    host thread.  The whole system sits in L2 and in one block."""
+    from tool_godot_curvenet_b200 import CutMeshSolver, cut_mesh, synth
+    m, h, t = synth.config1()
+    tris, parent = cut_mesh(m.positions.shape[0], m.tris, m.loops)
+    pos = np.ascontiguousarray(m.positions[parent])
+    dev = f"cuda:{local}"
+    d_t = torch.from_numpy(t).to(dev)
+    d_x = torch.empty((pos.shape[0], 3), dtype=torch.float64, device=dev)
+    out = {"workload": "cylinder64x32_1seam_rings_fixed_and_rigid_3rhs", "n_verts": int(pos.shape[0]), "tol": 1e-10}
+    for precond, precision in [("ic0", "fp64"), ("ic0", "mixed"), ("bssor", "mixed"), ("jacobi", "fp64")]:
+        with CutMeshSolver(pos, tris, h, device=local, precond=precond) as s:
+            st, ms = time_device_solves(torch, s, local, 3, d_t.data_ptr(), d_x.data_ptr(), steps, 3,
+                                        mode="deform", precision=precision, tol=1e-10, max_iter=20000)
+            out[f"{precond}_{precision}"] = {"solves_per_s": 1e3 / statistics.mean(ms), "ms": statistics.mean(ms),
+                                             "iterations": st.iterations, "refinements": st.refinements,
+                                             "max_rel_residual": st.max_rel_residual,
+                                             "grid": s.info()["grid"]}
+    ref = oracle_system(pos, tris, h)
+    n, el = 0, 0.0
+    while el < 2.0 or n < 3:
+        el += oracle_round(ref, t, 1, tol=1e-10)
+        n += 1
+    out["cpu_oracle_1thread"] = {"solves_per_s": n / el, "sample": f"{n} FP64 IC(0)-PCG solves to 1e-10"}
+    return out
+
+
+def c4_section(local, reps=20):
+    """The adjoint workload (torus 128 x 64, 4 seams = 4 profile curves of 16
+    cubic control points, per-curve weights; loss 1/2 ||x - x_target||^2):
+    forward (cn_deform: curves -> handle targets -> deform solve) plus backward
+    (cn_adjoint: one solve with the same preconditioner, chain to the control
+    points and weights) pairs per second through the host-buffer calls, mixed
+    precision to 1e-8 and FP64 to 1e-10; the oracle's FP64 forward + adjoint
+    on one host thread beside it."""
+    from oracle import oracle as O
+    from tool_godot_curvenet_b200 import synth
+    from tool_godot_curvenet_b200.autograd import CurveDeformer
+    pos, tris, h, cof, tau, rest_cp, P, w, tcp, tw = synth.config4()
+    d = CurveDeformer(pos, tris, h, cof, tau, rest_cp, device=local)
+    xt = d.deform(tcp, tw, tol=1e-12, precision="fp64")
+    out = {"workload": "torus128x64_4seams_4curves_16cp", "n_verts": int(pos.shape[0]), "n_handles": int(h.size)}
+    grads = {}
+    for precision, tol in (("mixed", 1e-8), ("fp64", 1e-10)):
+        for _ in range(3):
+            x = d.deform(P, w, tol=tol, precision=precision)
+            d.adjoint(x - xt, tol=tol, precision=precision)
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            x = d.deform(P, w, tol=tol, precision=precision)
+            dP, dw = d.adjoint(x - xt, tol=tol, precision=precision)
+        el = time.perf_counter() - t0
+        grads[precision] = np.concatenate([dP.ravel(), dw])
+        out[precision] = {"fwd_bwd_per_s": reps / el, "ms_per_fwd_bwd": 1e3 * el / reps, "tol": tol}
+    out["mixed_grad_rel_diff_vs_fp64"] = float(np.linalg.norm(grads["mixed"] - grads["fp64"])
+                                               / np.linalg.norm(grads["fp64"]))
+    d.close()
+    ref = O.System(pos, tris, h)
+    e = ref.export()
+    Kp, Kc, Kv = O.assemble_csr(pos.shape[0], tris, pos)
+    S = rest_cp.shape[1] // 3
+    xo = np.empty((pos.shape[0], 3))
+    dPo = np.empty_like(rest_cp)
+    dwo = np.empty(rest_cp.shape[0])
+    n, el = 0, 0.0
+    while el < 2.0 or n < 2:
+        t0 = time.perf_counter()
+        O.lib().orc_deform_adjoint(ref._h, pos.shape[0], O.ip(Kp), O.ip(Kc), O.dp(Kv), ref.n, O.ip(e["free_of"]),
+                                   rest_cp.shape[0], S, O.dp(O.f64(rest_cp)), O.dp(O.f64(P)), O.dp(O.f64(w)),
+                                   h.size, O.ip(O.i32(h)), O.ip(O.i32(cof)), O.dp(O.f64(tau)), O.dp(O.f64(pos)),
+                                   O.dp(O.f64(xt)), 1e-10, 100000, O.dp(xo), O.dp(dPo), O.dp(dwo))
+        el += time.perf_counter() - t0
+        n += 1
+    out["cpu_oracle_1thread"] = {"fwd_bwd_per_s": n / el, "sample": f"{n} FP64 forward + adjoint to 1e-10"}
+    return out
+
+
+def c5_section(torch, local, peak, steps=3):
+    """The large-scale workload (torus 1024 x 1024 = 1.05M vertices, 16 seams,
+    1% handles, U(-0.5, 0.5), 3 RHS, 1e-8): IC(0), HSC, block SSOR and Jacobi
+    in mixed precision and IC(0) in FP64 -- iterations, build and solve time,
+    and for IC(0) the achieved bandwidth of its algorithmic bytes (SpMV, the
+    two triangular sweeps, 9 vector passes per iteration).  The vectors and
+    the factor exceed L2; L2 is flushed before every timed solve as well."""
+    from tool_godot_curvenet_b200 import CutMeshSolver, cut_mesh, synth
+    m, h, t = synth.config5()
+    tris, parent = cut_mesh(m.positions.shape[0], m.tris, m.loops)
+    pos = np.ascontiguousarray(m.positions[parent])
+    dev = f"cuda:{local}"
+    d_t = torch.from_numpy(t).to(dev)
+    d_x = torch.empty((pos.shape[0], 3), dtype=torch.float64, device=dev)
+    flush = torch.ones(64 << 20, dtype=torch.float32, device=dev)
+    out = {"workload": "torus1024x1024_16seams_1pct_handles_3rhs", "n_verts": int(pos.shape[0]), "tol": 1e-8,
+           "l2": "flushed (256 MB read) before every timed solve"}
+    for precond, precision in [("ic0", "mixed"), ("hsc", "mixed"), ("bssor", "mixed"), ("jacobi", "mixed"),
+                               ("ic0", "fp64")]:
+        t0 = time.perf_counter()
+        with CutMeshSolver(pos, tris, h, device=local, precond=precond) as s:
+            build_s = time.perf_counter() - t0
+            info = s.info()
+            st, ms = time_device_solves(torch, s, local, 3, d_t.data_ptr(), d_x.data_ptr(), steps, 1, flush,
+                                        mode="deform", precision=precision, tol=1e-8, max_iter=20000)
+            row = {"ms": statistics.mean(ms), "iterations": st.iterations, "refinements": st.refinements,
+                   "max_rel_residual": st.max_rel_residual, "build_s": build_s}
+            if precond == "ic0":
+                byts = algorithmic_bytes(info, st, 3, precision == "mixed")
+                row.update(algorithmic_bytes=byts, achieved_gbs=byts / (row["ms"] * 1e-3) / 1e9,
+                           frac=byts / (row["ms"] * 1e-3) / 1e9 / peak, n_levels=info["n_levels"])
+            out[f"{precond}_{precision}"] = row
+        if precond == "ic0" and precision == "mixed":
+            out["n_free"], out["nnz_A"] = info["n_free"], info["nnz_A"]
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -454,6 +679,8 @@ def main():
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-spmv", action="store_true")
     ap.add_argument("--no-ddm", action="store_true")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the sections of the cylinder, adjoint and 1M-vertex torus workloads")
     ap.add_argument("--batch-meshes", type=int, default=512,
                     help="meshes of the batched workload (the first N of the 512-mesh set; 512 is the benchmark)")
     args = ap.parse_args()
@@ -583,19 +810,18 @@ def main():
     bytes_mixed = algorithmic_bytes_bssor(info, st_mixed, k, True)
     bytes_fp64 = algorithmic_bytes_pipelined(info, st_fp64, k, False)
     ach = bytes_mixed / (ms_mixed * 1e-3) / 1e9
-    traffic = None
-    try:
-        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
-            tj = json.load(f)
-        traffic = tj.get("cn_pipe_solve_bssor_mixed", {}).get("dram_bytes_per_launch")
-    except Exception:
-        pass
+    traffic, traffic_src = capture_traffic("cn_pipe_solve_bssor_mixed", WORKLOAD, info, st_mixed)
     spmv = None
     if not args.no_spmv and rank == 0:
         spmv = spmv_section(torch, local, peak)
     ddm = None
     if not args.no_ddm and rank == 0:
         ddm = ddm_section(torch, local)
+    c1 = c4 = c5 = None
+    if not args.no_configs and rank == 0:
+        c1 = c1_section(torch, local)
+        c4 = c4_section(local)
+        c5 = c5_section(torch, local, peak)
     batch = None
     if not args.no_batch:
         solver.close()
@@ -605,7 +831,7 @@ def main():
     if rank == 0:
         x = d_x.cpu().numpy()
         line = {
-            "metric": "solves/sec at 1e-8 rel. residual (mixed FP32+FP64 refinement)",
+            "metric": METRIC,
             "value": world * 1e3 / ms_mixed,
             "unit": "solves/s",
             "n_gpus": world,
@@ -640,9 +866,15 @@ def main():
             "speedup_mixed_vs_fp64_plain": ms_plain / ms_mixed,
             "speedup_mixed_vs_fp64_fused": ms_fp64 / ms_mixed,
             "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
-                         "peak_kind": peak_kind, "traffic": traffic,
+                         "peak_kind": peak_kind, "traffic": traffic, "traffic_capture": traffic_src,
+                         "limiter": "latency: team barriers, L2 round trips of the gathered vectors and the "
+                                    "shared-memory colour sweeps; A and the CG state stay in shared memory",
+                         "dram_achieved_gbs": (traffic / (ms_mixed * 1e-3) / 1e9) if traffic else None,
+                         "dram_frac": (traffic / (ms_mixed * 1e-3) / 1e9 / peak) if traffic else None,
                          "kernel": f"k_pipe_grid<float,3,2> (row-cached persistent solve, block SSOR, grid {info['grid']})",
-                         "note": "rows of A and the own-row state stay in shared memory, the gathered vectors in L2: DRAM traffic per launch is a small fraction of the algorithmic bytes; latency-bound (team barriers and L2 round trips)",
+                         "note": "achieved = the algorithmic bytes of an unfused solve (every iteration streams A, "
+                                 "the sweeps and the vectors) / device time; dram_* = the bytes the fused kernel "
+                                 "actually moves (ncu) / device time",
                          "algorithmic_bytes_per_launch": bytes_mixed,
                          "fp64_fused_achieved": bytes_fp64 / (ms_fp64 * 1e-3) / 1e9},
             "e2e": {"value": world * 1e3 / ms_e2e, "unit": "solves/s", "h2d_bytes_per_step": int(h_t.numel() * 8),
@@ -657,6 +889,10 @@ def main():
             line["spmv"] = spmv
         if ddm is not None:
             line["ddm"] = ddm
+        if c1 is not None:
+            line["config1_cylinder"] = c1
+            line["config4_adjoint"] = c4
+            line["config5_large"] = c5
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(pos, tris, h, t)
         print(json.dumps(line), flush=True)

@@ -55,9 +55,10 @@ typedef struct {
 
 /* BSSOR: block SSOR, M = (D + L) D^-1 (D + U) over the rows each block of
  * the row-cached kernel owns (couplings between blocks dropped; L / U in the
- * order of a greedy colouring inside the block), applied by colour sweeps in
- * shared memory; no counterpart in the reference (its PCG takes Jacobi or
- * IC(0)).  Fewer iterations than Jacobi at the cost of a sweep per iteration. */
+ * order of a DSatur colouring inside the block, couplings between rows of one
+ * colour dropped on both sides), applied by colour sweeps in shared memory;
+ * no counterpart in the reference (its PCG takes Jacobi or IC(0)).  Fewer
+ * iterations than Jacobi at the cost of a sweep per iteration. */
 enum { CN_PRECOND_JACOBI = 0, CN_PRECOND_IC0 = 1, CN_PRECOND_HSC = 2, CN_PRECOND_BSSOR = 3 };
 /* AUTO: COLOR with IC(0) (its levels), NATURAL otherwise (neighbouring
  * vertices stay neighbouring rows, so row gathers coalesce). */
@@ -100,6 +101,9 @@ typedef struct {
   int32_t max_refine;  /* FP64 residual refinements (mixed precision) */
   double inner_tol;    /* mixed precision: inner relative tolerance */
   int32_t warm_start;  /* 1: start from this handle's previous solution */
+  double wait_limit_ms;  /* bound of every device-side wait of a multi-block solve (its grid
+                          * barriers), in ms; a wait that runs out ends the solve with
+                          * CN_TIMEOUT and leaves the handle usable (0 = 2000 ms) */
 } cn_solve_opts;
 
 typedef struct {
@@ -285,9 +289,11 @@ void* cn_batch_stream(cn_batch_handle b);
 cn_status cn_batch_info(cn_batch_handle b, int64_t* info);
 /* n_meshes + 1 offsets (in doubles) of each mesh's targets and positions. */
 cn_status cn_batch_offsets(cn_batch_handle b, int64_t* tgt_off, int64_t* out_off);
-/* Per-mesh results of the last solve with stats. */
+/* Per-mesh results of the last solve with stats (each array nullable,
+ * n_meshes entries): status, inner iterations, largest relative residual
+ * over the mesh's columns, FP64 residual evaluations after the first. */
 cn_status cn_batch_mesh_stats(cn_batch_handle b, int32_t* status, int32_t* iterations,
-                              double* max_rel_residual);
+                              double* max_rel_residual, int32_t* refinements);
 
 /* FP64 Jacobi-preconditioned CG on a caller-owned device CSR matrix
  * (n rows, sorted columns, FP64 values) for k = 1, 3 or 9 right-hand sides,
@@ -300,20 +306,42 @@ cn_status cn_batch_mesh_stats(cn_batch_handle b, int32_t* status, int32_t* itera
  * the matrix (d_rowptr n+1, d_colidx, d_vals), the right-hand sides d_b
  * (n x k, row-major) and the solution d_x (n x k: initial guess in, solution
  * out); every temporary lives in one fixed device array inside the library
- * (about 14 MB per GPU, kept until the process exits).
+ * (about 14 MB per GPU, kept until the process exits).  The matrix is
+ * trusted, not checked: row pointers non-decreasing from 0, every column
+ * index in [0, n), columns sorted within a row, the matrix symmetric
+ * positive definite.
  *
  * Limits: n <= 65,536 and n * k <= 196,608; larger systems return
  * CN_BAD_INPUT with the reason in cn_last_error().  The stopping test is the
- * relative residual ||b - A x|| <= tol ||b|| per column.  The work is
- * enqueued on `stream` (a cudaStream_t; NULL = the default stream) of the
- * current device; with stats == NULL the call does not synchronise.  Every
- * call shares the same scratch array, so calls that overlap on the GPU (two
- * streams or two threads at once) race and must be serialised by the caller.
- * The first call on a device looks up the array's device address; make that
- * first call before any stream capture. */
+ * relative residual ||b - A x|| <= tol ||b|| per column.  max_iter bounds the
+ * CG iterations of one pass; after a pass the FP64 residual is recomputed
+ * from b - A x and CG restarts from it, at most 4 passes, so a call runs at
+ * most 4 * max_iter iterations.  A grid barrier that waits more than 2 s
+ * ends the call with CN_TIMEOUT.
+ *
+ * The work is enqueued on `stream` (a cudaStream_t; NULL = the default
+ * stream) of the current device.  With stats != NULL the call reads the
+ * statistics back and synchronises the stream, and returns the solve's
+ * status.  With stats == NULL it does neither and CN_OK only means the work
+ * was enqueued; this is the form to use while a stream is being captured
+ * (reading back and synchronising are not allowed during a capture).  The
+ * results of the last call stay in the scratch: after synchronising, read
+ * them with cn_pcg_csr_noalloc_last_stats.
+ *
+ * Every call shares the same scratch array, so calls that overlap on the GPU
+ * (two streams or two threads at once) race and must be serialised by the
+ * caller.  Each call looks up the array's device address on the current
+ * device; the first lookup on a device loads the library's device code, so
+ * make the first call on each device before any stream capture. */
 cn_status cn_pcg_csr_noalloc(int32_t n, const int32_t* d_rowptr, const int32_t* d_colidx,
                              const double* d_vals, int32_t k, const double* d_b, double* d_x,
                              double tol, int32_t max_iter, void* stream, cn_solve_stats* stats);
+/* Statistics of the last cn_pcg_csr_noalloc call on the current device
+ * (status, iterations, FP64 residual passes after the first, k, per-column
+ * relative residuals), read from the scratch with a blocking copy; call it
+ * after synchronising the stream of that call.  Returns that call's status.
+ * No counterpart in the reference. */
+cn_status cn_pcg_csr_noalloc_last_stats(cn_solve_stats* stats);
 
 #ifdef __cplusplus
 }

@@ -105,3 +105,20 @@ def composed_deformation(oracle, pos, tris, h, Fc, Xc):
     x[free_of] = spl.spsolve(A.tocsc(), rhs[free_of])
     x[h] = Xc
     return x
+
+
+def pivot_breakdown_mesh(seed=2566):
+    """A planar 8 x 8 grid with in-plane jitter U(-0.49, 0.49) and x stretched
+    by a seeded factor: its obtuse triangles give large positive off-diagonal
+    entries, and IC(0) of the reduced matrix in colour order meets a
+    non-positive pivot on A and on A + s diag(A) for every retry shift s.
+    Handles: the first row.  Returns (positions, tris, handles)."""
+    from tool_godot_curvenet_b200 import synth
+    rng = np.random.default_rng(seed)
+    a, l = int(rng.integers(4, 10)), int(rng.integers(4, 10))
+    xs, ys = np.meshgrid(np.arange(a, dtype=float), np.arange(l, dtype=float))
+    pos = np.stack([xs.ravel(), ys.ravel(), np.zeros(a * l)], 1)
+    pos[:, :2] += rng.uniform(-0.49, 0.49, (a * l, 2))
+    pos[:, 0] *= float(rng.uniform(0.05, 20))
+    tris = synth._quads(l, a, False, False, lambda r, c: r * a + c)
+    return np.ascontiguousarray(pos), tris, np.arange(a, dtype=np.int32)

@@ -77,3 +77,13 @@ def test_build_without_device_reports_status():
     st = L.lib().cn_build(C.byref(desc), None, C.byref(out))
     assert st in (L.CN_NO_DEVICE, L.CN_CUDA_ERROR)
     assert not out.value
+
+
+def test_oracle_ic0_breaks_down_after_shift_retries(oracle):
+    """The failure-path fixture of tests/test_gpu_failures.py: the oracle's
+    IC(0) in colour order meets a non-positive pivot on A and on every shifted
+    A + s diag(A), so a build reports CN_NONPOS_PIVOT (3)."""
+    from tests.helpers import pivot_breakdown_mesh
+    pos, tris, h = pivot_breakdown_mesh()
+    assert oracle.System(pos, tris, h, ordering=1).status == 3
+    assert oracle.System(pos, tris, h, ordering=1, precond=0).status == 0

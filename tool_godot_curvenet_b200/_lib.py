@@ -35,7 +35,7 @@ class BuildOpts(C.Structure):
 class SolveOpts(C.Structure):
     _fields_ = [("precision", C.c_int32), ("mode", C.c_int32), ("algo", C.c_int32),
                 ("tol", C.c_double), ("max_iter", C.c_int32), ("max_refine", C.c_int32),
-                ("inner_tol", C.c_double), ("warm_start", C.c_int32)]
+                ("inner_tol", C.c_double), ("warm_start", C.c_int32), ("wait_limit_ms", C.c_double)]
 
 
 class BatchStats(C.Structure):
@@ -89,9 +89,10 @@ SIGNATURES = {
     "cn_batch_stream": (_P, [_P]),
     "cn_batch_info": (C.c_int, [_P, C.POINTER(C.c_int64)]),
     "cn_batch_offsets": (C.c_int, [_P, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
-    "cn_batch_mesh_stats": (C.c_int, [_P, _I32P, _I32P, _DP]),
+    "cn_batch_mesh_stats": (C.c_int, [_P, _I32P, _I32P, _DP, _I32P]),
     "cn_pcg_csr_noalloc": (C.c_int, [C.c_int32, _P, _P, _P, C.c_int32, _P, _P, C.c_double, C.c_int32, _P,
                                      C.POINTER(SolveStats)]),
+    "cn_pcg_csr_noalloc_last_stats": (C.c_int, [C.POINTER(SolveStats)]),
 }
 
 _lib = None

@@ -260,12 +260,14 @@ cn_status cn_batch_offsets(cn_batch_handle B, int64_t* tgt_off, int64_t* out_off
   return CN_OK;
 }
 
-cn_status cn_batch_mesh_stats(cn_batch_handle B, int32_t* status, int32_t* iterations, double* max_rel) {
+cn_status cn_batch_mesh_stats(cn_batch_handle B, int32_t* status, int32_t* iterations, double* max_rel,
+                              int32_t* refinements) {
   if (!B) return CN_BAD_INPUT;
   for (int m = 0; m < B->nm; ++m) {
     const DevStats& d = B->h_stats[m];
     if (status) status[m] = d.status;
     if (iterations) iterations[m] = d.iterations;
+    if (refinements) refinements[m] = d.refinements;
     if (max_rel) {
       double mx = 0.0;
       for (int c = 0; c < B->K && c < 32; ++c) mx = std::max(mx, d.rel_residual[c]);

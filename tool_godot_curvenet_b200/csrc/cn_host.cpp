@@ -248,6 +248,7 @@ void cn_default_solve_opts(cn_solve_opts* o) {
   o->max_refine = 8;
   o->inner_tol = 1e-5;
   o->warm_start = 0;
+  o->wait_limit_ms = 2000.0;
 }
 
 const char* cn_status_string(int32_t s) {
@@ -544,7 +545,7 @@ cn_status cn_solve_device(cn_handle S, int32_t k, const double* d_targets, doubl
   a.max_iter = o.max_iter;
   a.max_refine = o.max_refine;
   a.ctl = S->d_ctl; a.stats = S->d_stats;
-  a.timeout_ns = 2000000000LL;
+  a.timeout_ns = o.wait_limit_ms > 0.0 ? (long long)(o.wait_limit_ms * 1e6) : 2000000000LL;
   a.m0 = S->d_m[0]; a.m1 = S->d_m[1]; a.m2 = S->d_m[2]; a.pown = S->d_pown; a.dinv64 = S->D.dinv64;
   if (o.algo == CN_ALGO_PIPELINED && (S->hsc || S->opts.precond != CN_PRECOND_JACOBI)) {
     set_err("the pipelined form needs the Jacobi preconditioner");

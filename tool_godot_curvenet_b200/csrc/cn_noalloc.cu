@@ -11,12 +11,14 @@
 // library, held until the process exits.  The array is shared by every call
 // and keeps the last call's contents: each call rewrites what it needs
 // before use, and calls that overlap on the GPU (two streams, two threads)
-// race on it.  The first call on a device looks up the array's device
-// address (cudaGetSymbolAddress); make that first call before any stream
-// capture.
+// race on it.  Every call looks up the array's device address on the
+// current device (cudaGetSymbolAddress; the first lookup on a device loads
+// the module, so make the first call before any stream capture).  A call
+// without a statistics pointer does not synchronise; its results stay in the
+// scratch until the next call and cn_pcg_csr_noalloc_last_stats reads them
+// once the caller has synchronised.
 #include <cstdio>
 #include <cstring>
-#include <mutex>
 
 #include "cn_pcg_body.cuh"
 
@@ -47,14 +49,12 @@ constexpr size_t kScratchBytes = kOffVec + kNaVectors * kVecBytes;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
-std::mutex g_mu;
-void* g_base[64] = {};
-
-// Per-call preparation: the control block and statistics start at zero, the
+// Per-call preparation: the control block and statistics start at zero (the
+// right-hand-side count goes in the statistics' spare word), the
 // Jacobi scale 1/sqrt(A_ii) (a zero diagonal maps to 0 as in
 // SparseLinAlg.lean:92-97), the identity row map, the empty strictly-lower
 // pattern and the single level [0, n).
-__global__ void k_na_prepare(int n, const int* rowptr, const int* colidx, const double* vals,
+__global__ void k_na_prepare(int n, int k, const int* rowptr, const int* colidx, const double* vals,
                              unsigned char* base) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double* dinv = (double*)(base + kOffDinv);
@@ -64,7 +64,8 @@ __global__ void k_na_prepare(int n, const int* rowptr, const int* colidx, const 
     Control* c = (Control*)(base + kOffCtl);
     c->bar_count = 0; c->bar_gen = 0; c->abort = 0; c->status = 0;
     DevStats* st = (DevStats*)(base + kOffStats);
-    st->status = 0; st->iterations = 0; st->refinements = 0;
+    st->status = 0; st->iterations = 0; st->refinements = 0; st->pad = k;
+    for (int c = 0; c < 32; ++c) st->rel_residual[c] = 0.0;
     int* lev = (int*)(base + kOffLev);
     lev[0] = 0;
     lev[1] = n;
@@ -120,6 +121,34 @@ cn_status na_fail(cn_status s) {
   return s;
 }
 
+// Device address of the scratch on the current device, looked up on every
+// call (a cached address would outlive a context reset).
+cn_status na_base(unsigned char** out) {
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess || !p) {
+    snprintf(g_na_err, sizeof g_na_err, "cudaGetSymbolAddress of the scratch failed: %s", cudaGetErrorString(e));
+    return na_fail(CN_CUDA_ERROR);
+  }
+  *out = (unsigned char*)p;
+  return CN_OK;
+}
+
+cn_status na_stats(const DevStats& ds, cn_solve_stats* stats) {
+  memset(stats, 0, sizeof *stats);
+  stats->status = ds.status;
+  stats->iterations = ds.iterations;
+  stats->refinements = ds.refinements;
+  stats->k = ds.pad;
+  double mx = 0.0;
+  for (int c = 0; c < ds.pad && c < 32; ++c) {
+    stats->rel_residual[c] = ds.rel_residual[c];
+    mx = mx > ds.rel_residual[c] ? mx : ds.rel_residual[c];
+  }
+  stats->max_rel_residual = mx;
+  return (cn_status)ds.status;
+}
+
 }  // namespace
 }  // namespace cn
 
@@ -149,28 +178,14 @@ extern "C" cn_status cn_pcg_csr_noalloc(int32_t n, const int32_t* d_rowptr, cons
     return na_fail(CN_BAD_INPUT);
   }
   int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+  if (cudaGetDevice(&dev) != cudaSuccess) {
     snprintf(g_na_err, sizeof g_na_err, "no current CUDA device");
     return na_fail(CN_NO_DEVICE);
   }
-  void* base = nullptr;
-  {
-    std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_base[dev]) {
-      void* p = nullptr;
-      const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-      if (e != cudaSuccess || !p) {
-        snprintf(g_na_err, sizeof g_na_err, "cudaGetSymbolAddress of the scratch failed: %s",
-                 cudaGetErrorString(e));
-        return na_fail(CN_CUDA_ERROR);
-      }
-      g_base[dev] = p;
-    }
-    base = g_base[dev];
-  }
-  unsigned char* B = (unsigned char*)base;
+  unsigned char* B = nullptr;
+  if (na_base(&B) != CN_OK) return CN_CUDA_ERROR;
   cudaStream_t st = (cudaStream_t)stream;
-  k_na_prepare<<<(n + 1 + 255) / 256, 256, 0, st>>>(n, d_rowptr, d_colidx, d_vals, B);
+  k_na_prepare<<<(n + 1 + 255) / 256, 256, 0, st>>>(n, k, d_rowptr, d_colidx, d_vals, B);
   SolveArgs a{};
   a.n = n;
   a.nlev = 1;
@@ -200,21 +215,28 @@ extern "C" cn_status cn_pcg_csr_noalloc(int32_t n, const int32_t* d_rowptr, cons
   }
   if (!stats) return CN_OK;
   DevStats ds;
-  if (cudaMemcpyAsync(&ds, B + kOffStats, sizeof ds, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-      cudaStreamSynchronize(st) != cudaSuccess) {
-    snprintf(g_na_err, sizeof g_na_err, "solve failed: %s", cudaGetErrorString(cudaGetLastError()));
+  e = cudaMemcpyAsync(&ds, B + kOffStats, sizeof ds, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) {
+    snprintf(g_na_err, sizeof g_na_err, "solve failed: %s", cudaGetErrorString(e));
     return na_fail(CN_CUDA_ERROR);
   }
-  memset(stats, 0, sizeof *stats);
-  stats->status = ds.status;
-  stats->iterations = ds.iterations;
-  stats->refinements = ds.refinements;
-  stats->k = k;
-  double mx = 0.0;
-  for (int c = 0; c < k && c < 32; ++c) {
-    stats->rel_residual[c] = ds.rel_residual[c];
-    mx = mx > ds.rel_residual[c] ? mx : ds.rel_residual[c];
+  return na_stats(ds, stats);
+}
+
+extern "C" cn_status cn_pcg_csr_noalloc_last_stats(cn_solve_stats* stats) {
+  using namespace cn;
+  g_na_err[0] = 0;
+  set_last_error_text("");
+  if (!stats) {
+    snprintf(g_na_err, sizeof g_na_err, "null statistics pointer");
+    return na_fail(CN_BAD_INPUT);
   }
-  stats->max_rel_residual = mx;
-  return (cn_status)ds.status;
+  DevStats ds;
+  const cudaError_t e = cudaMemcpyFromSymbol(&ds, g_noalloc_scratch, sizeof ds, kOffStats, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) {
+    snprintf(g_na_err, sizeof g_na_err, "reading the statistics failed: %s", cudaGetErrorString(e));
+    return na_fail(CN_CUDA_ERROR);
+  }
+  return na_stats(ds, stats);
 }

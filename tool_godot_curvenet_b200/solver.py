@@ -181,12 +181,14 @@ class CutMeshSolver:
     # -- solves
     @staticmethod
     def make_opts(mode="deform", precision="mixed", tol=1e-8, max_iter=2000, max_refine=8,
-                  inner_tol=1e-5, warm_start=False, algo="fused"):
+                  inner_tol=1e-5, warm_start=False, algo="fused", wait_limit_ms=None):
         o = L.SolveOpts()
         L.lib().cn_default_solve_opts(C.byref(o))
         o.mode, o.precision, o.algo = _MODE[mode], _PREC[precision], _ALGO[algo]
         o.tol, o.max_iter, o.max_refine, o.inner_tol = tol, max_iter, max_refine, inner_tol
         o.warm_start = int(bool(warm_start))
+        if wait_limit_ms is not None:
+            o.wait_limit_ms = wait_limit_ms
         return o
 
     def solve(self, targets, x0=None, check=True, **kw):
@@ -334,12 +336,15 @@ class BatchSolver:
     def stream(self):
         return L.lib().cn_batch_stream(self._h)
 
-    def mesh_stats(self):
+    def mesh_stats(self, refinements=False):
+        """(status, iterations, max relative residual[, refinements]) per mesh
+        of the last solve with statistics."""
         st = np.zeros(self.n_meshes, np.int32)
         it = np.zeros(self.n_meshes, np.int32)
         rel = np.zeros(self.n_meshes)
-        L.lib().cn_batch_mesh_stats(self._h, _ip(st), _ip(it), _dp(rel))
-        return st, it, rel
+        ref = np.zeros(self.n_meshes, np.int32)
+        L.lib().cn_batch_mesh_stats(self._h, _ip(st), _ip(it), _dp(rel), _ip(ref))
+        return (st, it, rel, ref) if refinements else (st, it, rel)
 
     def solve(self, targets, check=True, **kw):
         """targets: list of (n_handles_m, k) arrays.  Returns (list of
