@@ -514,9 +514,9 @@ def ddm_section(torch, local):
 def capture_traffic(key, workload, info, stats):
     """DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of
     the ncu capture recorded in profiles/traffic.json under `key`, used only
-    when the capture's workload, launch grid and inner-iteration count match
-    this run's (otherwise the figure belongs to another kernel or workload
-    and None is reported)."""
+    when the capture's workload and launch grid match this run's and its
+    inner-iteration count is within 2% (otherwise the figure belongs to
+    another kernel or workload and None is reported)."""
     try:
         with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
             e = json.load(f)[key]
@@ -524,7 +524,7 @@ def capture_traffic(key, workload, info, stats):
         return None, None
     src = {k: e.get(k) for k in ("workload", "kernel", "grid", "iterations", "source")}
     same = (e.get("workload") == workload and e.get("grid") == info["grid"]
-            and e.get("iterations") == stats.iterations)
+            and abs((e.get("iterations") or 0) - stats.iterations) <= max(2, 0.02 * stats.iterations))
     src["matches_this_run"] = bool(same)
     return (e["dram_bytes_per_launch"] if same else None), src
 

@@ -250,6 +250,64 @@ cn_status cn_adjoint(cn_handle h, const double* dL_dx, double* dL_dcp, double* d
                      const cn_solve_opts* opts, cn_solve_stats* stats);
 
 /* ---------------------------------------------------------------------------
+ * Curvenet: the curve side of the deformer on the GPU (DeGoes22 section 3 as
+ * the reference specifies it in ScaledFrames.lean, SegmentGradient.lean,
+ * IntersectionFrames.lean and CurveInterp.lean).  Each curve is a composite
+ * cubic Bezier (EndToEndExample.lean:52-60 per segment) sampled at
+ * n_samples fixed parameters; consecutive samples bound the polyline
+ * segments (a closed curve's last segment joins its last sample to its
+ * first).  Per segment and side the constraint gradient is
+ *   isolated curve (closed, or no intersection at either end):
+ *     F = (l / l_rest) R(t_rest, t)  (ScaledFrames.lean:71-98, both sides);
+ *   curve with an intersection at one or both ends:
+ *     F^+- = (B S)_posed (B S)_rest^-1  (ScaledFrames.lean:120-170) with the
+ *     scaled frame B S = [t l | (n x t) w | n sqrt(l w)]
+ *     (IntersectionFrames.lean:160-170), where the per-side normal n and
+ *     width w come from the intersection frames of the curve's end segments
+ *     (corner normals with the T-junction fallback, per-side widths:
+ *     IntersectionFrames.lean:65-143) and are interpolated linearly along
+ *     the curve (CurveInterp.lean:45-60), rest and posed separately.
+ * The assembly rules are this library's definition (the reference states the
+ * pieces): a curve end at an intersection leaves along its end segment (the
+ * last segment reversed at the curve's end, where plus and minus swap); with
+ * an intersection at one end only, that end's data hold along the whole
+ * curve; a handle bound to (curve, sample i, side) takes F of the segment
+ * starting at sample i (an open curve's last sample: the last segment) and
+ * X_c = the posed curve point at sample i (EndToEndExample.lean:140-142);
+ * handles bound to no curve keep F = I and X_c = their rest position.
+ * Results equal the FP64 restatement bit for bit (no FMA contraction). */
+typedef struct {
+  int32_t n_curves;
+  int32_t n_segments;          /* cubic segments per curve: 3 n_segments + 1 control points */
+  int32_t n_samples;           /* samples per curve (>= 2) */
+  const double* rest_cp;       /* n_curves x (3 n_segments + 1) x 3 */
+  const double* sample_tau;    /* n_curves x n_samples, strictly rising in [0, n_segments] */
+  const int32_t* closed;       /* n_curves (nullable: all open) */
+  int32_t n_nodes;             /* intersections */
+  const int32_t* node_ptr;     /* n_nodes + 1 */
+  const int32_t* node_ends;    /* per intersection, counter-clockwise: 2 curve + (0 start, 1 end); 2..16 ends */
+  const int32_t* handle_curve; /* per handle of the mesh: curve, or -1 */
+  const int32_t* handle_sample;
+  const int32_t* handle_side;  /* 0: plus side, 1: minus side */
+} cn_curvenet_desc;
+
+/* Bind a curvenet to the handles of h (copies the tables to the device). */
+cn_status cn_bind_curvenet(cn_handle h, const cn_curvenet_desc* net);
+/* F_c (n_poses x n_handles x 9, row-major 3x3) and X_c (n_poses x n_handles
+ * x 3) from posed control points (n_poses x n_curves x (3S+1) x 3): device
+ * pointers, enqueued on the handle's stream (no synchronisation). */
+cn_status cn_curvenet_constraints_device(cn_handle h, int32_t n_poses, const double* d_posed_cp, double* d_Fc,
+                                         double* d_Xc);
+/* The same with host buffers (synchronous). */
+cn_status cn_curvenet_constraints(cn_handle h, int32_t n_poses, const double* posed_cp, double* Fc, double* Xc);
+/* Curves to positions for one pose: F_c and X_c on the GPU, then the
+ * two-stage solve of cn_solve_deformation (DeformSolve.lean:110-135) without
+ * leaving the device; x_out: n_verts x 3 with X_c overlaid.  Needs a build
+ * with max_rhs = 9. */
+cn_status cn_deform_curvenet(cn_handle h, const double* posed_cp, double* x_out, const cn_solve_opts* opts,
+                             cn_solve_stats* stats);
+
+/* ---------------------------------------------------------------------------
  * Batched solves: many meshes of uneven size, each with k right-hand sides
  * (k = 24: 8 poses x 3 coordinates, or k = 3), in ONE persistent,
  * CUDA-graph-captured launch.  Each thread-block cluster takes the next mesh

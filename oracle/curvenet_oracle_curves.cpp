@@ -90,6 +90,238 @@ void orc_isolated_segment_gradient(const double* rp, const double* rq, const dou
   for (int k = 0; k < 9; ++k) F[k] = r * ((I[k] + K[k]) + invd * K2[k]);
 }
 
+// ---------------------------------------------------------------------------
+// The curvenet (DeGoes22 section 3): the primitives of ScaledFrames.lean,
+// IntersectionFrames.lean and CurveInterp.lean, and their assembly into
+// per-handle F_c / X_c as the product documents it (curvenet_b200.h,
+// cn_curvenet_desc).
+
+// ScaledFrames.lean:40-45 tangentLength
+double orc_tangent_length(const double* p, const double* q, double* t) {
+  double d[3] = {q[0] - p[0], q[1] - p[1], q[2] - p[2]};
+  double l = std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+  double inv = l == 0.0 ? 0.0 : 1.0 / l;
+  t[0] = d[0] * inv; t[1] = d[1] * inv; t[2] = d[2] * inv;
+  return l;
+}
+
+// ScaledFrames.lean:71-84 smallestRotation: R = (I + K) + K^2 / (1 + cos)
+void orc_smallest_rotation(const double* f, const double* to, double* R) {
+  double cx = f[1] * to[2] - f[2] * to[1];
+  double cy = f[2] * to[0] - f[0] * to[2];
+  double cz = f[0] * to[1] - f[1] * to[0];
+  double cosT = f[0] * to[0] + f[1] * to[1] + f[2] * to[2];
+  double K[9] = {0.0, -cz, cy, cz, 0.0, -cx, -cy, cx, 0.0};
+  double denom = 1.0 + cosT;
+  double invd = denom == 0.0 ? 0.0 : 1.0 / denom;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double k2 = K[i * 3 + 0] * K[0 * 3 + j] + K[i * 3 + 1] * K[1 * 3 + j] + K[i * 3 + 2] * K[2 * 3 + j];
+      double id = i == j ? 1.0 : 0.0;
+      R[i * 3 + j] = (id + K[i * 3 + j]) + invd * k2;
+    }
+}
+
+// ScaledFrames.lean:59-65 mat3Mul
+void orc_mat3_mul(const double* a, const double* b, double* o) {
+  double t[9];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j)
+      t[i * 3 + j] = a[i * 3 + 0] * b[0 * 3 + j] + a[i * 3 + 1] * b[1 * 3 + j] + a[i * 3 + 2] * b[2 * 3 + j];
+  std::memcpy(o, t, sizeof t);
+}
+
+// ScaledFrames.lean:120-131 mat3Det
+double orc_mat3_det(const double* m) {
+  double a = m[0], b = m[1], c = m[2], d = m[3], e = m[4], f = m[5], g = m[6], h = m[7], i = m[8];
+  return a * (e * i - f * h) - b * (d * i - f * g) + c * (d * h - e * g);
+}
+
+// ScaledFrames.lean:135-160 mat3Inv (adjugate / det; det = 0 gives 0)
+void orc_mat3_inv(const double* m, double* o) {
+  double a = m[0], b = m[1], c = m[2], d = m[3], e = m[4], f = m[5], g = m[6], h = m[7], i = m[8];
+  double det = a * (e * i - f * h) - b * (d * i - f * g) + c * (d * h - e * g);
+  double inv = det == 0.0 ? 0.0 : 1.0 / det;
+  double t[9] = {inv * (e * i - f * h), inv * (c * h - b * i), inv * (b * f - c * e),
+                 inv * (f * g - d * i), inv * (a * i - c * g), inv * (c * d - a * f),
+                 inv * (d * h - e * g), inv * (b * g - a * h), inv * (a * e - b * d)};
+  std::memcpy(o, t, sizeof t);
+}
+
+// ScaledFrames.lean:164-166 deformationGradient = posed * rest^-1
+void orc_deformation_gradient(const double* rest, const double* posed, double* F) {
+  double inv[9];
+  orc_mat3_inv(rest, inv);
+  orc_mat3_mul(posed, inv, F);
+}
+
+// IntersectionFrames.lean:65-110 cornerVectors / cornerNormals (with the
+// T-junction fallback, eps 1e-12); t: n x 3 unit tangents in CCW order.
+void orc_corner_normals(int n, const double* t, double* cv, double* m) {
+  for (int i = 0; i < n; ++i) {
+    const double* a = t + 3 * i;
+    const double* b = t + 3 * ((i + 1) % n);
+    cv[3 * i + 0] = a[1] * b[2] - a[2] * b[1];
+    cv[3 * i + 1] = a[2] * b[0] - a[0] * b[2];
+    cv[3 * i + 2] = a[0] * b[1] - a[1] * b[0];
+  }
+  const double eps = 1.0e-12;
+  for (int i = 0; i < n; ++i) {
+    const double* c = cv + 3 * i;
+    double nrm = std::sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
+    if (nrm > eps) {
+      double s = 1.0 / nrm;
+      m[3 * i + 0] = s * c[0]; m[3 * i + 1] = s * c[1]; m[3 * i + 2] = s * c[2];
+    } else {
+      const double* cP = cv + 3 * ((i + 1) % n);
+      const double* cM = cv + 3 * ((i + n - 1) % n);
+      double sum[3] = {cP[0] + cM[0], cP[1] + cM[1], cP[2] + cM[2]};
+      double sn = std::sqrt(sum[0] * sum[0] + sum[1] * sum[1] + sum[2] * sum[2]);
+      if (sn > eps) {
+        double s = 1.0 / sn;
+        m[3 * i + 0] = s * sum[0]; m[3 * i + 1] = s * sum[1]; m[3 * i + 2] = s * sum[2];
+      } else {
+        m[3 * i + 0] = 0.0; m[3 * i + 1] = 0.0; m[3 * i + 2] = 0.0;
+      }
+    }
+  }
+}
+
+// IntersectionFrames.lean:128-143 perSideWidths
+void orc_per_side_widths(int n, const double* t, const double* l, double* wp, double* wm) {
+  std::vector<double> cv(3 * (size_t)n), m(3 * (size_t)n);
+  orc_corner_normals(n, t, cv.data(), m.data());
+  for (int i = 0; i < n; ++i) {
+    double li = l[i], liP = l[(i + 1) % n], liM = l[(i + n - 1) % n];
+    const double* c = &cv[3 * i];
+    const double* cm = &cv[3 * ((i + n - 1) % n)];
+    double cMag = std::sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
+    double cMagM = std::sqrt(cm[0] * cm[0] + cm[1] * cm[1] + cm[2] * cm[2]);
+    wp[i] = li + cMag * (liP - li);
+    wm[i] = li + cMagM * (liM - li);
+  }
+}
+
+// IntersectionFrames.lean:160-170 scaledFrame
+void orc_scaled_frame(const double* t, const double* n, double l, double w, double* M) {
+  double bx = n[1] * t[2] - n[2] * t[1];
+  double by = n[2] * t[0] - n[0] * t[2];
+  double bz = n[0] * t[1] - n[1] * t[0];
+  double h = std::sqrt(l * w);
+  M[0] = t[0] * l; M[1] = bx * w; M[2] = n[0] * h;
+  M[3] = t[1] * l; M[4] = by * w; M[5] = n[1] * h;
+  M[6] = t[2] * l; M[7] = bz * w; M[8] = n[2] * h;
+}
+
+// CurveInterp.lean:45-60 interpAlongCurve; a side record is (n[3], w) and a
+// segment record (plus side, minus side) = 8 doubles.  out: n x 8.
+void orc_interp_along_curve(const double* first, const double* last, int n, double* out) {
+  if (n <= 0) return;
+  if (n == 1) { for (int k = 0; k < 8; ++k) out[k] = first[k]; return; }
+  double denom = (double)(n - 1);
+  for (int i = 0; i < n; ++i) {
+    double t = (double)i / denom;
+    for (int k = 0; k < 8; ++k) out[8 * i + k] = (1.0 - t) * first[k] + t * last[k];
+  }
+}
+
+// The assembly into F_c / X_c per pose (see cn_curvenet_desc).  Inputs as the
+// product takes them; rest: vertex positions (n_verts x 3), handles: nh ids.
+// Fc: n_poses x nh x 9, Xc: n_poses x nh x 3.  Returns 0, or -1 on a
+// malformed curvenet.
+int orc_curvenet_constraints(int C, int S, int M, const double* rest_cp, const double* tau, const int* closed,
+                             int n_nodes, const int* node_ptr, const int* node_ends, int nh,
+                             const int* h_curve, const int* h_sample, const int* h_side, const int* handles,
+                             const double* rest, int n_poses, const double* posed_cp, double* Fc, double* Xc) {
+  const int np = 3 * S + 1;
+  std::vector<int> seg_off(C + 1, 0), kind(C, 0);
+  for (int c = 0; c < C; ++c) seg_off[c + 1] = seg_off[c] + ((closed && closed[c]) ? M : M - 1);
+  for (int j = 0; j < n_nodes; ++j)
+    for (int q = node_ptr[j]; q < node_ptr[j + 1]; ++q) kind[node_ends[q] >> 1] |= (node_ends[q] & 1) ? 2 : 1;
+  for (int pose = 0; pose < n_poses; ++pose) {
+    const double* PP = posed_cp + (size_t)pose * C * np * 3;
+    // segment records: [cfg][t(3), l]
+    std::vector<double> seg(8 * (size_t)seg_off[C]);
+    for (int c = 0; c < C; ++c)
+      for (int i = 0; i < seg_off[c + 1] - seg_off[c]; ++i) {
+        int j = i + 1 < M ? i + 1 : 0;
+        double* o = &seg[8 * (size_t)(seg_off[c] + i)];
+        for (int cfg = 0; cfg < 2; ++cfg) {
+          const double* P = (cfg == 0 ? rest_cp : PP) + (size_t)c * np * 3;
+          double a[3], b[3];
+          eval_curve(P, S, tau[(size_t)c * M + i], a);
+          eval_curve(P, S, tau[(size_t)c * M + j], b);
+          o[4 * cfg + 3] = orc_tangent_length(a, b, o + 4 * cfg);
+        }
+      }
+    // curve-end side records: [end][cfg][plus n, plus w, minus n, minus w]
+    std::vector<double> ends(32 * (size_t)C, 0.0);
+    for (int jn = 0; jn < n_nodes; ++jn) {
+      int b = node_ptr[jn], n = node_ptr[jn + 1] - b;
+      if (n < 2) return -1;
+      for (int cfg = 0; cfg < 2; ++cfg) {
+        std::vector<double> t(3 * (size_t)n), l(n), cv(3 * (size_t)n), m(3 * (size_t)n), wp(n), wm(n);
+        for (int q = 0; q < n; ++q) {
+          int e = node_ends[b + q], c = e >> 1;
+          int sg = (e & 1) ? seg_off[c + 1] - 1 : seg_off[c];
+          const double* s = &seg[8 * (size_t)sg + 4 * cfg];
+          for (int d = 0; d < 3; ++d) t[3 * q + d] = (e & 1) ? -s[d] : s[d];
+          l[q] = s[3];
+        }
+        orc_corner_normals(n, t.data(), cv.data(), m.data());
+        orc_per_side_widths(n, t.data(), l.data(), wp.data(), wm.data());
+        for (int q = 0; q < n; ++q) {
+          int e = node_ends[b + q];
+          bool swap = (e & 1) != 0;
+          const double* nP = &m[3 * q];
+          const double* nM = &m[3 * ((q + n - 1) % n)];
+          double* o = &ends[(((size_t)(e >> 1)) * 2 + (e & 1)) * 16 + 8 * cfg];
+          const double* a = swap ? nM : nP;
+          const double* bb = swap ? nP : nM;
+          o[0] = a[0]; o[1] = a[1]; o[2] = a[2]; o[3] = swap ? wm[q] : wp[q];
+          o[4] = bb[0]; o[5] = bb[1]; o[6] = bb[2]; o[7] = swap ? wp[q] : wm[q];
+        }
+      }
+    }
+    for (int h = 0; h < nh; ++h) {
+      double* F = Fc + ((size_t)pose * nh + h) * 9;
+      double* X = Xc + ((size_t)pose * nh + h) * 3;
+      int c = h_curve[h];
+      if (c < 0) {
+        for (int k = 0; k < 9; ++k) F[k] = (k % 4 == 0) ? 1.0 : 0.0;
+        for (int d = 0; d < 3; ++d) X[d] = rest[3 * (size_t)handles[h] + d];
+        continue;
+      }
+      int i = h_sample[h], side = h_side[h];
+      int nseg = seg_off[c + 1] - seg_off[c];
+      int si = i < nseg ? i : nseg - 1;
+      const double* s = &seg[8 * (size_t)(seg_off[c] + si)];
+      if (kind[c] == 0) {
+        double R[9];
+        orc_smallest_rotation(s, s + 4, R);
+        double r = s[3] == 0.0 ? 0.0 : s[7] / s[3];
+        for (int k = 0; k < 9; ++k) F[k] = r * R[k];
+      } else {
+        const double* E = &ends[(size_t)c * 32];
+        const double* first = (kind[c] & 1) ? E : E + 16;
+        const double* last = (kind[c] & 2) ? E + 16 : E;
+        double fr[2][9];
+        for (int cfg = 0; cfg < 2; ++cfg) {
+          double f8[8], g8[8];
+          for (int k = 0; k < 8; ++k) { f8[k] = first[8 * cfg + k]; g8[k] = last[8 * cfg + k]; }
+          std::vector<double> arr(8 * (size_t)nseg);
+          orc_interp_along_curve(f8, g8, nseg, arr.data());
+          const double* sd = &arr[8 * (size_t)si + 4 * side];
+          orc_scaled_frame(s + 4 * cfg, sd, s[4 * cfg + 3], sd[3], fr[cfg]);
+        }
+        orc_deformation_gradient(fr[0], fr[1], F);
+      }
+      eval_curve(PP + (size_t)c * np * 3, S, tau[(size_t)c * M + i], X);
+    }
+  }
+  return 0;
+}
+
 // Handle targets from curves.  rest_cp / posed_cp: ncurves x (3S+1) x 3,
 // weights: ncurves, curve_of/tau: per handle, rest: nv x 3, handles: nh.
 // out: nh x 3.

@@ -73,6 +73,18 @@ def lib():
             "orc_bezier3": (None, [_D, C.c_double, _D]),
             "orc_isolated_segment_gradient": (None, [_D, _D, _D, _D, _D]),
             "orc_curve_targets": (None, [C.c_int, C.c_int, _D, _D, _D, C.c_int, _I, _I, _D, _D, _D]),
+            "orc_tangent_length": (C.c_double, [_D, _D, _D]),
+            "orc_smallest_rotation": (None, [_D, _D, _D]),
+            "orc_mat3_mul": (None, [_D, _D, _D]),
+            "orc_mat3_det": (C.c_double, [_D]),
+            "orc_mat3_inv": (None, [_D, _D]),
+            "orc_deformation_gradient": (None, [_D, _D, _D]),
+            "orc_corner_normals": (None, [C.c_int, _D, _D, _D]),
+            "orc_per_side_widths": (None, [C.c_int, _D, _D, _D, _D]),
+            "orc_scaled_frame": (None, [_D, _D, C.c_double, C.c_double, _D]),
+            "orc_interp_along_curve": (None, [_D, _D, C.c_int, _D]),
+            "orc_curvenet_constraints": (C.c_int, [C.c_int, C.c_int, C.c_int, _D, _D, _I, C.c_int, _I, _I, C.c_int,
+                                                   _I, _I, _I, _I, _D, C.c_int, _D, _D, _D]),
             "orc_deform_adjoint": (C.c_double, [_P, C.c_int, _I, _I, _D, C.c_int, _I, C.c_int, C.c_int, _D, _D, _D,
                                                 C.c_int, _I, _I, _D, _D, _D, C.c_double, C.c_int, _D, _D, _D]),
         }
@@ -354,6 +366,99 @@ class System:
         st = lib().orc_system_solve(self._h, k, dp(t), mode, tol, max_iter, threads,
                                     dp(f64(x0)) if x0 is not None else None, dp(x), ip(it), dp(rel))
         return st, x, it, rel
+
+
+# --------------------------------------------------------------------- curvenet (DeGoes22 section 3)
+def tangent_length(p, q):
+    t = np.empty(3)
+    l = lib().orc_tangent_length(dp(f64(p)), dp(f64(q)), dp(t))
+    return t, l
+
+
+def smallest_rotation(a, b):
+    R = np.empty(9)
+    lib().orc_smallest_rotation(dp(f64(a)), dp(f64(b)), dp(R))
+    return R.reshape(3, 3)
+
+
+def isolated_segment_gradient(rp, rq, pp, pq):
+    F = np.empty(9)
+    lib().orc_isolated_segment_gradient(dp(f64(rp)), dp(f64(rq)), dp(f64(pp)), dp(f64(pq)), dp(F))
+    return F.reshape(3, 3)
+
+
+def mat3_mul(a, b):
+    o = np.empty(9)
+    lib().orc_mat3_mul(dp(f64(a).ravel()), dp(f64(b).ravel()), dp(o))
+    return o.reshape(3, 3)
+
+
+def mat3_det(m):
+    return lib().orc_mat3_det(dp(f64(m).ravel()))
+
+
+def mat3_inv(m):
+    o = np.empty(9)
+    lib().orc_mat3_inv(dp(f64(m).ravel()), dp(o))
+    return o.reshape(3, 3)
+
+
+def deformation_gradient(rest, posed):
+    o = np.empty(9)
+    lib().orc_deformation_gradient(dp(f64(rest).ravel()), dp(f64(posed).ravel()), dp(o))
+    return o.reshape(3, 3)
+
+
+def corner_normals(tangents):
+    t = f64(tangents).reshape(-1, 3)
+    cv, m = np.empty_like(t), np.empty_like(t)
+    lib().orc_corner_normals(t.shape[0], dp(t), dp(cv), dp(m))
+    return cv, m
+
+
+def per_side_widths(tangents, lengths):
+    t = f64(tangents).reshape(-1, 3)
+    wp, wm = np.empty(t.shape[0]), np.empty(t.shape[0])
+    lib().orc_per_side_widths(t.shape[0], dp(t), dp(f64(lengths)), dp(wp), dp(wm))
+    return wp, wm
+
+
+def scaled_frame(t, n, l, w):
+    o = np.empty(9)
+    lib().orc_scaled_frame(dp(f64(t)), dp(f64(n)), l, w, dp(o))
+    return o.reshape(3, 3)
+
+
+def interp_along_curve(first, last, n):
+    """first / last: 8 doubles (plus n, plus w, minus n, minus w); (n, 8)."""
+    out = np.empty((max(n, 1), 8))
+    lib().orc_interp_along_curve(dp(f64(first)), dp(f64(last)), n, dp(out))
+    return out[:n]
+
+
+def curvenet_constraints(net, rest_positions, handles, posed_cp):
+    """F_c (poses, nh, 3, 3) and X_c (poses, nh, 3) of a curvenet dict with the
+    fields of cn_curvenet_desc (rest_cp, sample_tau, closed, node_ptr,
+    node_ends, handle_curve, handle_sample, handle_side)."""
+    rest_cp = f64(net["rest_cp"])
+    C, npts, _ = rest_cp.shape
+    S = (npts - 1) // 3
+    tau = f64(net["sample_tau"])
+    M = tau.shape[1]
+    closed = i32(net.get("closed", np.zeros(C)))
+    node_ptr = i32(net.get("node_ptr", [0]))
+    node_ends = i32(net.get("node_ends", [0]) if len(net.get("node_ends", [])) else [0])
+    hc, hs, hd = i32(net["handle_curve"]), i32(net["handle_sample"]), i32(net["handle_side"])
+    P = f64(posed_cp).reshape(-1, C, npts, 3)
+    nh = hc.size
+    F = np.empty((P.shape[0], nh, 9))
+    X = np.empty((P.shape[0], nh, 3))
+    r = lib().orc_curvenet_constraints(C, S, M, dp(rest_cp), dp(tau), ip(closed), node_ptr.size - 1, ip(node_ptr),
+                                       ip(node_ends), nh, ip(hc), ip(hs), ip(hd), ip(i32(handles)),
+                                       dp(f64(rest_positions)), P.shape[0], dp(P), dp(F), dp(X))
+    if r != 0:
+        raise ValueError("malformed curvenet")
+    return F.reshape(P.shape[0], nh, 3, 3), X
 
 
 # --------------------------------------------------------------------- Direct Delta Mush

@@ -205,6 +205,81 @@ def main():
         rec("EndToEndExample.lean:202-211", "curve_deform", P_rest=prest, P_posed=prot, t=0.5, t_fwd=0.6,
             rows={"1": [0.0, 1.0, 0.0], "2": [0.0, 0.5, 0.8660254037844386]}, eps=1e-9, **tws),
     ]
+    # ---------------------------------------------------------------- curvenet frames (DeGoes22 section 3)
+    O3, X1, Y1 = [0.0, 0.0, 0.0], [1.0, 0.0, 0.0], [0.0, 1.0, 0.0]
+    D234 = [2.0, 0.0, 0.0, 0.0, 3.0, 0.0, 0.0, 0.0, 4.0]
+    M121 = [2.0, 1.0, 0.0, 1.0, 2.0, 1.0, 0.0, 1.0, 2.0]
+    M123 = [1.0, 2.0, 3.0, 0.0, 1.0, 4.0, 5.0, 6.0, 0.0]
+    out += [
+        rec("ScaledFrames.lean:163-165", "isolated_gradient", seg=[O3, X1, O3, X1], F=I9, eps=1e-12),
+        rec("ScaledFrames.lean:168-171", "isolated_gradient", seg=[O3, X1, O3, Y1], F=RZ, eps=1e-12),
+        rec("ScaledFrames.lean:174-178", "rotate_vector", a=X1, b=Y1, v=X1, expected=[0.0, 1.0, 0.0], eps=1e-12),
+        rec("ScaledFrames.lean:182-185", "isolated_gradient", seg=[O3, X1, O3, [2.0, 0.0, 0.0]], F=S2, eps=1e-12),
+        rec("ScaledFrames.lean:190-195", "gradient_displacement", seg=[O3, X1, O3, [0.0, 3.0, 0.0]], v=X1,
+            expected=[0.0, 3.0, 0.0], eps=1e-12),
+        rec("ScaledFrames.lean:198-199", "smallest_rotation", a=X1, b=X1, R=I9, eps=1e-12),
+        rec("ScaledFrames.lean:207", "det", M=I9, expected=1.0, eps=1e-12),
+        rec("ScaledFrames.lean:210-212", "det", M=D234, expected=24.0, eps=1e-12),
+        rec("ScaledFrames.lean:215-216", "inv", M=I9, expected=I9, eps=1e-12),
+        rec("ScaledFrames.lean:219-222", "inv", M=D234,
+            expected=[0.5, 0.0, 0.0, 0.0, 1.0 / 3.0, 0.0, 0.0, 0.0, 0.25], eps=1e-12),
+        rec("ScaledFrames.lean:225-227", "inv_times", M=M121, expected=I9, eps=1e-10),
+        rec("ScaledFrames.lean:230-231", "deformation_gradient", rest=I9, posed=I9, F=I9, eps=1e-12),
+        rec("ScaledFrames.lean:234-236", "deformation_gradient", rest=I9, posed=D234, F=D234, eps=1e-12),
+        rec("ScaledFrames.lean:239-241", "deformation_gradient", rest=M121, posed=M121, F=I9, eps=1e-10),
+        rec("ScaledFrames.lean:244-246", "times_inv", M=M121, expected=I9, eps=1e-10),
+        rec("ScaledFrames.lean:249-251", "times_inv", M=M123, expected=I9, eps=1e-10),
+        rec("ScaledFrames.lean:254-256", "inv_times", M=M123, expected=I9, eps=1e-10),
+        rec("ScaledFrames.lean:259-261", "inv_inv", M=M121, expected=M121, eps=1e-9),
+        rec("ScaledFrames.lean:264-266", "times_inv", M=RZ, expected=I9, eps=1e-12),
+        rec("SegmentGradient.lean:88-93", "gradient_pair_isolated", seg=[O3, X1, O3, X1], Fp=I9, Fm=I9, eps=1e-12),
+        rec("SegmentGradient.lean:95-102", "gradient_pair_isolated", seg=[O3, X1, O3, Y1], Fp=RZ, Fm=RZ, eps=1e-12),
+        rec("SegmentGradient.lean:104-113", "gradient_pair_intersection", rp=I9, pp=I9, rm=I9, pm=I9, Fp=I9, Fm=I9,
+            eps=1e-12),
+        rec("SegmentGradient.lean:115-133", "gradient_pair_intersection", rp=I9,
+            pp=[1.0, 0.0, 0.0, 0.0, 2.0, 0.0, 0.0, 0.0, 1.0], rm=I9, pm=I9,
+            Fp=[1.0, 0.0, 0.0, 0.0, 2.0, 0.0, 0.0, 0.0, 1.0], Fm=I9, eps=1e-12),
+    ]
+    perp = [[1.0, 0.0, 0.0], [0.0, 1.0, 0.0]]
+    s60, c60 = 0.8660254037844386, 0.5
+    trij = [[1.0, 0.0, 0.0], [-c60, s60, 0.0], [-c60, -s60, 0.0]]
+    tj = [[1.0, 0.0, 0.0], [0.0, 1.0, 0.0], [-1.0, 0.0, 0.0]]
+    out += [
+        rec("IntersectionFrames.lean:189-197", "corner_normals", t=perp, m=[[0.0, 0.0, 1.0], [0.0, 0.0, -1.0]],
+            eps=1e-12),
+        rec("IntersectionFrames.lean:199-205", "per_side_normals", t=perp, seg=0, np=[0.0, 0.0, 1.0],
+            nm=[0.0, 0.0, -1.0], eps=1e-12),
+        rec("IntersectionFrames.lean:215-222", "corner_normals_z", t=trij, z=[1.0, 1.0, 1.0], eps=1e-12),
+        rec("IntersectionFrames.lean:226-231", "widths", t=trij, l=[1.0, 1.0, 1.0], seg=0, wp=1.0, wm=1.0,
+            eps=1e-12),
+        rec("IntersectionFrames.lean:240-244", "widths", t=perp, l=[1.0, 3.0], seg=0, wp=3.0, wm=3.0, eps=1e-12),
+        rec("IntersectionFrames.lean:257-259", "scaled_frame", t=X1, n=[0.0, 0.0, 1.0], l=1.0, w=1.0, M=I9,
+            eps=1e-12),
+        rec("IntersectionFrames.lean:263-271", "scaled_frame", t=X1, n=[0.0, 0.0, 1.0], l=2.0, w=3.0,
+            M=[2.0, 0.0, 0.0, 0.0, 3.0, 0.0, 0.0, 0.0, math.sqrt(6.0)], eps=1e-12),
+        rec("IntersectionFrames.lean:275-282", "per_side_frames", t=perp, l=[1.0, 1.0], seg=0,
+            entries=[["p", 0, 1.0], ["p", 8, 1.0], ["m", 0, 1.0], ["m", 8, -1.0]], eps=1e-12),
+        rec("IntersectionFrames.lean:301-305", "corner_vector", t=tj, i=2, expected=[0.0, 0.0, 0.0], eps=1e-12),
+        rec("IntersectionFrames.lean:309-314", "corner_normals_z", t=tj, z=[1.0, 1.0, 1.0], eps=1e-12),
+        rec("IntersectionFrames.lean:317-322", "normal_unit", t=tj, i=2, eps=1e-12),
+        rec("IntersectionFrames.lean:329-339", "normals_reflect", t=perp, eps=1e-12),
+        rec("IntersectionFrames.lean:343-350", "widths_equal", t=trij, l=[1.0, 1.0, 1.0], eps=1e-12),
+        rec("IntersectionFrames.lean:354-368", "frame_homogeneous", t=X1, n=[0.0, 0.0, 1.0], l=1.0, s=2.0,
+            eps=1e-12),
+    ]
+    first = [0.0, 0.0, 1.0, 1.0, 0.0, 0.0, -1.0, 1.0]
+    last = [1.0, 0.0, 0.0, 5.0, -1.0, 0.0, 0.0, 3.0]
+    out += [
+        rec("CurveInterp.lean:86-95", "interp", first=first, last=last, n=2,
+            entries=[[0, 3, 1.0], [0, 2, 1.0], [1, 3, 5.0], [1, 0, 1.0], [0, 6, -1.0], [1, 4, -1.0]], eps=1e-12),
+        rec("CurveInterp.lean:98-110", "interp", first=first, last=last, n=3,
+            entries=[[1, 0, 0.5], [1, 1, 0.0], [1, 2, 0.5], [1, 3, 3.0], [1, 4, -0.5], [1, 6, -0.5], [1, 7, 2.0]],
+            eps=1e-12),
+        rec("CurveInterp.lean:112-120", "interp", first=first, last=last, n=5,
+            entries=[[1, 3, 2.0], [2, 3, 3.0]], eps=1e-12),
+        rec("CurveInterp.lean:122-125", "interp_size", first=first, last=last, n=1, size=1),
+        rec("CurveInterp.lean:127-130", "interp_size", first=first, last=last, n=0, size=0),
+    ]
     # ---------------------------------------------------------------- Direct Delta Mush
     ident = [1.0, 0.0, 0.0, 0.0, 0.0, 1.0, 0.0, 0.0, 0.0, 0.0, 1.0, 0.0, 0.0, 0.0, 0.0, 1.0]
 

@@ -122,3 +122,65 @@ def pivot_breakdown_mesh(seed=2566):
     pos[:, 0] *= float(rng.uniform(0.05, 20))
     tris = synth._quads(l, a, False, False, lambda r, c: r * a + c)
     return np.ascontiguousarray(pos), tris, np.arange(a, dtype=np.int32)
+
+
+def line_curve(p0, p1, nseg=1):
+    """A composite cubic Bezier of nseg segments along the straight line p0 -> p1
+    (control points at thirds), (3 nseg + 1, 3)."""
+    p0, p1 = np.asarray(p0, float), np.asarray(p1, float)
+    s = np.linspace(0.0, 1.0, 3 * nseg + 1)
+    return p0[None, :] + s[:, None] * (p1 - p0)[None, :]
+
+
+def star_curvenet(nh, n_samples=6, seed=0):
+    """Intersection test net: four open curves leaving one node along +x, +y,
+    -x, -y (counter-clockwise), each bent by seeded control-point noise, plus
+    a triangle of three curves whose corners are three more nodes (both ends
+    of each curve at a node), plus a T-junction (two anti-parallel curves and
+    one perpendicular).  Handles 0..nh-1 are bound round-robin to (curve,
+    sample, side); every 7th stays unbound.  Returns (net dict, rest_cp)."""
+    rng = np.random.default_rng(seed)
+    curves = []
+    for d in ([1, 0, 0], [0, 1, 0], [-1, 0, 0], [0, -1, 0]):
+        curves.append(line_curve([0, 0, 0], np.asarray(d, float) * 2.0, 2))
+    tri = [np.array([3.0, 0.0, 0.2]), np.array([4.0, 1.5, 0.0]), np.array([2.5, 1.2, -0.3])]
+    for i in range(3):
+        curves.append(line_curve(tri[i], tri[(i + 1) % 3], 2))
+    c0 = np.array([0.0, -3.0, 0.0])
+    curves.append(line_curve(c0, c0 + [1.5, 0, 0], 2))
+    curves.append(line_curve(c0, c0 + [0, 1.5, 0], 2))
+    curves.append(line_curve(c0, c0 + [-1.5, 0, 0], 2))
+    rest_cp = np.array(curves)
+    # interior control points bent a little (ends stay on the nodes)
+    rest_cp[:, 1:-1] += rng.normal(0.0, 0.05, rest_cp[:, 1:-1].shape)
+    C = rest_cp.shape[0]
+    S = (rest_cp.shape[1] - 1) // 3
+    tau = np.tile(np.linspace(0.0, S, n_samples), (C, 1))
+    node_ptr = [0, 4, 6, 8, 10, 13]
+    node_ends = [2 * 0, 2 * 1, 2 * 2, 2 * 3,                  # star centre, CCW
+                 2 * 4 + 0, 2 * 6 + 1, 2 * 5 + 0, 2 * 4 + 1,  # triangle corners
+                 2 * 6 + 0, 2 * 5 + 1,
+                 2 * 7, 2 * 8, 2 * 9]                          # T-junction: +x, +y, -x
+    hc = np.array([(h % C) if h % 7 else -1 for h in range(nh)], np.int32)
+    hs = np.array([(h // C) % n_samples for h in range(nh)], np.int32)
+    hd = np.array([(h // (C * n_samples)) % 2 for h in range(nh)], np.int32)
+    net = dict(rest_cp=rest_cp, sample_tau=tau, closed=np.zeros(C, np.int32), node_ptr=np.array(node_ptr, np.int32),
+               node_ends=np.array(node_ends, np.int32), handle_curve=hc, handle_sample=hs, handle_side=hd)
+    return net, rest_cp
+
+
+def loop_curvenet(seed=4, nseg=5):
+    """The adjoint workload's torus 128 x 64 with its 4 seams as closed
+    profile curves (isolated): every seam vertex and its copy bound to its
+    curve's sample (plus side for the original, minus for the copy).
+    Returns (positions, tris, handles, net dict)."""
+    from tool_godot_curvenet_b200 import synth
+    pos, tris, h, cof, tau, rest_cp, _, _, _, _ = synth.config4(seed, nseg)
+    V = 64
+    samples = np.tile(nseg * np.arange(V) / V, (rest_cp.shape[0], 1))
+    hs = np.rint(np.asarray(tau) * V / nseg).astype(np.int32)
+    hd = np.tile(np.array([0, 1], np.int32), h.size // 2)
+    net = dict(rest_cp=rest_cp, sample_tau=samples, closed=np.ones(rest_cp.shape[0], np.int32),
+               node_ptr=np.zeros(1, np.int32), node_ends=np.zeros(0, np.int32), handle_curve=np.asarray(cof, np.int32),
+               handle_sample=hs, handle_side=hd)
+    return pos, tris, h, net

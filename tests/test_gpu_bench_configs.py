@@ -55,7 +55,7 @@ def oracle_solution(name, tol=1e-13):
     pos, tris, h, t = workload(name)
     t = t[:, :3] if name in ("c2", "c5") else t
     st, x, _, rel = O.System(pos, tris, h).solve(t, mode=1, tol=tol, threads=3)
-    assert st == 0 and np.all(rel <= tol * 1.0001)
+    assert st == 0 and np.all(rel <= 2 * tol)  # the oracle stops on its recursive residual
     return x
 
 

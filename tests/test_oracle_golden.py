@@ -36,6 +36,97 @@ def fid(f):
     return f"{f['src']}:{f['kind']}"
 
 
+CURVENET_KINDS = ("isolated_gradient", "rotate_vector", "gradient_displacement", "smallest_rotation", "det",
+                  "inv", "inv_times", "times_inv", "inv_inv", "deformation_gradient", "gradient_pair_isolated",
+                  "gradient_pair_intersection", "corner_normals", "per_side_normals", "corner_normals_z", "widths",
+                  "scaled_frame", "per_side_frames", "corner_vector", "normal_unit", "normals_reflect",
+                  "widths_equal", "frame_homogeneous", "interp", "interp_size")
+
+
+def check_curvenet_fixture(O, f):
+    """ScaledFrames.lean, SegmentGradient.lean, IntersectionFrames.lean and
+    CurveInterp.lean examples against the oracle's primitives."""
+    k = f["kind"]
+    eps = f.get("eps", 0.0)
+
+    def close(a, b, e=eps):
+        return np.all(np.abs(np.asarray(a, float).ravel() - np.asarray(b, float).ravel()) < e)
+
+    def m3(x):
+        return np.asarray(x, float).reshape(3, 3)
+    if k == "isolated_gradient":
+        assert close(O.isolated_segment_gradient(*f["seg"]), f["F"])
+    elif k == "rotate_vector":
+        assert close(m3(O.smallest_rotation(f["a"], f["b"])) @ np.asarray(f["v"]), f["expected"])
+    elif k == "gradient_displacement":
+        F = O.isolated_segment_gradient(*f["seg"])
+        assert close(F @ np.asarray(f["v"]), f["expected"])
+    elif k == "smallest_rotation":
+        assert close(O.smallest_rotation(f["a"], f["b"]), f["R"])
+    elif k == "det":
+        assert abs(O.mat3_det(f["M"]) - f["expected"]) < eps
+    elif k == "inv":
+        assert close(O.mat3_inv(f["M"]), f["expected"])
+    elif k == "inv_times":
+        assert close(O.mat3_mul(O.mat3_inv(f["M"]), f["M"]), f["expected"])
+    elif k == "times_inv":
+        assert close(O.mat3_mul(f["M"], O.mat3_inv(f["M"])), f["expected"])
+    elif k == "inv_inv":
+        assert close(O.mat3_inv(O.mat3_inv(f["M"])), f["expected"])
+    elif k == "deformation_gradient":
+        assert close(O.deformation_gradient(f["rest"], f["posed"]), f["F"])
+    elif k == "gradient_pair_isolated":  # both sides take the isolated gradient
+        F = O.isolated_segment_gradient(*f["seg"])
+        assert close(F, f["Fp"]) and close(F, f["Fm"])
+    elif k == "gradient_pair_intersection":
+        assert close(O.deformation_gradient(f["rp"], f["pp"]), f["Fp"])
+        assert close(O.deformation_gradient(f["rm"], f["pm"]), f["Fm"])
+    elif k == "corner_normals":
+        assert close(O.corner_normals(f["t"])[1], f["m"])
+    elif k == "per_side_normals":
+        m = O.corner_normals(f["t"])[1]
+        i, n = f["seg"], len(f["t"])
+        assert close(m[i], f["np"]) and close(m[(i + n - 1) % n], f["nm"])
+    elif k == "corner_normals_z":
+        assert close(O.corner_normals(f["t"])[1][:, 2], f["z"])
+    elif k == "widths":
+        wp, wm = O.per_side_widths(f["t"], f["l"])
+        assert abs(wp[f["seg"]] - f["wp"]) < eps and abs(wm[f["seg"]] - f["wm"]) < eps
+    elif k == "scaled_frame":
+        assert close(O.scaled_frame(f["t"], f["n"], f["l"], f["w"]), f["M"])
+    elif k == "per_side_frames":
+        t = np.asarray(f["t"], float)
+        m = O.corner_normals(t)[1]
+        wp, wm = O.per_side_widths(t, f["l"])
+        i, n = f["seg"], t.shape[0]
+        Bp = O.scaled_frame(t[i], m[i], f["l"][i], wp[i]).ravel()
+        Bm = O.scaled_frame(t[i], m[(i + n - 1) % n], f["l"][i], wm[i]).ravel()
+        for side, idx, want in f["entries"]:
+            assert abs((Bp if side == "p" else Bm)[idx] - want) < eps
+    elif k == "corner_vector":
+        assert close(O.corner_normals(f["t"])[0][f["i"]], f["expected"])
+    elif k == "normal_unit":
+        assert abs(np.linalg.norm(O.corner_normals(f["t"])[1][f["i"]]) - 1.0) < eps
+    elif k == "normals_reflect":
+        m = O.corner_normals(f["t"])[1]
+        n = m.shape[0]
+        for i in range(n):
+            assert close(m[i] + m[(i + n - 1) % n], np.zeros(3))
+    elif k == "widths_equal":
+        wp, wm = O.per_side_widths(f["t"], f["l"])
+        assert close(wp, wm)
+    elif k == "frame_homogeneous":
+        a = O.scaled_frame(f["t"], f["n"], f["l"], f["l"])
+        b = O.scaled_frame(f["t"], f["n"], f["s"] * f["l"], f["s"] * f["l"])
+        assert close(b, f["s"] * a)
+    elif k == "interp":
+        arr = O.interp_along_curve(f["first"], f["last"], f["n"])
+        for i, j, want in f["entries"]:
+            assert abs(arr[i, j] - want) < eps
+    elif k == "interp_size":
+        assert O.interp_along_curve(f["first"], f["last"], f["n"]).shape[0] == f["size"]
+
+
 @pytest.mark.parametrize("f", FIX, ids=[fid(f) for f in FIX])
 def test_known_answer(f, oracle):
     O = oracle
@@ -250,6 +341,8 @@ def test_known_answer(f, oracle):
         dense = np.zeros_like(W)
         np.put_along_axis(dense, idx, w, axis=1)
         assert np.all(np.abs(dense.sum(axis=1) - 1.0) < eps)
+    elif k in CURVENET_KINDS:
+        check_curvenet_fixture(O, f)
     else:
         pytest.fail(f"unknown fixture kind {k}")
 

@@ -38,6 +38,14 @@ class SolveOpts(C.Structure):
                 ("inner_tol", C.c_double), ("warm_start", C.c_int32), ("wait_limit_ms", C.c_double)]
 
 
+class CurvenetDesc(C.Structure):
+    _fields_ = [("n_curves", C.c_int32), ("n_segments", C.c_int32), ("n_samples", C.c_int32),
+                ("rest_cp", C.POINTER(C.c_double)), ("sample_tau", C.POINTER(C.c_double)),
+                ("closed", C.POINTER(C.c_int32)), ("n_nodes", C.c_int32), ("node_ptr", C.POINTER(C.c_int32)),
+                ("node_ends", C.POINTER(C.c_int32)), ("handle_curve", C.POINTER(C.c_int32)),
+                ("handle_sample", C.POINTER(C.c_int32)), ("handle_side", C.POINTER(C.c_int32))]
+
+
 class BatchStats(C.Structure):
     _fields_ = [("status", C.c_int32), ("n_meshes", C.c_int32), ("n_failed", C.c_int32),
                 ("max_iterations", C.c_int32), ("total_iterations", C.c_int64),
@@ -81,6 +89,10 @@ SIGNATURES = {
     "cn_bind_curves": (C.c_int, [_P, C.c_int32, C.c_int32, _DP, _I32P, _DP]),
     "cn_deform": (C.c_int, [_P, _DP, _DP, _DP, C.POINTER(SolveOpts), C.POINTER(SolveStats)]),
     "cn_adjoint": (C.c_int, [_P, _DP, _DP, _DP, C.POINTER(SolveOpts), C.POINTER(SolveStats)]),
+    "cn_bind_curvenet": (C.c_int, [_P, C.POINTER(CurvenetDesc)]),
+    "cn_curvenet_constraints_device": (C.c_int, [_P, C.c_int32, _P, _P, _P]),
+    "cn_curvenet_constraints": (C.c_int, [_P, C.c_int32, _DP, _DP, _DP]),
+    "cn_deform_curvenet": (C.c_int, [_P, _DP, _DP, C.POINTER(SolveOpts), C.POINTER(SolveStats)]),
     "cn_build_batch": (C.c_int, [C.POINTER(MeshDesc), C.c_int32, C.POINTER(BuildOpts), C.c_int32, C.c_int32,
                                  C.c_int32, C.POINTER(_P)]),
     "cn_destroy_batch": (None, [_P]),

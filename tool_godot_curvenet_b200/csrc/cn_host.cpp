@@ -86,6 +86,13 @@ struct cn_system {
   int *d_curve_of = nullptr, *d_row_of = nullptr;
   double *d_tau = nullptr, *d_rest_cp = nullptr, *d_posed_cp = nullptr, *d_weights = nullptr;
   double *d_dLdx = nullptr, *d_dP = nullptr, *d_dw = nullptr;
+  // profile curvenet (cn_bind_curvenet): bound tables, per-pose scratch and
+  // the host-call staging buffers, own allocations
+  bool have_cnet = false;
+  cn::CurvenetArgs cnet{};
+  std::vector<void*> cnet_mem;
+  int cnet_pose_cap = 0;
+  double *d_cnet_posed = nullptr, *d_cnet_F = nullptr, *d_cnet_X = nullptr;
 };
 
 namespace {
@@ -408,6 +415,10 @@ void cn_destroy(cn_handle S) {
   if (S->stream) cudaStreamSynchronize(S->stream);
   if (S->buf) cudaFree(S->buf);
   for (void* p : S->hsc_mem) cudaFree(p);
+  for (void* p : S->cnet_mem) cudaFree(p);
+  for (void* p : {(void*)S->cnet.seg, (void*)S->cnet.ends, (void*)S->d_cnet_posed, (void*)S->d_cnet_F,
+                  (void*)S->d_cnet_X})
+    if (p) cudaFree(p);
   for (void* p : {(void*)S->d_curve_of, (void*)S->d_row_of, (void*)S->d_tau, (void*)S->d_rest_cp,
                   (void*)S->d_posed_cp, (void*)S->d_weights, (void*)S->d_dLdx, (void*)S->d_dP, (void*)S->d_dw,
                   (void*)S->d_vf_ptr, (void*)S->d_vf_face, (void*)S->d_vf_corner, (void*)S->d_contrib,
@@ -948,6 +959,53 @@ cn_status cn_adjoint(cn_handle S, const double* dL_dx, double* dL_dcp, double* d
 
 // DeGoes22 two-stage solve (DeformSolve.lean:110-135): Stage 1 (k = 9
 // harmonic solve of F), the bridge (cn_deform.cu), Stage 2 (k = 3).
+// Device tables of the two-stage solve (vertex -> incident faces, per-face
+// contributions, X_c), allocated on first use.
+static cn_status ensure_deform_tables(cn_handle S) {
+  const MeshHost& H = S->H;
+  if (S->d_vf_ptr) return CN_OK;
+  CN_CUDA(cudaMalloc((void**)&S->d_vf_ptr, sizeof(int) * H.vf_ptr.size()));
+  CN_CUDA(cudaMalloc((void**)&S->d_vf_face, sizeof(int) * std::max<size_t>(H.vf_face.size(), 1)));
+  CN_CUDA(cudaMalloc((void**)&S->d_vf_corner, sizeof(int) * std::max<size_t>(H.vf_corner.size(), 1)));
+  CN_CUDA(cudaMalloc((void**)&S->d_contrib, sizeof(double) * 9 * std::max(H.nt, 1)));
+  CN_CUDA(cudaMalloc((void**)&S->d_Xc, sizeof(double) * 3 * std::max(H.nh, 1)));
+  CN_CUDA(cudaMemcpy(S->d_vf_ptr, H.vf_ptr.data(), sizeof(int) * H.vf_ptr.size(), cudaMemcpyHostToDevice));
+  if (!H.vf_face.empty()) {
+    CN_CUDA(cudaMemcpy(S->d_vf_face, H.vf_face.data(), sizeof(int) * H.vf_face.size(), cudaMemcpyHostToDevice));
+    CN_CUDA(cudaMemcpy(S->d_vf_corner, H.vf_corner.data(), sizeof(int) * H.vf_corner.size(),
+                       cudaMemcpyHostToDevice));
+  }
+  return CN_OK;
+}
+
+// DeformSolve.lean:110-135 from F_c in d_targets (n_handles x 9) and X_c in
+// d_Xc (n_handles x 3), both on the device: Stage 1 (k = 9 harmonic solve),
+// the Eq.(3) bridge, Stage 2 (k = 3); positions in d_xout, handle rows not
+// yet overlaid.
+static cn_status deform_stages(cn_handle S, const cn_solve_opts& o, cn_solve_stats* stats) {
+  const MeshHost& H = S->H;
+  cn_solve_opts o1 = o;
+  o1.mode = CN_MODE_HARMONIC;
+  o1.warm_start = 0;
+  cn_solve_stats s1;
+  cn_status st = cn_solve_device(S, 9, S->d_targets, S->d_xout, &o1, &s1);
+  if (st != CN_OK) return st;
+  cn::DeformArgs d{};
+  d.nt = H.nt; d.n = H.n; d.tris = S->D.tris; d.pos = S->D.pos; d.face_m = S->D.face_m;
+  d.hidx = S->D.hidx; d.Fv = S->d_xout; d.Xc = S->d_Xc; d.free_of = S->D.free_of;
+  d.vf_ptr = S->d_vf_ptr; d.vf_face = S->d_vf_face; d.vf_corner = S->d_vf_corner;
+  d.contrib = S->d_contrib; d.b = S->d_targets;
+  CN_CUDA(cn::launch_deform_bridge(d, S->stream));
+  cn_solve_opts o2 = o;
+  o2.mode = CN_MODE_RHS;
+  o2.warm_start = 0;
+  cn_solve_stats s2;
+  st = cn_solve_device(S, 3, S->d_targets, S->d_xout, &o2, stats ? stats : &s2);
+  S->have_solution = false;
+  if (stats) stats->iterations += s1.iterations;
+  return st;
+}
+
 cn_status cn_solve_deformation(cn_handle S, const double* Fc, const double* Xc, double* x_out,
                                const cn_solve_opts* opts, cn_solve_stats* stats) {
   if (!S || !Fc || !Xc || !x_out) {
@@ -970,50 +1028,234 @@ cn_status cn_solve_deformation(cn_handle S, const double* Fc, const double* Xc, 
       return CN_NAN;
     }
   CN_CUDA(cudaSetDevice(S->device));
-  if (!S->d_vf_ptr) {
-    CN_CUDA(cudaMalloc((void**)&S->d_vf_ptr, sizeof(int) * H.vf_ptr.size()));
-    CN_CUDA(cudaMalloc((void**)&S->d_vf_face, sizeof(int) * std::max<size_t>(H.vf_face.size(), 1)));
-    CN_CUDA(cudaMalloc((void**)&S->d_vf_corner, sizeof(int) * std::max<size_t>(H.vf_corner.size(), 1)));
-    CN_CUDA(cudaMalloc((void**)&S->d_contrib, sizeof(double) * 9 * std::max(H.nt, 1)));
-    CN_CUDA(cudaMalloc((void**)&S->d_Xc, sizeof(double) * 3 * std::max(H.nh, 1)));
-    CN_CUDA(cudaMemcpy(S->d_vf_ptr, H.vf_ptr.data(), sizeof(int) * H.vf_ptr.size(), cudaMemcpyHostToDevice));
-    if (!H.vf_face.empty()) {
-      CN_CUDA(cudaMemcpy(S->d_vf_face, H.vf_face.data(), sizeof(int) * H.vf_face.size(), cudaMemcpyHostToDevice));
-      CN_CUDA(cudaMemcpy(S->d_vf_corner, H.vf_corner.data(), sizeof(int) * H.vf_corner.size(),
-                         cudaMemcpyHostToDevice));
-    }
-  }
+  cn_status st = ensure_deform_tables(S);
+  if (st != CN_OK) return st;
   cn_solve_opts o;
   if (opts) o = *opts;
   else cn_default_solve_opts(&o);
-  o.warm_start = 0;
-  // Stage 1: F_v, handles overlaid with F_c, into d_xout (n_verts x 9)
   if (H.nh) CN_CUDA(cudaMemcpyAsync(S->d_targets, Fc, sizeof(double) * 9 * H.nh, cudaMemcpyHostToDevice, S->stream));
   CN_CUDA(cudaMemcpyAsync(S->d_Xc, Xc, sizeof(double) * 3 * std::max(H.nh, 0), cudaMemcpyHostToDevice, S->stream));
-  cn_solve_opts o1 = o;
-  o1.mode = CN_MODE_HARMONIC;
-  cn_solve_stats s1;
-  cn_status st = cn_solve_device(S, 9, S->d_targets, S->d_xout, &o1, &s1);
-  if (st != CN_OK) return st;
-  // bridge: Stage-2 right-hand side (solve order) into d_targets
-  cn::DeformArgs d{};
-  d.nt = H.nt; d.n = H.n; d.tris = S->D.tris; d.pos = S->D.pos; d.face_m = S->D.face_m;
-  d.hidx = S->D.hidx; d.Fv = S->d_xout; d.Xc = S->d_Xc; d.free_of = S->D.free_of;
-  d.vf_ptr = S->d_vf_ptr; d.vf_face = S->d_vf_face; d.vf_corner = S->d_vf_corner;
-  d.contrib = S->d_contrib; d.b = S->d_targets;
-  CN_CUDA(cn::launch_deform_bridge(d, S->stream));
-  // Stage 2, then the overlay of X_c on the handles (DeformSolve.lean:108-109)
-  cn_solve_opts o2 = o;
-  o2.mode = CN_MODE_RHS;
-  cn_solve_stats s2;
-  st = cn_solve_device(S, 3, S->d_targets, S->d_xout, &o2, stats ? stats : &s2);
-  S->have_solution = false;
+  st = deform_stages(S, o, stats);
   if (st != CN_OK && st != CN_MAX_ITER) return st;
   CN_CUDA(cudaMemcpyAsync(x_out, S->d_xout, sizeof(double) * 3 * (size_t)H.nv, cudaMemcpyDeviceToHost, S->stream));
   CN_CUDA(cudaStreamSynchronize(S->stream));
   for (int h = 0; h < H.nh; ++h)
     for (int c = 0; c < 3; ++c) x_out[3 * (size_t)H.handles[h] + c] = Xc[3 * (size_t)h + c];
-  if (stats) stats->iterations += s1.iterations;
+  return st;
+}
+
+// ---------------------------------------------------------------------------
+// Profile curvenet (cn_curvenet.cu holds the kernels and the rules).
+
+static cn_status cnet_upload_bytes(cn_system* S, void** dst, const void* h, size_t bytes) {
+  void* d = nullptr;
+  CN_CUDA(cudaMalloc(&d, std::max<size_t>(bytes, 8)));
+  S->cnet_mem.push_back(d);
+  if (bytes) CN_CUDA(cudaMemcpy(d, h, bytes, cudaMemcpyHostToDevice));
+  *dst = d;
+  return CN_OK;
+}
+static cn_status cnet_upload_i(cn_system* S, const int** dst, const int* h, size_t n) {
+  return cnet_upload_bytes(S, (void**)dst, h, sizeof(int) * n);
+}
+static cn_status cnet_upload_d(cn_system* S, const double** dst, const double* h, size_t n) {
+  return cnet_upload_bytes(S, (void**)dst, h, sizeof(double) * n);
+}
+
+cn_status cn_bind_curvenet(cn_handle S, const cn_curvenet_desc* net) {
+  if (!S || !net || !net->rest_cp || !net->sample_tau || !net->handle_curve || !net->handle_sample ||
+      !net->handle_side) {
+    set_err("null argument");
+    return CN_BAD_INPUT;
+  }
+  const int C = net->n_curves, Sg = net->n_segments, M = net->n_samples, nn = net->n_nodes;
+  if (C < 1 || Sg < 1 || M < 2 || nn < 0 || (nn > 0 && (!net->node_ptr || !net->node_ends))) {
+    set_err("cn_bind_curvenet: need n_curves >= 1, n_segments >= 1, n_samples >= 2 and node tables");
+    return CN_BAD_INPUT;
+  }
+  const size_t np = 3 * (size_t)Sg + 1;
+  for (size_t i = 0; i < (size_t)C * np * 3; ++i)
+    if (!std::isfinite(net->rest_cp[i])) {
+      set_err("rest control point %zu is not finite", i);
+      return CN_NAN;
+    }
+  for (int c = 0; c < C; ++c)
+    for (int i = 0; i < M; ++i) {
+      const double t = net->sample_tau[(size_t)c * M + i];
+      if (!(t >= 0.0 && t <= (double)Sg) || (i > 0 && !(t > net->sample_tau[(size_t)c * M + i - 1]))) {
+        set_err("sample parameters of curve %d must rise strictly inside [0, %d]", c, Sg);
+        return CN_BAD_INPUT;
+      }
+    }
+  std::vector<int> closed(C, 0), kind(C, 0), seg_off(C + 1, 0);
+  for (int c = 0; c < C; ++c) closed[c] = net->closed ? (net->closed[c] != 0) : 0;
+  std::vector<int> used(2 * (size_t)C, 0);
+  if (nn > 0) {
+    if (net->node_ptr[0] != 0) {
+      set_err("node_ptr[0] must be 0");
+      return CN_BAD_INPUT;
+    }
+    for (int j = 0; j < nn; ++j) {
+      const int deg = net->node_ptr[j + 1] - net->node_ptr[j];
+      if (deg < 2 || deg > cn::kCnetMaxNodeDegree) {
+        set_err("intersection %d has %d curve ends (2..%d)", j, deg, cn::kCnetMaxNodeDegree);
+        return CN_BAD_INPUT;
+      }
+      for (int q = net->node_ptr[j]; q < net->node_ptr[j + 1]; ++q) {
+        const int e = net->node_ends[q];
+        if (e < 0 || e >= 2 * C || closed[e >> 1] || used[e]) {
+          set_err("intersection %d: curve end %d is out of range, on a closed curve or used twice", j, e);
+          return CN_BAD_INPUT;
+        }
+        used[e] = 1;
+        kind[e >> 1] |= (e & 1) ? 2 : 1;
+      }
+    }
+  }
+  for (int c = 0; c < C; ++c) seg_off[c + 1] = seg_off[c] + (closed[c] ? M : M - 1);
+  const MeshHost& H = S->H;
+  for (int h = 0; h < H.nh; ++h) {
+    const int c = net->handle_curve[h];
+    if (c < -1 || c >= C || (c >= 0 && (net->handle_sample[h] < 0 || net->handle_sample[h] >= M)) ||
+        (c >= 0 && net->handle_side[h] != 0 && net->handle_side[h] != 1)) {
+      set_err("handle %d: curve, sample or side out of range", h);
+      return CN_BAD_INPUT;
+    }
+  }
+  CN_CUDA(cudaSetDevice(S->device));
+  CN_CUDA(cudaStreamSynchronize(S->stream));
+  for (void* p : S->cnet_mem) cudaFree(p);
+  S->cnet_mem.clear();
+  cn::CurvenetArgs& a = S->cnet;
+  // the per-pose scratch is sized for the new binding on the next call
+  for (void* p : {(void*)a.seg, (void*)a.ends, (void*)S->d_cnet_posed, (void*)S->d_cnet_F, (void*)S->d_cnet_X})
+    if (p) cudaFree(p);
+  S->d_cnet_posed = S->d_cnet_F = S->d_cnet_X = nullptr;
+  S->cnet_pose_cap = 0;
+  S->have_cnet = false;
+  a = cn::CurvenetArgs{};
+  a.n_curves = C; a.n_segments = Sg; a.n_samples = M; a.n_nodes = nn; a.total_segs = seg_off[C]; a.nh = H.nh;
+  cn_status st;
+  std::vector<int> zero1(1, 0);
+  if ((st = cnet_upload_d(S, &a.rest_cp, net->rest_cp, (size_t)C * np * 3)) != CN_OK ||
+      (st = cnet_upload_d(S, &a.sample_tau, net->sample_tau, (size_t)C * M)) != CN_OK ||
+      (st = cnet_upload_i(S, &a.seg_off, seg_off.data(), seg_off.size())) != CN_OK ||
+      (st = cnet_upload_i(S, &a.curve_kind, kind.data(), kind.size())) != CN_OK ||
+      (st = cnet_upload_i(S, &a.node_ptr, nn > 0 ? net->node_ptr : zero1.data(), nn > 0 ? (size_t)nn + 1 : 1)) !=
+          CN_OK ||
+      (st = cnet_upload_i(S, &a.node_ends, net->node_ends, nn > 0 ? (size_t)net->node_ptr[nn] : 0)) != CN_OK ||
+      (st = cnet_upload_i(S, &a.h_curve, net->handle_curve, (size_t)H.nh)) != CN_OK ||
+      (st = cnet_upload_i(S, &a.h_sample, net->handle_sample, (size_t)H.nh)) != CN_OK ||
+      (st = cnet_upload_i(S, &a.h_side, net->handle_side, (size_t)H.nh)) != CN_OK)
+    return st;
+  a.handles = S->D.handles;
+  a.pos = S->D.pos;
+  S->have_cnet = true;
+  return CN_OK;
+}
+
+static cn_status cnet_scratch(cn_system* S, int n_poses) {
+  if (n_poses <= S->cnet_pose_cap) return CN_OK;
+  cn::CurvenetArgs& a = S->cnet;
+  for (void* p : {(void*)a.seg, (void*)a.ends, (void*)S->d_cnet_posed, (void*)S->d_cnet_F, (void*)S->d_cnet_X})
+    if (p) cudaFree(p);
+  a.seg = a.ends = S->d_cnet_posed = S->d_cnet_F = S->d_cnet_X = nullptr;
+  S->cnet_pose_cap = 0;
+  const size_t np = 3 * (size_t)a.n_segments + 1;
+  CN_CUDA(cudaMalloc((void**)&a.seg, sizeof(double) * 8 * std::max<size_t>((size_t)n_poses * a.total_segs, 1)));
+  CN_CUDA(cudaMalloc((void**)&a.ends, sizeof(double) * 32 * (size_t)n_poses * a.n_curves));
+  CN_CUDA(cudaMalloc((void**)&S->d_cnet_posed, sizeof(double) * (size_t)n_poses * a.n_curves * np * 3));
+  CN_CUDA(cudaMalloc((void**)&S->d_cnet_F, sizeof(double) * 9 * std::max<size_t>((size_t)n_poses * a.nh, 1)));
+  CN_CUDA(cudaMalloc((void**)&S->d_cnet_X, sizeof(double) * 3 * std::max<size_t>((size_t)n_poses * a.nh, 1)));
+  // the intersection records of curve ends without a node stay zero
+  CN_CUDA(cudaMemset(a.ends, 0, sizeof(double) * 32 * (size_t)n_poses * a.n_curves));
+  S->cnet_pose_cap = n_poses;
+  return CN_OK;
+}
+
+cn_status cn_curvenet_constraints_device(cn_handle S, int32_t n_poses, const double* d_posed_cp, double* d_Fc,
+                                         double* d_Xc) {
+  if (!S || !d_posed_cp || !d_Fc || !d_Xc || n_poses < 1) {
+    set_err("null argument or n_poses < 1");
+    return CN_BAD_INPUT;
+  }
+  if (!S->have_cnet) {
+    set_err("no curvenet bound (cn_bind_curvenet)");
+    return CN_BAD_INPUT;
+  }
+  CN_CUDA(cudaSetDevice(S->device));
+  cn_status st = cnet_scratch(S, n_poses);
+  if (st != CN_OK) return st;
+  CN_CUDA(cn::launch_curvenet_constraints(S->cnet, n_poses, d_posed_cp, d_Fc, d_Xc, S->stream));
+  return CN_OK;
+}
+
+cn_status cn_curvenet_constraints(cn_handle S, int32_t n_poses, const double* posed_cp, double* Fc, double* Xc) {
+  if (!S || !posed_cp || !Fc || !Xc || n_poses < 1) {
+    set_err("null argument or n_poses < 1");
+    return CN_BAD_INPUT;
+  }
+  if (!S->have_cnet) {
+    set_err("no curvenet bound (cn_bind_curvenet)");
+    return CN_BAD_INPUT;
+  }
+  const cn::CurvenetArgs& a = S->cnet;
+  const size_t ncp = (size_t)n_poses * a.n_curves * (3 * (size_t)a.n_segments + 1) * 3;
+  for (size_t i = 0; i < ncp; ++i)
+    if (!std::isfinite(posed_cp[i])) {
+      set_err("posed control point %zu is not finite", i);
+      return CN_NAN;
+    }
+  CN_CUDA(cudaSetDevice(S->device));
+  cn_status st = cnet_scratch(S, n_poses);
+  if (st != CN_OK) return st;
+  CN_CUDA(cudaMemcpyAsync(S->d_cnet_posed, posed_cp, sizeof(double) * ncp, cudaMemcpyHostToDevice, S->stream));
+  CN_CUDA(cn::launch_curvenet_constraints(S->cnet, n_poses, S->d_cnet_posed, S->d_cnet_F, S->d_cnet_X, S->stream));
+  CN_CUDA(cudaMemcpyAsync(Fc, S->d_cnet_F, sizeof(double) * 9 * (size_t)n_poses * a.nh, cudaMemcpyDeviceToHost,
+                          S->stream));
+  CN_CUDA(cudaMemcpyAsync(Xc, S->d_cnet_X, sizeof(double) * 3 * (size_t)n_poses * a.nh, cudaMemcpyDeviceToHost,
+                          S->stream));
+  CN_CUDA(cudaStreamSynchronize(S->stream));
+  return CN_OK;
+}
+
+cn_status cn_deform_curvenet(cn_handle S, const double* posed_cp, double* x_out, const cn_solve_opts* opts,
+                             cn_solve_stats* stats) {
+  if (!S || !posed_cp || !x_out) {
+    set_err("null argument");
+    return CN_BAD_INPUT;
+  }
+  if (!S->have_cnet) {
+    set_err("no curvenet bound (cn_bind_curvenet)");
+    return CN_BAD_INPUT;
+  }
+  if (S->kmax < 9) {
+    set_err("the two-stage solve needs a build with max_rhs = 9");
+    return CN_BAD_INPUT;
+  }
+  const MeshHost& H = S->H;
+  const cn::CurvenetArgs& a = S->cnet;
+  const size_t ncp = (size_t)a.n_curves * (3 * (size_t)a.n_segments + 1) * 3;
+  for (size_t i = 0; i < ncp; ++i)
+    if (!std::isfinite(posed_cp[i])) {
+      set_err("posed control point %zu is not finite", i);
+      return CN_NAN;
+    }
+  CN_CUDA(cudaSetDevice(S->device));
+  cn_status st = ensure_deform_tables(S);
+  if (st != CN_OK) return st;
+  if ((st = cnet_scratch(S, 1)) != CN_OK) return st;
+  cn_solve_opts o;
+  if (opts) o = *opts;
+  else cn_default_solve_opts(&o);
+  CN_CUDA(cudaMemcpyAsync(S->d_cnet_posed, posed_cp, sizeof(double) * ncp, cudaMemcpyHostToDevice, S->stream));
+  // F_c straight into the Stage-1 targets, X_c into the bridge's table
+  CN_CUDA(cn::launch_curvenet_constraints(S->cnet, 1, S->d_cnet_posed, S->d_targets, S->d_Xc, S->stream));
+  st = deform_stages(S, o, stats);
+  if (st != CN_OK && st != CN_MAX_ITER) return st;
+  CN_CUDA(cn::launch_curvenet_overlay(H.nh, S->D.handles, S->d_Xc, S->d_xout, S->stream));
+  CN_CUDA(cudaMemcpyAsync(x_out, S->d_xout, sizeof(double) * 3 * (size_t)H.nv, cudaMemcpyDeviceToHost, S->stream));
+  CN_CUDA(cudaStreamSynchronize(S->stream));
   return st;
 }
 

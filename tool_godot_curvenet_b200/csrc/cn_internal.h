@@ -246,6 +246,32 @@ struct DeformArgs {
 };
 cudaError_t launch_deform_bridge(const DeformArgs& d, cudaStream_t s);
 
+// Profile curves on the GPU (cn_curvenet.cu): samples, segment tangents and
+// lengths, intersection frames, per-handle F_c and X_c for many poses.
+constexpr int kCnetMaxNodeDegree = 16;
+struct CurvenetArgs {
+  int n_curves, n_segments, n_samples;
+  const double* rest_cp;     // n_curves x (3 n_segments + 1) x 3
+  const double* sample_tau;  // n_curves x n_samples
+  const int* seg_off;        // n_curves + 1: first polyline segment of each curve
+  int total_segs;
+  const int* curve_kind;     // 0 isolated, bit 0: start at a node, bit 1: end at a node
+  int n_nodes;
+  const int* node_ptr;       // n_nodes + 1
+  const int* node_ends;      // 2 curve + end, counter-clockwise per node
+  int nh;
+  const int* h_curve;        // per handle: curve (-1: rest, F = I)
+  const int* h_sample;
+  const int* h_side;         // 0 plus, 1 minus
+  const int* handles;        // handle -> vertex
+  const double* pos;         // rest positions, n_verts x 3
+  double* seg;               // scratch: poses x total_segs x 8
+  double* ends;              // scratch: poses x n_curves x 2 x 16
+};
+cudaError_t launch_curvenet_constraints(const CurvenetArgs& a, int n_poses, const double* posed_cp, double* Fc,
+                                        double* Xc, cudaStream_t s);
+cudaError_t launch_curvenet_overlay(int nh, const int* handles, const double* Xc, double* x, cudaStream_t s);
+
 // Plain FP64 Jacobi-PCG with one kernel per primitive and the scalars folded
 // on the host each iteration (the reference's GPU orchestration).
 struct PlainArgs {

@@ -219,6 +219,53 @@ class CutMeshSolver:
             raise CnError(st, "cn_solve_deformation")
         return SolveResult(x, stats)
 
+    # -- profile curvenet (DeGoes22 section 3 on the GPU)
+    def bind_curvenet(self, rest_cp, sample_tau, handle_curve, handle_sample, handle_side, closed=None,
+                      node_ptr=None, node_ends=None):
+        """Bind curves to the handles (cn_bind_curvenet).  rest_cp:
+        (n_curves, 3S+1, 3); sample_tau: (n_curves, n_samples); per handle its
+        curve (-1: none), sample and side (0 plus, 1 minus); closed: per curve;
+        node_ptr / node_ends: intersections as lists of curve ends (2 c + end)
+        in counter-clockwise order."""
+        rest_cp = _f64(rest_cp)
+        C_, npts, _ = rest_cp.shape
+        tau = _f64(sample_tau)
+        self._cnet_keep = [rest_cp, tau, _i32(handle_curve), _i32(handle_sample), _i32(handle_side),
+                           _i32(closed if closed is not None else np.zeros(C_)),
+                           _i32(node_ptr if node_ptr is not None else [0]),
+                           _i32(node_ends if node_ends is not None and len(node_ends) else [0])]
+        rc, tu, hc, hs, hd, cl, npt, ne = self._cnet_keep
+        d = L.CurvenetDesc(C_, (npts - 1) // 3, tau.shape[1], _dp(rc), _dp(tu), _ip(cl), npt.size - 1, _ip(npt),
+                           _ip(ne), _ip(hc), _ip(hs), _ip(hd))
+        st = L.lib().cn_bind_curvenet(self._h, C.byref(d))
+        if st != L.CN_OK:
+            raise CnError(st, "cn_bind_curvenet")
+        self._cnet_shape = (C_, npts)
+
+    def curvenet_constraints(self, posed_cp):
+        """F_c (poses, n_handles, 3, 3) and X_c (poses, n_handles, 3) from
+        posed control points (poses, n_curves, 3S+1, 3), on the GPU."""
+        P = _f64(posed_cp).reshape(-1, *self._cnet_shape, 3)
+        nh = self.handles.size
+        F = np.empty((P.shape[0], nh, 9))
+        X = np.empty((P.shape[0], nh, 3))
+        st = L.lib().cn_curvenet_constraints(self._h, P.shape[0], _dp(P), _dp(F), _dp(X))
+        if st != L.CN_OK:
+            raise CnError(st, "cn_curvenet_constraints")
+        return F.reshape(P.shape[0], nh, 3, 3), X
+
+    def deform_curvenet(self, posed_cp, **kw):
+        """Curves to deformed positions in one call (F_c, X_c on the GPU, then
+        the two-stage solve of DeformSolve.lean:110-135).  Needs max_rhs=9."""
+        P = _f64(posed_cp)
+        x = np.empty((self.n_verts, 3))
+        o = self.make_opts(**kw)
+        stats = L.SolveStats()
+        st = L.lib().cn_deform_curvenet(self._h, _dp(P), _dp(x), C.byref(o), C.byref(stats))
+        if st != L.CN_OK:
+            raise CnError(st, "cn_deform_curvenet")
+        return SolveResult(x, stats)
+
     def ddm_bind(self, nu=2, omega=0.5, top_k=4, **kw):
         """Direct Delta Mush influences (DirectDeltaMushBind.lean:6-40):
         (idx, w), each (n_verts, min(top_k, n_handles)); row v's entries are
