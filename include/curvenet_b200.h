@@ -74,8 +74,12 @@ enum { CN_MODE_HARMONIC = 0, CN_MODE_DEFORM = 1, CN_MODE_RHS = 2 };
  * drift on ill-conditioned meshes).  With IC(0) / HSC: the level-scheduled
  * kernel.  CLASSIC: the two-reduction CG (row-cached kernel with Jacobi).
  * PIPELINED: the pipelined CG without fall-back, both precisions (Jacobi
- * only).  PLAIN: one kernel per primitive, FP64 Jacobi. */
-enum { CN_ALGO_FUSED = 0, CN_ALGO_PLAIN = 1, CN_ALGO_CLASSIC = 2, CN_ALGO_PIPELINED = 3 };
+ * only).  PLAIN: one kernel per primitive, FP64 Jacobi.  SINGLE: the
+ * single-reduction CG (Chronopoulos & Gear: alpha and beta from one
+ * reduction of (r, z), (z, A z), ||r||^2) on the row-cached kernel, Jacobi
+ * or block SSOR: one grid barrier per iteration, z exchanged with the
+ * neighbour blocks only. */
+enum { CN_ALGO_FUSED = 0, CN_ALGO_PLAIN = 1, CN_ALGO_CLASSIC = 2, CN_ALGO_PIPELINED = 3, CN_ALGO_SINGLE = 4 };
 
 typedef struct {
   int32_t precond;       /* CN_PRECOND_* (default IC0) */

@@ -191,3 +191,19 @@ def test_c5_solvers_match_oracle():
                 r = s.solve(t, mode="deform", precision="fp64", tol=1e-13, max_iter=40000)
                 _check(r, 1e-13)
                 assert rel_err(r.x, xo) <= FP64_TOL
+
+
+@pytest.mark.parametrize("precond", ["bssor", "jacobi"])
+def test_c2_single_reduction_form_matches_oracle(precond):
+    pos, tris, h, t = workload("c2")
+    xo = oracle_solution("c2")
+    with CutMeshSolver(pos, tris, h, precond=precond) as s:
+        r = s.solve(t, mode="deform", precision="mixed", algo="single", tol=1e-8)
+        _check(r, 1e-8)
+        assert rel_err(r.x, xo) <= STOP_TOL
+        r = s.solve(t, mode="deform", precision="mixed", algo="single", tol=1e-11, max_refine=30)
+        _check(r, 1e-11)
+        assert rel_err(r.x, xo) <= TIGHT_TOL
+        r = s.solve(t, mode="deform", precision="fp64", algo="single", tol=1e-13, max_iter=20000)
+        _check(r, 1e-13)
+        assert rel_err(r.x, xo) <= FP64_TOL

@@ -369,3 +369,37 @@ def test_block_ssor_rejects_pipelined_form():
         with pytest.raises(CnError) as e:
             s.solve(t[:, :3], mode="deform", algo="pipelined")
         assert e.value.status == L.CN_BAD_INPUT
+
+
+@pytest.mark.parametrize("name", ["cyl_tiny", "c1", "torus_small", "torus_mid", "c3_0"])
+@pytest.mark.parametrize("precond", ["bssor", "jacobi"])
+@pytest.mark.parametrize("k", [1, 3, 9])
+def test_single_reduction_form_matches_oracle(name, precond, k, oracle):
+    """The single-reduction CG (one grid barrier per iteration, z exchanged
+    with the neighbour blocks by release / acquire flags) on the row-cached
+    kernel: FP64 and mixed precision against the oracle, default launch and
+    a one-block launch."""
+    pos, tris, h, _ = workload(name)
+    rng = np.random.default_rng(11 + k)
+    t = rng.normal(size=(h.size, k))
+    ref = oracle.System(pos, tris, h)
+    st, xo, _, _ = ref.solve(t, mode=0, tol=1e-13)
+    assert st == 0
+    for kw in ({}, {"grid": 1, "block": 512}):
+        with CutMeshSolver(pos, tris, h, max_rhs=k, precond=precond, **kw) as s:
+            r = s.solve(t, mode="harmonic", precision="fp64", tol=1e-13, max_iter=20000, algo="single")
+            rm = s.solve(t, mode="harmonic", precision="mixed", tol=1e-8, max_iter=20000, algo="single")
+            rc = s.solve(t, mode="harmonic", precision="mixed", tol=1e-8, max_iter=20000, algo="classic")
+        assert r.status == 0 and rm.status == 0
+        assert np.all(r.rel_residual <= 1e-13) and np.all(rm.rel_residual <= 1e-8)
+        assert rel_err(r.x, xo) <= FP64_TOL
+        assert rel_err(rm.x, xo) <= MIXED_TOL
+        # the same iteration count as the two-reduction form, within rounding drift
+        assert abs(rm.iterations - rc.iterations) <= max(8, 0.1 * rc.iterations)
+
+
+def test_single_reduction_rejected_on_level_scheduled_handles():
+    pos, tris, h, t = workload("c1")
+    with CutMeshSolver(pos, tris, h, precond="ic0") as s:
+        with pytest.raises(CnError):
+            s.solve(t, mode="deform", precision="mixed", algo="single")

@@ -16,7 +16,7 @@ ORDER_NATURAL, ORDER_COLOR, ORDER_AUTO = 0, 1, 2
 LAPLACIAN_COT, LAPLACIAN_ROBUST = 0, 1
 PREC_FP64, PREC_MIXED = 0, 1
 MODE_HARMONIC, MODE_DEFORM, MODE_RHS = 0, 1, 2
-ALGO_FUSED, ALGO_PLAIN, ALGO_CLASSIC, ALGO_PIPELINED = 0, 1, 2, 3
+ALGO_FUSED, ALGO_PLAIN, ALGO_CLASSIC, ALGO_PIPELINED, ALGO_SINGLE = 0, 1, 2, 3, 4
 
 
 class MeshDesc(C.Structure):

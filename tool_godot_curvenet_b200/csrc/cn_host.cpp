@@ -62,6 +62,7 @@ struct cn_system {
   long long bss_lent_cap = 0;
   int bss_loff_cap = 0, bss_rb = -1, bss_grid = -1;
   int* d_status = nullptr;
+  unsigned* d_nbflag = nullptr;  // single-reduction form: per-block publication counts (inside buf)
   // pipelined solve: shared-memory needs of the last (grid, block, precision, k)
   int pipe_grid = -1, pipe_block = -1, pipe_prec = -1, pipe_k = -1;
   size_t pipe_cache = 0, pipe_full = 0;
@@ -129,6 +130,7 @@ void layout_all(cn::Bump& b, cn_system* S) {
   S->d_targets = b.take<double>((size_t)std::max(S->H.nh, S->H.n) * S->kmax + 1);
   S->d_xout = b.take<double>((size_t)S->H.nv * S->kmax + 1);
   S->d_status = b.take<int>(1);
+  S->d_nbflag = b.take<unsigned>((size_t)S->max_grid_alloc);
 }
 
 void choose_launch(cn_system* S) {
@@ -520,7 +522,7 @@ cn_status cn_solve_device(cn_handle S, int32_t k, const double* d_targets, doubl
     return worst;
   }
   if (!(o.tol > 0.0) || o.max_iter < 0 || o.max_refine < 1 || o.algo < CN_ALGO_FUSED ||
-      o.algo > CN_ALGO_PIPELINED) {
+      o.algo > CN_ALGO_SINGLE) {
     set_err("bad solve options");
     return CN_BAD_INPUT;
   }
@@ -562,6 +564,10 @@ cn_status cn_solve_device(cn_handle S, int32_t k, const double* d_targets, doubl
     set_err("the pipelined form needs the Jacobi preconditioner");
     return CN_BAD_INPUT;
   }
+  if (o.algo == CN_ALGO_SINGLE && !row_cached(S)) {
+    set_err("the single-reduction form runs on Jacobi and block SSOR handles");
+    return CN_BAD_INPUT;
+  }
   if (row_cached(S)) {
     // FP64: pipelined, falling back to the two-reduction form if an inner
     // solve stalls; mixed: the two-reduction form (the FP32 pipelined
@@ -570,6 +576,8 @@ cn_status cn_solve_device(cn_handle S, int32_t k, const double* d_targets, doubl
                 : o.precision == CN_PREC_FP64 ? 2 : 0;
     const bool bssor = S->opts.precond == CN_PRECOND_BSSOR;
     if (bssor) a.pipe_mode = 0;  // the pipelined recurrences assume a diagonal M
+    if (o.algo == CN_ALGO_SINGLE) a.pipe_mode = 3;
+    a.nbflag = S->d_nbflag;
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, S->device);
     // the grid: every SM, or fewer blocks of at least 256 rows for a small mesh
@@ -662,6 +670,8 @@ cn_status cn_solve_device(cn_handle S, int32_t k, const double* d_targets, doubl
       a.bss_loff = S->d_bss_loff;
     }
     CN_CUDA(cudaMemsetAsync(S->d_ctl, 0, sizeof(Control), S->stream));
+    if (a.pipe_mode == 3)
+      CN_CUDA(cudaMemsetAsync(S->d_nbflag, 0, sizeof(unsigned) * (size_t)std::max(grid, 1), S->stream));
     CN_CUDA(cudaEventRecord(S->ev0, S->stream));
     CN_CUDA(cn::launch_pipelined_solve(a, o.precision, k, block, grid, qr, S->stream));
     CN_CUDA(cudaEventRecord(S->ev1, S->stream));

@@ -76,7 +76,8 @@ struct SolveArgs {
   void* m0;   // T
   void* m1;   // T
   void* m2;   // T (the classic form's first records [z | p])
-  int pipe_mode;
+  int pipe_mode;           // 0 two-reduction, 1 pipelined, 2 pipelined with fall-back, 3 single-reduction
+  unsigned* nbflag;        // single-reduction form: one z-publication count per block (zeroed per launch)
   double* pown;            // FP64 own-row state when it is not in shared memory: 7 x [rows][K]
   const double* dinv64;    // 1 / sqrt(A_ii), FP64
   int cache_bytes;         // dynamic shared memory (row cache, then own-row state)

@@ -34,6 +34,15 @@
 // r, applies z = M^-1 r (inline for Jacobi, by the block's colour sweeps in
 // shared memory for block SSOR), (r, z) and ||r||^2.
 //
+// Single-reduction form (Jacobi or block SSOR; Chronopoulos & Gear, "s-step
+// iterative methods for symmetric linear systems", J. Comput. Appl. Math. 25,
+// 1989): one reduction of gamma = (r, z), delta = (z, A z) and ||r||^2 per
+// iteration and ONE grid barrier; alpha = gamma / (delta - beta gamma /
+// alpha'), beta = gamma / gamma', A p by s = A z + beta s'.  The exchange of
+// z between the reduction's barriers is point to point: a block publishes
+// its z with a release flag (an epoch count) and waits, with acquire loads,
+// only for the flags of the blocks its rows couple to.
+//
 // Partial sums alternate between two slot groups by phase parity (a block
 // may write phase i+1's partials while a slower block still reads phase i's);
 // the gathered vectors alternate between two buffers for the same reason.
@@ -57,6 +66,8 @@ struct MRow {
 };
 
 constexpr int kPipeSplits = 8;  // partial-sum read: up to 8 x 128 blocks
+constexpr int kNbrWords = 64;        // single-reduction form: neighbour-block bitmap (up to 2048 blocks)
+constexpr int kMaxNbrBlocks = 64;    // neighbour blocks a block waits for one by one
 constexpr int kMaxColours = 64;   // block SSOR: colours of a block (greedy: at most the row length)
 constexpr int kSweepRows = 4;     // block SSOR, tables in global memory: rows a thread sweeps at a time
 // The pipelined recurrences in FP32 lose track of the true residual below
@@ -67,8 +78,15 @@ constexpr double kPipeInnerFloor = 1e-3;
 template <int K>
 struct PipeSmem {
   Smem<K> sm;
-  double red2[kMaxWarps * 2 * K];
-  double psum[2 * K][kPipeSplits];
+  double red2[kMaxWarps * 3 * K];
+  double psum[3 * K][kPipeSplits];
+  // single-reduction form: the other blocks whose rows this block's rows
+  // couple to (bitmap over blocks, then the list; nbn < 0: more than
+  // kMaxNbrBlocks, the z exchange then waits at a grid barrier)
+  unsigned nbm[kNbrWords];
+  int nbl[kMaxNbrBlocks];
+  int nbn;
+  int nbok;
   double tau2[K], stop[K], gprev[K], aprev[K], alpha[K], beta[K], rrprev[K];
   int use_pipe;
   int act[K];
@@ -652,6 +670,39 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
     ownq[q] = own_ref(q, okq[q] ? row : 0);
   }
 
+  // ---- single-reduction form: the blocks that own the columns of this
+  // block's rows (their z is what this block gathers)
+  if (a.pipe_mode == 3) {
+    for (int i = t; i < kNbrWords; i += B) s->nbm[i] = 0u;
+    __syncthreads();
+    const long long rows_per = (long long)Qg * B;
+    for (int q = 0; q < Qb; ++q) {
+      const int row = row0 + q * R;
+      if (row >= n) break;
+      const RowRef<T> rr = row_ref(q, row);
+      for (int e = 0; e < rr.len; ++e) {
+        const int j = rr.c[e * rr.stride];
+        if (j < 0) continue;
+        const int ob = (int)(j / rows_per);
+        if (ob != team.rank() && ob < kNbrWords * 32) atomicOr(&s->nbm[ob >> 5], 1u << (ob & 31));
+      }
+    }
+    __syncthreads();
+    if (t == 0) {
+      int cnt = 0;
+      for (int w = 0; w < kNbrWords; ++w)
+        for (unsigned m = s->nbm[w]; m; m &= m - 1) {
+          if (cnt < kMaxNbrBlocks) s->nbl[cnt] = 32 * w + __ffs(m) - 1;
+          ++cnt;
+        }
+      // more neighbours than the list holds (or blocks than the bitmap
+      // covers): wait for every other block's flag
+      s->nbn = (cnt > kMaxNbrBlocks || tsize > kNbrWords * 32) ? -1 : cnt;
+    }
+    __syncthreads();
+  }
+  unsigned epoch = 0;  // z publications of this launch (the host zeroes the flags)
+
   // ---- phase A: right-hand side (HarmonicSolve.lean:51-66 / DeformSolve.lean:123-135)
   {
     double bb[K];
@@ -936,6 +987,216 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
         pipe_update<T, K>(own_ref(q, row), row, nn, alpha, beta, b0, mnext, d2);
       }
       block_reduce_strided<2 * K, T>(d2, s->red2, pipe_ptr(g ^ 1) + team.rank(), tsize);
+      ++total_iters;
+      if (!team.sync()) { status = CN_TIMEOUT; goto done; }
+    }
+    } else if (a.pipe_mode == 3) {
+    // ---- the single-reduction CG, one grid barrier per iteration:
+    //   gamma, delta, ||r||^2 of the last phase -> stop?, beta, alpha;
+    //   p = z + beta p'; s = w + beta s'; x += alpha p; r -= alpha s;
+    //   z = M^-1 r (inline for Jacobi, the colour sweeps for block SSOR),
+    //   (r, z), ||r||^2; publish z; wait for the neighbour blocks' z;
+    //   w = A z, (z, w); this block's partial sums; grid barrier.
+    // Partial tables [3K][blocks] (gamma, ||r||^2, delta) alternate by
+    // parity at slots 2 and 5.
+    double* const tR[2] = {part + (size_t)2 * tsize * K, part + (size_t)5 * tsize * K};
+    const int ns = (tsize + 127) >> 7, items = 3 * K * ns;
+    T* const zb[2] = {mb2, mb1};
+    // prologue: w = A z for the z = M^-1 r of phase R (mb2, visible since its barrier)
+    {
+      T d3[3 * K];
+#pragma unroll
+      for (int c = 0; c < 3 * K; ++c) d3[c] = (T)0;
+      for (int q = 0; q < Qb; ++q) {
+        const int row = row0 + q * R;
+        if (row >= n) break;
+        RowRef<T> r1[1] = {row_ref(q, row)};
+        const bool ok1[1] = {true};
+        T acc1[1][K];
+        gather_rows<T, K, UP, 1>(r1, ok1, mb2, acc1);
+        const OwnRef<T, K> o = own_ref(q, row);
+#pragma unroll
+        for (int c = 0; c < K; ++c) {
+          const T r = o(kQr, c), z = o(kQz, c), w = acc1[0][c];
+          o(kQw, c) = w;
+          d3[c] += r * z;
+          d3[K + c] += r * r;
+          d3[2 * K + c] += z * w;
+        }
+      }
+      block_reduce_strided<3 * K, T>(d3, s->red2, tR[0] + team.rank(), tsize);
+      if (!team.sync()) { status = CN_TIMEOUT; goto done; }
+    }
+    for (int it = 0;; ++it) {
+      const int g = it & 1;
+      T* const zn = zb[g ^ 1];
+      for (int item = warp; item < items; item += nw) {
+        const int fc = item / ns, sp = item - fc * ns;
+        double v[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const int b = sp * 128 + i * 32 + lane;
+          v[i] = b < tsize ? __ldcg(tR[g] + (size_t)fc * tsize + b) : 0.0;
+        }
+        double x = (v[0] + v[1]) + (v[2] + v[3]);
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) x += __shfl_xor_sync(0xffffffffu, x, off);
+        if (lane == 0) s->psum[fc][sp] = x;
+      }
+      __syncthreads();
+      if (warp == 0) {
+        int act = 0, bad = 0;
+        if (lane < K) {
+          const int c = lane;
+          act = s->act[c];
+          double ga = 0.0, rr = 0.0, de = 0.0;
+          for (int sp = 0; sp < ns; ++sp) {
+            ga += s->psum[c][sp];
+            rr += s->psum[K + c][sp];
+            de += s->psum[2 * K + c][sp];
+          }
+          if (!(ga == ga) || !(rr == rr) || !(de == de)) bad = 1;
+          if (act && rr < s->stop[c]) act = 0;
+          double be = 0.0, al = 0.0;
+          if (act) {
+            be = (it == 0 || s->gprev[c] == 0.0) ? 0.0 : ga / s->gprev[c];
+            // (p, A p) = delta - beta gamma / alpha'; SparseLinAlg.lean:118
+            // stops on pAp == 0: a non-positive value ends this column's
+            // inner solve (the next FP64 residual decides)
+            const double den = it == 0 ? de : de - be * ga / s->aprev[c];
+            if (den > 0.0) al = ga / den;
+            else act = 0;
+          }
+          s->beta[c] = act ? be : 0.0;
+          s->alpha[c] = act ? al : 0.0;
+          if (act) {
+            s->gprev[c] = ga;
+            s->aprev[c] = al;
+          }
+          s->act[c] = act;
+        }
+        const int any = __any_sync(0xffffffffu, act), anybad = __any_sync(0xffffffffu, bad);
+        if (lane == 0) s->flag = anybad ? 2 : (any ? 1 : 0);
+      }
+      __syncthreads();
+      if (s->flag == 2) { status = CN_NAN; goto done; }
+      if (s->flag == 0 || it >= a.max_iter) break;
+      {
+        T alpha[K], beta[K];
+#pragma unroll
+        for (int c = 0; c < K; ++c) {
+          alpha[c] = (T)s->alpha[c];
+          beta[c] = (T)s->beta[c];
+        }
+        T d3[3 * K];
+#pragma unroll
+        for (int c = 0; c < 3 * K; ++c) d3[c] = (T)0;
+        for (int q = 0; q < Qb; ++q) {
+          const int row = row0 + q * R;
+          if (row >= n) break;
+          const OwnRef<T, K> o = own_ref(q, row);
+          const T mi = o(kQminv, 0);
+          T rec[K];
+#pragma unroll
+          for (int c = 0; c < K; ++c) {
+            const T p = o(kQz, c) + beta[c] * o(kQp, c);
+            const T sv_ = o(kQw, c) + beta[c] * o(kQs, c);  // A p
+            o(kQp, c) = p;
+            o(kQs, c) = sv_;
+            o(kQx, c) += alpha[c] * p;
+            const T r = o(kQr, c) - alpha[c] * sv_;
+            o(kQr, c) = r;
+            if (!bssor) {
+              const T z = mi * r;
+              o(kQz, c) = z;
+              rec[c] = z;
+              d3[c] += r * z;
+              d3[K + c] += r * r;
+            } else {
+              rec[c] = mi * r;  // block SSOR: the sweeps start from M^-1 r
+            }
+          }
+          if (!bssor) store_m<T, K>(zn, row, rec);
+          else sv_store(q * B + t, rec);
+        }
+        if (bssor && sm_ssor && s->ncb >= 2) {  // the sweeps also write the records, zn and the dots
+          __syncthreads();
+          ssor_fast_fin(true, zn, d3);
+        } else if (bssor) {
+          __syncthreads();
+          ssor_apply();
+          for (int q = 0; q < Qb; ++q) {
+            const int row = row0 + q * R;
+            if (row >= n) break;
+            const OwnRef<T, K> o = own_ref(q, row);
+            T zf[K];
+            sv_load(q * B + t, zf);
+#pragma unroll
+            for (int c = 0; c < K; ++c) {
+              const T r = o(kQr, c);
+              o(kQz, c) = zf[c];
+              d3[c] += r * zf[c];
+              d3[K + c] += r * r;
+            }
+            store_m<T, K>(zn, row, zf);
+          }
+        }
+        // publish z, then wait (bounded) for the z of the neighbour blocks
+        __syncthreads();
+        ++epoch;
+        if (t == 0) {
+          __threadfence();
+          asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(a.nbflag + team.rank()), "r"(epoch) : "memory");
+        }
+        if (warp == 0) {
+          const int nb = s->nbn < 0 ? tsize : s->nbn;
+          int ok = 1;
+          for (int i = lane; i < nb && ok; i += 32) {
+            const int ob = s->nbn < 0 ? i : s->nbl[i];
+            if (ob == team.rank()) continue;
+            const unsigned* f = a.nbflag + ob;
+            if (ld_acquire_u32(f) < epoch) {
+              const unsigned long long t0 = global_ns();
+              unsigned spins = 0;
+              while (ld_acquire_u32(f) < epoch) {
+                if ((long long)(global_ns() - t0) > a.timeout_ns) {
+                  atomicExch(&a.ctl->abort, 1);
+                  ok = 0;
+                  break;
+                }
+                if ((++spins & 63u) == 0 && *(volatile int*)&a.ctl->abort) { ok = 0; break; }
+              }
+            }
+          }
+          ok = __all_sync(0xffffffffu, ok);
+          if (lane == 0) s->nbok = ok;
+        }
+        __syncthreads();
+        if (!s->nbok) { status = CN_TIMEOUT; goto done; }
+        // w = A z, (z, w)
+        T accq[QR][K];
+        gather_rows<T, K, UP, QR>(rrq, okq, zn, accq);
+        auto take_w = [&](const OwnRef<T, K>& o, const T (&acc)[K]) {
+#pragma unroll
+          for (int c = 0; c < K; ++c) {
+            o(kQw, c) = acc[c];
+            d3[2 * K + c] += o(kQz, c) * acc[c];
+          }
+        };
+#pragma unroll
+        for (int q = 0; q < QR; ++q)
+          if (okq[q]) take_w(ownq[q], accq[q]);
+        for (int q = QR; q < Qb; ++q) {
+          const int row = row0 + q * R;
+          if (row >= n) break;
+          RowRef<T> r1[1] = {row_ref(q, row)};
+          const bool ok1[1] = {true};
+          T acc1[1][K];
+          gather_rows<T, K, UP, 1>(r1, ok1, zn, acc1);
+          take_w(own_ref(q, row), acc1[0]);
+        }
+        block_reduce_strided<3 * K, T>(d3, s->red2, tR[g ^ 1] + team.rank(), tsize);
+      }
       ++total_iters;
       if (!team.sync()) { status = CN_TIMEOUT; goto done; }
     }

@@ -44,7 +44,7 @@ _LAP = {"cot": L.LAPLACIAN_COT, "robust": L.LAPLACIAN_ROBUST}
 _PREC = {"fp64": L.PREC_FP64, "mixed": L.PREC_MIXED}
 _MODE = {"harmonic": L.MODE_HARMONIC, "deform": L.MODE_DEFORM, "rhs": L.MODE_RHS}
 _ALGO = {"fused": L.ALGO_FUSED, "plain": L.ALGO_PLAIN, "classic": L.ALGO_CLASSIC,
-         "pipelined": L.ALGO_PIPELINED}
+         "pipelined": L.ALGO_PIPELINED, "single": L.ALGO_SINGLE}
 
 
 def cut_mesh(n_verts, tris, loops):
