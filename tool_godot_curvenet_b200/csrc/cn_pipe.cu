@@ -820,7 +820,7 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
         // the pipelined form falls back to the classic one (for the rest of
         // the solve) when its last inner solve cut the FP64 residual of some
         // column by less than 10x
-        if (refine == 0) s->use_pipe = a.pipe_mode != 0;
+        if (refine == 0) s->use_pipe = a.pipe_mode == 1 || a.pipe_mode == 2;
         if (s->use_pipe && a.pipe_mode == 2 && refine > 0)
           for (int c = 0; c < K; ++c)
             if (s->rrprev[c] > 0.0 && !(s->sm.sum[c] <= 1e-2 * s->rrprev[c])) s->use_pipe = 0;
