@@ -1099,8 +1099,9 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
           T rec[K];
 #pragma unroll
           for (int c = 0; c < K; ++c) {
-            const T p = o(kQz, c) + beta[c] * o(kQp, c);
-            const T sv_ = o(kQw, c) + beta[c] * o(kQs, c);  // A p
+            // the first iteration reads no p', s' (the records may hold anything)
+            const T p = it == 0 ? o(kQz, c) : o(kQz, c) + beta[c] * o(kQp, c);
+            const T sv_ = it == 0 ? o(kQw, c) : o(kQw, c) + beta[c] * o(kQs, c);  // A p
             o(kQp, c) = p;
             o(kQs, c) = sv_;
             o(kQx, c) += alpha[c] * p;
