@@ -136,6 +136,39 @@ cn_status cn_cut_mesh(int32_t n_verts, int32_t n_tris, const int32_t* tris, int3
                       const int32_t* loop_ptr, const int32_t* loop_verts, int32_t* tris_out,
                       int32_t* parent_out, int32_t* n_verts_out);
 
+/* ---------------------------------------------------------------------------
+ * Cut-mesh construction on the GPU (current device; host buffers in and
+ * out).  Halfedge records are 4 int32 each: target, twin (-1 none), next,
+ * face (-1 the outer face).
+ *
+ * cn_halfedges: HalfedgeBuilder.fromTriangles (HalfedgeBuilder.lean:34-90):
+ * interior halfedges 3f, 3f+1, 3f+2 run t0->t1, t1->t2, t2->t0; a twin is the
+ * lowest interior index with the reversed (source, target); each interior
+ * halfedge without one gets a boundary halfedge, appended in interior index
+ * order; a boundary halfedge's next is the lowest boundary index whose
+ * source is its target (itself if none).  he_out capacity: 6 n_tris records.
+ * Bit-exact with the specification on any triangle soup. */
+cn_status cn_halfedges(int32_t n_verts, int32_t n_tris, const int32_t* tris, int32_t* he_out, int32_t* n_he_out);
+/* The seam cut of cn_cut_mesh (same arguments and results) computed on the
+ * GPU: the halfedges above, then one thread per loop vertex sweeping its fan
+ * from the interior halfedge vertex -> next loop vertex by twin(prev(h)) up
+ * to the halfedge vertex -> previous loop vertex. */
+cn_status cn_cut_mesh_gpu(int32_t n_verts, int32_t n_tris, const int32_t* tris, int32_t n_loops,
+                          const int32_t* loop_ptr, const int32_t* loop_verts, int32_t* tris_out,
+                          int32_t* parent_out, int32_t* n_verts_out);
+/* Batches of the cut surgery (CutAlgorithm.lean:49-100 subdivideEdge,
+ * :125-170 splitFace, :225-251 insertCrack) on halfedge records `he`
+ * (capacity counts[2] + 2m), counts = {vertices, faces, halfedges} updated in
+ * place.  Operation k of a batch takes the new vertex counts[0] + k (or new
+ * face counts[1] + k) and the new halfedges counts[2] + 2k, 2k + 1: the result
+ * equals the operations applied one after another in batch order.  A batch
+ * must touch disjoint records: subdivided halfedges and their twins distinct,
+ * split pairs (a, b) in distinct faces, crack anchors distinct (otherwise
+ * CN_BAD_INPUT). */
+cn_status cn_subdivide_edges(int32_t* counts, int32_t* he, int32_t m, const int32_t* edges);
+cn_status cn_split_faces(int32_t* counts, int32_t* he, int32_t m, const int32_t* a, const int32_t* b);
+cn_status cn_insert_cracks(int32_t* counts, int32_t* he, int32_t m, const int32_t* anchors);
+
 /* Assemble K = V^T L_h V (CutMeshLaplacian.lean:86-93) into CSR on the GPU,
  * reduce to the free unknowns, order, and factor (IncompleteCholesky.lean:30-33;
  * SlangCodegen/IncompleteCholesky.lean:9-12 for the level/colour schedule). */

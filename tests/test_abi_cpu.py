@@ -87,3 +87,21 @@ def test_oracle_ic0_breaks_down_after_shift_retries(oracle):
     pos, tris, h = pivot_breakdown_mesh()
     assert oracle.System(pos, tris, h, ordering=1).status == 3
     assert oracle.System(pos, tris, h, ordering=1, precond=0).status == 0
+
+
+def test_surgery_batches_reject_overlapping_records():
+    """Batches whose operations would touch one record twice are refused on
+    the host, before any device work (no GPU needed)."""
+    import ctypes as C
+    he = np.array([[1, 5, 1, 0], [2, 4, 2, 0], [0, 3, 0, 0], [2, 2, 4, -1], [1, 1, 5, -1], [0, 0, 3, -1]], np.int32)
+    counts = np.array([3, 1, 6], np.int32)
+    buf = np.zeros((10, 4), np.int32)
+    buf[:6] = he
+    IP = C.POINTER(C.c_int32)
+    ip = lambda a: a.ctypes.data_as(IP)  # noqa: E731
+    edges = np.array([0, 5], np.int32)  # halfedge 0 and its twin 5
+    assert L.lib().cn_subdivide_edges(ip(counts), ip(buf), 2, ip(edges)) == L.CN_BAD_INPUT
+    anchors = np.array([1, 1], np.int32)
+    assert L.lib().cn_insert_cracks(ip(counts), ip(buf), 2, ip(anchors)) == L.CN_BAD_INPUT
+    a, b = np.array([0, 1], np.int32), np.array([1, 2], np.int32)  # two splits of face 0
+    assert L.lib().cn_split_faces(ip(counts), ip(buf), 2, ip(a), ip(b)) == L.CN_BAD_INPUT

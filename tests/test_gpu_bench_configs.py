@@ -184,10 +184,10 @@ def test_c5_solvers_match_oracle():
             r = s.solve(t, mode="deform", precision="mixed", tol=1e-8, max_iter=20000)
             _check(r, 1e-8)
             assert rel_err(r.x, xo) <= STOP_TOL_C5, precond
-            r = s.solve(t, mode="deform", precision="mixed", tol=1e-11, max_iter=20000, max_refine=30)
-            _check(r, 1e-11)
-            assert rel_err(r.x, xo) <= TIGHT_TOL, precond
             if precond == "ic0":
+                r = s.solve(t, mode="deform", precision="mixed", tol=1e-11, max_iter=3000, max_refine=30)
+                _check(r, 1e-11)
+                assert rel_err(r.x, xo) <= TIGHT_TOL
                 r = s.solve(t, mode="deform", precision="fp64", tol=1e-13, max_iter=40000)
                 _check(r, 1e-13)
                 assert rel_err(r.x, xo) <= FP64_TOL

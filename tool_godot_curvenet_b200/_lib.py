@@ -70,6 +70,11 @@ SIGNATURES = {
     "cn_last_error": (C.c_char_p, []),
     "cn_cut_mesh": (C.c_int, [C.c_int32, C.c_int32, _I32P, C.c_int32, _I32P, _I32P, _I32P, _I32P, _I32P]),
     "cn_build": (C.c_int, [C.POINTER(MeshDesc), C.POINTER(BuildOpts), C.POINTER(_P)]),
+    "cn_halfedges": (C.c_int, [C.c_int32, C.c_int32, _I32P, _I32P, _I32P]),
+    "cn_cut_mesh_gpu": (C.c_int, [C.c_int32, C.c_int32, _I32P, C.c_int32, _I32P, _I32P, _I32P, _I32P, _I32P]),
+    "cn_subdivide_edges": (C.c_int, [_I32P, _I32P, C.c_int32, _I32P]),
+    "cn_split_faces": (C.c_int, [_I32P, _I32P, C.c_int32, _I32P, _I32P]),
+    "cn_insert_cracks": (C.c_int, [_I32P, _I32P, C.c_int32, _I32P]),
     "cn_destroy": (None, [_P]),
     "cn_solve": (C.c_int, [_P, C.c_int32, _DP, _DP, _DP, C.POINTER(SolveOpts), C.POINTER(SolveStats)]),
     "cn_solve_device": (C.c_int, [_P, C.c_int32, _P, _P, C.POINTER(SolveOpts), C.POINTER(SolveStats)]),

@@ -688,6 +688,12 @@ cn_status cn_solve_device(cn_handle S, int32_t k, const double* d_targets, doubl
     }
     grid = std::min(std::min(grid, mg), S->max_grid_alloc);
   }
+  // one block: the sweeps' y and z in shared memory when both fit
+  a.cache_bytes = 0;
+  if (grid <= 1 && !S->hsc) {
+    const size_t half = ((size_t)S->H.n * k * (mixed ? sizeof(float) : sizeof(double)) + 15) & ~(size_t)15;
+    if (2 * half <= (size_t)220 * 1024) a.cache_bytes = (int)(2 * half);
+  }
   CN_CUDA(cudaMemsetAsync(S->d_ctl, 0, sizeof(Control), S->stream));
   CN_CUDA(cudaEventRecord(S->ev0, S->stream));
   CN_CUDA(cn::launch_persistent_solve(a, o.precision, k, S->lanes, S->block, grid, S->stream));

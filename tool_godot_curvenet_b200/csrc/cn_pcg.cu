@@ -39,17 +39,34 @@ __global__ void __launch_bounds__(1024) k_solve_grid(SolveArgs a) {
   solve_body<T, K, G>(a, team, &s);
 }
 
+// One block solving alone.  With a.cache_bytes > 0 the two vectors the
+// sweeps and the product gather (y of the forward sweep, z of the backward
+// sweep and the SpMV) live in dynamic shared memory for the whole launch, so
+// the dependent chain of a level step is a shared-memory round trip instead
+// of an L2 one.
 template <typename T, int K, int G>
 __global__ void __launch_bounds__(1024) k_solve_cta(SolveArgs a) {
   __shared__ Smem<K> s;
+  extern __shared__ __align__(16) unsigned char dyn[];
   CtaTeam team;
+  if (a.cache_bytes > 0) {
+    const size_t half = (((size_t)a.n * K * sizeof(T)) + 15) & ~(size_t)15;
+    a.y = dyn;
+    a.z = dyn + half;
+  }
   solve_body<T, K, G>(a, team, &s);
 }
 
 template <typename T, int K, int G>
 cudaError_t launch_tg(const SolveArgs& a, int block, int grid, cudaStream_t st) {
   if (grid <= 1) {
-    k_solve_cta<T, K, G><<<1, block, 0, st>>>(a);
+    const int dyn = a.cache_bytes;
+    if (dyn > 0) {
+      const cudaError_t e = cudaFuncSetAttribute(k_solve_cta<T, K, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 dyn);
+      if (e != cudaSuccess) return e;
+    }
+    k_solve_cta<T, K, G><<<1, block, dyn, st>>>(a);
     return cudaGetLastError();
   }
   SolveArgs copy = a;
