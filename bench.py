@@ -298,6 +298,9 @@ def batch_section(torch, dist, world, rank, local, steps, warmup, n_meshes=512):
     d_t = torch.from_numpy(flat).to(f"cuda:{local}")
     d_x = torch.empty(int(B.out_off[-1]), dtype=torch.float64, device=f"cuda:{local}")
     stream = torch.cuda.ExternalStream(B.stream(), device=local)
+    # rows per warp per size class of mesh, by the autotuner (cached per batch shape)
+    from tool_godot_curvenet_b200.tune import BATCH_CLASSES, tune_batch_lanes
+    lanes, lane_table = tune_batch_lanes(B, d_t.data_ptr(), d_x.data_ptr(), precision="mixed", tol=1e-8)
     st_mixed = B.solve_device(d_t.data_ptr(), d_x.data_ptr(), precision="mixed", tol=1e-8)
     sts, its, rel, refs = B.mesh_stats(refinements=True)
     st_fp64 = B.solve_device(d_t.data_ptr(), d_x.data_ptr(), precision="fp64", tol=1e-8)
@@ -354,6 +357,8 @@ def batch_section(torch, dist, world, rank, local, steps, warmup, n_meshes=512):
         "n_meshes": n_meshes, "meshes_this_rank": len(mine), "n_verts_rank0": info["n_verts"],
         "nnz_A_rank0": nnz, "n_free_rank0": n,
         "cluster_size": info["cluster_size"], "n_clusters": info["n_clusters"], "block": info["block"],
+        "lanes_per_row": {"class_max_free_rows": list(BATCH_CLASSES), "lanes": list(lanes),
+                          "tuning": lane_table, "note": "autotuned per size class (8 lanes = 4 rows per warp)"},
         "mixed": {"solves_per_s": solves / (ms_m * 1e-3), "ms_per_batch": ms_m, "p50_ms": p50, "p99_ms": p99,
                   "max_iterations": st_mixed.max_iterations, "total_iterations": st_mixed.total_iterations,
                   "max_rel_residual": st_mixed.max_rel_residual, "failed": st_mixed.n_failed},

@@ -384,6 +384,17 @@ void* cn_batch_stream(cn_batch_handle b);
 cn_status cn_batch_info(cn_batch_handle b, int64_t* info);
 /* n_meshes + 1 offsets (in doubles) of each mesh's targets and positions. */
 cn_status cn_batch_offsets(cn_batch_handle b, int64_t* tgt_off, int64_t* out_off);
+/* Rows per warp of the batched launch, per size class of mesh: a mesh with
+ * n free rows takes lanes[c] lanes per row for the first class c with
+ * n <= class_max_rows[c] (the last class takes the rest); with k = 24 a lane
+ * owns 24 / lanes columns, lanes 8 (4 rows per warp) or 4 (8 rows per warp);
+ * k = 3 takes 1.  Chosen per size class by the autotuner
+ * (tool_godot_curvenet_b200/tune.py); default 8.  The multi-RHS thread
+ * mapping of SlangCodegen/SpmvMulti.lean:12-14 per mesh, in one launch. */
+cn_status cn_batch_set_lanes(cn_batch_handle b, int32_t n_classes, const int32_t* class_max_rows,
+                             const int32_t* lanes);
+/* Lanes per row of each mesh (n_meshes entries). */
+cn_status cn_batch_lanes(cn_batch_handle b, int32_t* lanes);
 /* Per-mesh results of the last solve with stats (each array nullable,
  * n_meshes entries): status, inner iterations, largest relative residual
  * over the mesh's columns, FP64 residual evaluations after the first. */

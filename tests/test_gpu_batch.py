@@ -107,3 +107,27 @@ def test_batch_preconditioners_converge_to_oracle(precond):
                 assert rel_err(x, xo) <= bar
         xs, st = B.solve([m[3] for m in meshes], precision="fp64", tol=1e-13, max_iter=3, check=False)
         assert st.n_failed > 0
+
+
+@pytest.mark.parametrize("nclusters", [0, 1])
+def test_batch_lanes_per_size_class_match_oracle(nclusters):
+    """Rows per warp per size class (cn_batch_set_lanes): the small meshes at
+    4 lanes per row, the large ones at 8, in one graph launch (two kernels
+    side by side, or one after the other with a single cluster), FP64 and
+    mixed against the oracle."""
+    meshes = small_batch()
+    ref = oracle_solutions()
+    with BatchSolver([(p, t, h) for p, t, h, _ in meshes], k=24, n_clusters=nclusters) as B:
+        B.set_lanes([600, 1 << 30], [4, 8])
+        lanes = B.lanes()
+        assert set(lanes.tolist()) == {4, 8}
+        for precision, tol, bar in [("fp64", 1e-13, FP64_TOL), ("mixed", 1e-8, MIXED_TOL)]:
+            xs, st = B.solve([m[3] for m in meshes], precision=precision, tol=tol, max_iter=20000)
+            assert st.status == 0 and st.n_failed == 0 and st.max_rel_residual <= tol
+            for x, xo in zip(xs, ref):
+                assert rel_err(x, xo) <= bar
+        B.set_lanes([1 << 30], [4])  # every mesh at 4 lanes per row
+        xs, st = B.solve([m[3] for m in meshes], precision="mixed", tol=1e-8)
+        assert st.status == 0
+        for x, xo in zip(xs, ref):
+            assert rel_err(x, xo) <= MIXED_TOL

@@ -107,6 +107,8 @@ SIGNATURES = {
     "cn_batch_info": (C.c_int, [_P, C.POINTER(C.c_int64)]),
     "cn_batch_offsets": (C.c_int, [_P, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "cn_batch_mesh_stats": (C.c_int, [_P, _I32P, _I32P, _DP, _I32P]),
+    "cn_batch_set_lanes": (C.c_int, [_P, C.c_int32, _I32P, _I32P]),
+    "cn_batch_lanes": (C.c_int, [_P, _I32P]),
     "cn_pcg_csr_noalloc": (C.c_int, [C.c_int32, _P, _P, _P, C.c_int32, _P, _P, C.c_double, C.c_int32, _P,
                                      C.POINTER(SolveStats)]),
     "cn_pcg_csr_noalloc_last_stats": (C.c_int, [C.POINTER(SolveStats)]),

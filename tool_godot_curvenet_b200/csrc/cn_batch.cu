@@ -17,6 +17,10 @@
 // Thread mapping for many right-hand sides: C lanes per row, each lane owns
 // K / C consecutive columns and walks the row's entries; the C lanes of a row
 // read one neighbour row's K values as one contiguous, coalesced segment.
+// With K = 24 a mesh takes C = 8 (4 rows per warp) or C = 4 (8 rows per
+// warp), chosen per size class by the autotuner: the meshes of each C are one
+// work queue of one persistent kernel, and both kernels are nodes of the same
+// CUDA graph, running side by side on disjoint clusters.
 #include <cooperative_groups.h>
 
 #include "cn_batch.h"
@@ -430,7 +434,7 @@ __global__ void __launch_bounds__(512, sizeof(T) == 4 ? 3 : 2) k_batch(BatchArgs
   cg::cluster_group cl = cg::this_cluster();
   const int csize = (int)cl.num_blocks();
   ClusterTeam team{(int)cl.block_rank(), csize};
-  const int cid = blockIdx.x / csize;
+  const int cid = ba.cluster_base + blockIdx.x / csize;
   T* vt = (T*)ba.vec_T + (size_t)cid * 7 * ba.stride;
   double* v64 = ba.vec_64 + (size_t)cid * 2 * ba.stride;
   for (;;) {
@@ -495,8 +499,12 @@ int max_clusters_kc(int csize, int block) {
 
 }  // namespace
 
-cudaError_t launch_batch(const BatchArgs& ba, int precision, int K, int csize, int nclusters, int block,
+cudaError_t launch_batch(const BatchArgs& ba, int precision, int K, int lanes, int csize, int nclusters, int block,
                          cudaStream_t st) {
+  if (K == 24 && lanes == 4) {
+    if (precision == CN_PREC_MIXED) return launch_kc<float, 24, 4>(ba, csize, nclusters, block, st);
+    return launch_kc<double, 24, 4>(ba, csize, nclusters, block, st);
+  }
   if (K == 24) {
     if (precision == CN_PREC_MIXED) return launch_kc<float, 24, 8>(ba, csize, nclusters, block, st);
     return launch_kc<double, 24, 8>(ba, csize, nclusters, block, st);
@@ -508,7 +516,11 @@ cudaError_t launch_batch(const BatchArgs& ba, int precision, int K, int csize, i
   return cudaErrorInvalidValue;
 }
 
-int batch_max_clusters(int precision, int K, int csize, int block) {
+int batch_max_clusters(int precision, int K, int lanes, int csize, int block) {
+  if (K == 24 && lanes == 4) {
+    if (precision == CN_PREC_MIXED) return max_clusters_kc<float, 24, 4>(csize, block);
+    return max_clusters_kc<double, 24, 4>(csize, block);
+  }
   if (K == 24) {
     if (precision == CN_PREC_MIXED) return max_clusters_kc<float, 24, 8>(csize, block);
     return max_clusters_kc<double, 24, 8>(csize, block);

@@ -19,11 +19,13 @@ struct BatchArgs {
   double* vec_64;            // per cluster: 2 vectors of `stride` doubles
   size_t stride;             // max rows x K
   DevStats* stats;           // per mesh
+  int cluster_base;          // first per-cluster scratch slot of this launch
 };
 
-cudaError_t launch_batch(const BatchArgs& ba, int precision, int K, int csize, int nclusters, int block,
+// lanes: lanes per row (K = 24: 8 or 4; K = 3: 1)
+cudaError_t launch_batch(const BatchArgs& ba, int precision, int K, int lanes, int csize, int nclusters, int block,
                          cudaStream_t st);
 // Co-resident clusters of the batch kernel for this configuration (0 if none).
-int batch_max_clusters(int precision, int K, int csize, int block);
+int batch_max_clusters(int precision, int K, int lanes, int csize, int block);
 
 }  // namespace cn

@@ -58,6 +58,10 @@ struct cn_batch {
   cn_solve_opts g_o{};
   bool have_graph = false;
   std::vector<DevStats> h_stats;
+  std::vector<int> lanes;  // lanes per row of each mesh (K = 24: 4 or 8)
+  std::vector<int> order_h;  // processing order (largest first)
+  cudaStream_t side = nullptr;  // second branch of the captured graph (the 4-lane kernel)
+  cudaEvent_t fork = nullptr, join = nullptr;
 };
 
 namespace {
@@ -68,7 +72,7 @@ void layout_batch(cn::Bump& b, cn_batch* B) {
   B->d_order = b.take<int>(B->nm);
   B->d_tgt_off = b.take<long long>(B->nm + 1);
   B->d_out_off = b.take<long long>(B->nm + 1);
-  B->d_queue = b.take<int>(1);
+  B->d_queue = b.take<int>(2);
   B->d_stats = b.take<DevStats>(B->nm);
   B->d_status = b.take<int>(1);
   B->d_vecT = b.take<double>((size_t)B->nclusters * 7 * B->stride);
@@ -168,8 +172,9 @@ cn_status cn_build_batch(const cn_mesh_desc* meshes, int32_t n_meshes, const cn_
   B->csize = cluster_size > 0 ? cluster_size : 4;
   // each precision launches as many clusters as are co-resident for its kernel
   // (FP32 fits more per SM); the per-cluster scratch is sized for the larger
-  const int mc64 = cn::batch_max_clusters(CN_PREC_FP64, k, B->csize, B->block);
-  const int mc32 = cn::batch_max_clusters(CN_PREC_MIXED, k, B->csize, B->block);
+  const int l0 = k == 24 ? 8 : 1;
+  const int mc64 = cn::batch_max_clusters(CN_PREC_FP64, k, l0, B->csize, B->block);
+  const int mc32 = cn::batch_max_clusters(CN_PREC_MIXED, k, l0, B->csize, B->block);
   if (mc64 <= 0 || mc32 <= 0) {
     set_err("no co-resident cluster of %d x %d threads fits this device", B->csize, B->block);
     return fail(CN_CUDA_ERROR);
@@ -178,6 +183,9 @@ cn_status cn_build_batch(const cn_mesh_desc* meshes, int32_t n_meshes, const cn_
   B->ncl_prec[CN_PREC_MIXED] = n_clusters > 0 ? std::min(n_clusters, mc32) : mc32;
   B->nclusters = std::max(B->ncl_prec[CN_PREC_FP64], B->ncl_prec[CN_PREC_MIXED]);
   if (cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&B->side, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&B->fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&B->join, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreate(&B->ev0) != cudaSuccess || cudaEventCreate(&B->ev1) != cudaSuccess) {
     set_err("stream/event creation failed");
     return fail(CN_CUDA_ERROR);
@@ -213,6 +221,7 @@ cn_status cn_build_batch(const cn_mesh_desc* meshes, int32_t n_meshes, const cn_
     const long long cb = (long long)B->H[b].nnzA + 2LL * B->H[b].nnzL;
     return ca > cb;
   });
+  B->order_h = order;
   if (cudaMemcpyAsync(B->d_order, order.data(), sizeof(int) * n_meshes, cudaMemcpyHostToDevice, B->stream) ||
       cudaMemcpyAsync(B->d_tgt_off, B->tgt_off.data(), sizeof(long long) * (n_meshes + 1),
                       cudaMemcpyHostToDevice, B->stream) ||
@@ -223,7 +232,36 @@ cn_status cn_build_batch(const cn_mesh_desc* meshes, int32_t n_meshes, const cn_
     return fail(CN_CUDA_ERROR);
   }
   B->h_stats.resize(n_meshes);
+  B->lanes.assign(n_meshes, k == 24 ? 8 : 1);
   *out = B;
+  return CN_OK;
+}
+
+cn_status cn_batch_set_lanes(cn_batch_handle B, int32_t n_classes, const int32_t* class_max_rows,
+                             const int32_t* lanes) {
+  if (!B || n_classes < 1 || !class_max_rows || !lanes) {
+    set_err("null argument or no size class");
+    return CN_BAD_INPUT;
+  }
+  for (int c = 0; c < n_classes; ++c) {
+    const bool ok = B->K == 24 ? (lanes[c] == 4 || lanes[c] == 8) : lanes[c] == 1;
+    if (!ok || (c > 0 && class_max_rows[c] <= class_max_rows[c - 1])) {
+      set_err("size class %d: lanes per row must be 4 or 8 for k = 24 (1 for k = 3) and the bounds must rise", c);
+      return CN_BAD_INPUT;
+    }
+  }
+  for (int m = 0; m < B->nm; ++m) {
+    int c = 0;
+    while (c < n_classes - 1 && B->H[m].n > class_max_rows[c]) ++c;
+    B->lanes[m] = lanes[c];
+  }
+  B->have_graph = false;  // the per-mesh arguments change: capture again
+  return CN_OK;
+}
+
+cn_status cn_batch_lanes(cn_batch_handle B, int32_t* lanes) {
+  if (!B || !lanes) return CN_BAD_INPUT;
+  for (int m = 0; m < B->nm; ++m) lanes[m] = B->lanes[m];
   return CN_OK;
 }
 
@@ -236,6 +274,9 @@ void cn_destroy_batch(cn_batch_handle B) {
   if (B->ev0) cudaEventDestroy(B->ev0);
   if (B->ev1) cudaEventDestroy(B->ev1);
   if (B->stream) cudaStreamDestroy(B->stream);
+  if (B->side) cudaStreamDestroy(B->side);
+  if (B->fork) cudaEventDestroy(B->fork);
+  if (B->join) cudaEventDestroy(B->join);
   delete B;
 }
 
@@ -307,28 +348,74 @@ cn_status cn_solve_batch_device(cn_batch_handle B, const double* d_targets, doub
     CN_CUDA(cudaMemcpyAsync(B->d_args, args.data(), sizeof(SolveArgs) * B->nm, cudaMemcpyHostToDevice,
                             B->stream));
     CN_CUDA(cudaStreamSynchronize(B->stream));
-    BatchArgs ba{};
-    ba.meshes = B->d_args;
-    ba.order = B->d_order;
-    ba.tgt_off = B->d_tgt_off;
-    ba.out_off = B->d_out_off;
-    ba.targets = d_targets;
-    ba.x_out = d_x_out;
-    ba.n_meshes = B->nm;
-    ba.queue = B->d_queue;
-    ba.vec_T = B->d_vecT;
-    ba.vec_64 = B->d_vec64;
-    ba.stride = B->stride;
-    ba.stats = B->d_stats;
+    // the meshes of each lanes value in processing order: group 0 (8 lanes,
+    // or 1 for k = 3) first, group 1 (4 lanes) after it in d_order
+    std::vector<int> grp[2];
+    double cost[2] = {0.0, 0.0};
+    for (int m : B->order_h) {
+      const int gi = B->lanes[m] == 4 ? 1 : 0;
+      grp[gi].push_back(m);
+      cost[gi] += (double)B->H[m].nnzA + 2.0 * B->H[m].nnzL + 4.0 * B->H[m].n;
+    }
+    std::vector<int> ord(grp[0]);
+    ord.insert(ord.end(), grp[1].begin(), grp[1].end());
+    CN_CUDA(cudaMemcpyAsync(B->d_order, ord.data(), sizeof(int) * B->nm, cudaMemcpyHostToDevice, B->stream));
+    CN_CUDA(cudaStreamSynchronize(B->stream));
+    // clusters of each kernel: the co-resident total, split by work
+    const int total = B->ncl_prec[o.precision == CN_PREC_MIXED];
+    int ncl[2] = {total, 0};
+    bool side_by_side = true;  // else the 4-lane kernel runs after the 8-lane one
+    if (!grp[1].empty()) {
+      const int mc4 = cn::batch_max_clusters(o.precision, B->K, 4, B->csize, B->block);
+      const int tot = std::min(total, mc4 > 0 ? mc4 : total);
+      if (grp[0].empty()) {
+        ncl[0] = 0;
+        ncl[1] = tot;
+      } else if (tot >= 2) {
+        ncl[1] = std::max(1, std::min(tot - 1, (int)std::lround(tot * cost[1] / (cost[0] + cost[1]))));
+        ncl[0] = tot - ncl[1];
+      } else {
+        side_by_side = false;
+        ncl[0] = ncl[1] = tot;
+      }
+    }
+    BatchArgs ba[2] = {};
+    for (int gi = 0; gi < 2; ++gi) {
+      BatchArgs& b = ba[gi];
+      b.meshes = B->d_args;
+      b.order = B->d_order + (gi ? grp[0].size() : 0);
+      b.tgt_off = B->d_tgt_off;
+      b.out_off = B->d_out_off;
+      b.targets = d_targets;
+      b.x_out = d_x_out;
+      b.n_meshes = (int)grp[gi].size();
+      b.queue = B->d_queue + gi;
+      b.vec_T = B->d_vecT;
+      b.vec_64 = B->d_vec64;
+      b.stride = B->stride;
+      b.stats = B->d_stats;
+      b.cluster_base = gi && side_by_side ? ncl[0] : 0;
+    }
     if (B->gexec) {
       cudaGraphExecDestroy(B->gexec);
       B->gexec = nullptr;
     }
     cudaGraph_t g = nullptr;
     CN_CUDA(cudaStreamBeginCapture(B->stream, cudaStreamCaptureModeThreadLocal));
-    cudaError_t e1 = cudaMemsetAsync(B->d_queue, 0, sizeof(int), B->stream);
-    cudaError_t e2 = cn::launch_batch(ba, o.precision, B->K, B->csize, B->ncl_prec[o.precision == CN_PREC_MIXED],
-                                      B->block, B->stream);
+    cudaError_t e1 = cudaMemsetAsync(B->d_queue, 0, 2 * sizeof(int), B->stream);
+    cudaError_t e2 = cudaSuccess;
+    const bool fork = ncl[1] > 0 && side_by_side;
+    if (fork) {  // the 4-lane kernel on a parallel branch of the graph
+      if (e2 == cudaSuccess) e2 = cudaEventRecord(B->fork, B->stream);
+      if (e2 == cudaSuccess) e2 = cudaStreamWaitEvent(B->side, B->fork, 0);
+      if (e2 == cudaSuccess) e2 = cn::launch_batch(ba[1], o.precision, B->K, 4, B->csize, ncl[1], B->block, B->side);
+      if (e2 == cudaSuccess) e2 = cudaEventRecord(B->join, B->side);
+    }
+    if (e2 == cudaSuccess && ncl[0] > 0)
+      e2 = cn::launch_batch(ba[0], o.precision, B->K, B->K == 24 ? 8 : 1, B->csize, ncl[0], B->block, B->stream);
+    if (e2 == cudaSuccess && ncl[1] > 0 && !side_by_side)
+      e2 = cn::launch_batch(ba[1], o.precision, B->K, 4, B->csize, ncl[1], B->block, B->stream);
+    if (e2 == cudaSuccess && fork) e2 = cudaStreamWaitEvent(B->stream, B->join, 0);
     cudaError_t e3 = cudaStreamEndCapture(B->stream, &g);
     if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess) {
       set_err("graph capture failed: %s / %s / %s", cudaGetErrorString(e1), cudaGetErrorString(e2),

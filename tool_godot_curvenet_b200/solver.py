@@ -393,6 +393,18 @@ class BatchSolver:
         L.lib().cn_batch_mesh_stats(self._h, _ip(st), _ip(it), _dp(rel), _ip(ref))
         return (st, it, rel, ref) if refinements else (st, it, rel)
 
+    def set_lanes(self, class_max_rows, lanes):
+        """Lanes per row by size class (cn_batch_set_lanes)."""
+        cm, ln = _i32(class_max_rows), _i32(lanes)
+        st = L.lib().cn_batch_set_lanes(self._h, cm.size, _ip(cm), _ip(ln))
+        if st != L.CN_OK:
+            raise CnError(st, "cn_batch_set_lanes")
+
+    def lanes(self):
+        out = np.zeros(self.n_meshes, np.int32)
+        L.lib().cn_batch_lanes(self._h, _ip(out))
+        return out
+
     def solve(self, targets, check=True, **kw):
         """targets: list of (n_handles_m, k) arrays.  Returns (list of
         (n_verts_m, k) arrays, BatchStats)."""

@@ -6,7 +6,9 @@ and keeps the fastest; the choice is cached in a JSON file keyed by the
 system's size class (rows, nnz per row, levels, preconditioner, precision,
 right-hand sides) so later builds of similar systems reuse it.
 Batches: BatchSolver candidates (blocks per cluster x threads per block) are
-built and timed; the fastest is cached the same way.
+built and timed; the fastest is cached the same way.  Rows per warp of a
+batch (lanes per row, 8 or 4 for 24 right-hand sides) are tuned per size
+class of mesh inside one handle by tune_batch_lanes.
 
     python -m tool_godot_curvenet_b200.tune --workload config2 [--sweep]
 """
@@ -21,7 +23,11 @@ import numpy as np
 from . import _lib as L
 from .solver import BatchSolver, CnError, CutMeshSolver, cut_mesh
 
-CACHE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuned_shapes.json")
+# the cache lives in the user's cache directory (CN_TUNE_CACHE overrides),
+# not in the package
+CACHE = os.environ.get("CN_TUNE_CACHE") or os.path.join(
+    os.environ.get("XDG_CACHE_HOME") or os.path.join(os.path.expanduser("~"), ".cache"),
+    "tool_godot_curvenet_b200", "tuned_shapes.json")
 
 
 def size_class(info, precond, precision, k):
@@ -38,6 +44,7 @@ def _load(path):
 
 
 def _save(path, d):
+    os.makedirs(os.path.dirname(path), exist_ok=True)
     tmp = path + ".tmp"
     with open(tmp, "w") as f:
         json.dump(d, f, indent=1, sort_keys=True)
@@ -86,6 +93,54 @@ def tune_batch(meshes, targets_flat, k=24, shapes=((2, 512), (4, 512), (8, 512),
             ms = sorted(B.solve_device(d_t.data_ptr(), d_x.data_ptr(), **solve_kw).device_ms for _ in range(reps))
             out.append(dict(cluster_size=cs, block=blk, clusters=B.info()["n_clusters"], ms=ms[len(ms) // 2]))
     return min(out, key=lambda r: r["ms"]), out
+
+
+# size classes of the batched meshes (free rows), for the lanes per row
+BATCH_CLASSES = (4096, 16384, 1 << 30)
+
+
+def batch_key(B, precision, classes=BATCH_CLASSES):
+    info = B.info()
+    n_free = info["n_free"] // max(info["n_meshes"], 1)
+    return (f"batch|{precision}|k{info['k']}|m{info['n_meshes']}|avg2^{int(round(math.log2(max(n_free, 1))))}"
+            f"|cl{'-'.join(str(c) for c in classes)}")
+
+
+def tune_batch_lanes(B, d_targets, d_x, precision="mixed", classes=BATCH_CLASSES, reps=3, cache=CACHE,
+                     **solve_kw):
+    """Rows per warp of a batch, per size class: coordinate descent over the
+    classes (each class tried at 4 lanes per row, kept if the whole batch
+    launch gets faster, median of `reps` timed launches), starting from 8
+    everywhere.  Sets the winner on B and caches it; returns (lanes, table)."""
+    key = batch_key(B, precision, classes)
+    d = _load(cache) if cache else {}
+    if key in d:
+        lanes = d[key]["lanes"]
+        B.set_lanes(classes, lanes)
+        return lanes, d[key]["table"]
+    if B.info()["k"] != 24:
+        return [1] * len(classes), []
+
+    def timed(lanes):
+        B.set_lanes(classes, lanes)
+        B.solve_device(d_targets, d_x, precision=precision, **solve_kw)  # capture the graph
+        ms = sorted(B.solve_device(d_targets, d_x, precision=precision, **solve_kw).device_ms for _ in range(reps))
+        return ms[len(ms) // 2]
+    lanes = [8] * len(classes)
+    best = timed(lanes)
+    table = [dict(lanes=list(lanes), ms=best)]
+    for c in range(len(classes)):
+        trial = list(lanes)
+        trial[c] = 4
+        ms = timed(trial)
+        table.append(dict(lanes=list(trial), ms=ms))
+        if ms < best:
+            best, lanes = ms, trial
+    B.set_lanes(classes, lanes)
+    if cache:
+        d[key] = dict(lanes=lanes, ms=best, table=table)
+        _save(cache, d)
+    return lanes, table
 
 
 def main():
