@@ -73,11 +73,22 @@ def test_cut_mesh_gpu_bit_exact(name, oracle):
     assert np.array_equal(t_gpu, t_host) and np.array_equal(p_gpu, p_host)
 
 
-def test_cut_mesh_gpu_rejects_an_open_fan():
+def test_cut_mesh_gpu_rejects_an_open_fan(oracle):
     m = uncut("cyl_open")
-    boundary_ring = [np.arange(12, dtype=np.int32)]  # row 0: its fans are open
+    nv = m.positions.shape[0]
+    # the boundary ring of row 0 with the faces on its left: every sweep from
+    # v -> next reaches the halfedge v -> prev, so the oracle's walk accepts
+    # it (the copies take all of the ring's faces), and so does the GPU
+    ring = np.arange(12, dtype=np.int32)
+    t_gpu, p_gpu = G.cut_mesh_gpu(nv, m.tris, [ring])
+    t_orc, p_orc = oracle.cut_mesh(nv, m.tris, [ring])
+    assert np.array_equal(t_gpu, t_orc) and np.array_equal(p_gpu, p_orc)
+    # the same ring reversed: the faces lie on its right, the sweep leaves the
+    # mesh through the outer face, and the oracle rejects it too
+    with pytest.raises(ValueError):
+        oracle.cut_mesh(nv, m.tris, [ring[::-1].copy()])
     with pytest.raises(CnError):
-        G.cut_mesh_gpu(m.positions.shape[0], m.tris, boundary_ring)
+        G.cut_mesh_gpu(nv, m.tris, [ring[::-1].copy()])
     with pytest.raises(CnError):
         G.cut_mesh_gpu(m.positions.shape[0], m.tris, [m.loops[0], m.loops[0]])  # a vertex in two loops
 
