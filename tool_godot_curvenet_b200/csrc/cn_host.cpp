@@ -603,7 +603,7 @@ cn_status cn_solve_device(cn_handle S, int32_t k, const double* d_targets, doubl
         if (level == 2 && S->pipe_full > cap) level = 1;
         if (level == 1 && S->pipe_cache > cap) level = 0;
         a.cache_bytes = level == 2 ? (int)S->pipe_full : level == 1 ? (int)S->pipe_cache : 0;
-        const int mg = cn::pipelined_max_grid(o.precision, k, block, a.cache_bytes, qr);
+        const int mg = cn::pipelined_max_grid(o.precision, k, block, a.cache_bytes, qr, a.pipe_mode);
         if (mg >= grid) break;
         if (mg <= 0) {
           if (level == 0) {

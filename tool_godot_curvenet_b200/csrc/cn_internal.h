@@ -155,10 +155,11 @@ cudaError_t launch_spmm(int n, int k, int precision, const int* ptr, const int* 
 // 2: up to 512).  a.pipe_mode: 0 the classic two-reduction form (two
 // barriers per iteration), 1 the pipelined form, 2 the pipelined form with a
 // fall-back to the classic one when an inner solve stops reducing the FP64
-// residual.
+// residual, 3 the single-reduction form; each form runs in a kernel compiled
+// for it alone (pipe_mode is also needed by pipelined_max_grid).
 cudaError_t launch_pipelined_solve(const SolveArgs& a, int precision, int K, int block, int grid, int qr,
                                    cudaStream_t s);
-int pipelined_max_grid(int precision, int K, int block, int cache_bytes, int qr);
+int pipelined_max_grid(int precision, int K, int block, int cache_bytes, int qr, int pipe_mode);
 // Shared memory of the row-cached solve for this launch shape (the largest
 // block's share), given A's pattern: *cache = the row cache alone, *full =
 // the row cache and the own-row state (and, for block SSOR, the colour

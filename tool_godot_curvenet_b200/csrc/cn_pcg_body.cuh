@@ -25,8 +25,9 @@ __device__ __forceinline__ unsigned long long global_ns() {
 // number e completes when the counter reaches e * gridDim.x (the host zeroes
 // it before the launch).  Each block's thread 0 adds 1 with a fire-and-forget
 // reduction after a fence, then polls with acquire loads; the wait is bounded
-// by timeout_ns (checked at every poll) and by the shared abort flag (set by
-// the first block whose wait runs out; the others leave at their next wait).
+// by timeout_ns (checked at the first poll and every 64th) and by the shared
+// abort flag (set by the first block whose wait runs out; the others leave
+// at their next wait).
 struct GridTeam {
   Control* ctl;
   long long timeout_ns;
@@ -46,14 +47,19 @@ struct GridTeam {
         const unsigned long long t0 = global_ns();
         unsigned spins = 0;
         while (ld_acquire_u32(&ctl->bar_count) < target) {
-          // the clock on every poll (a limit shorter than one barrier ends
-          // the solve at its first barrier), the abort flag every 64th
-          if ((long long)(global_ns() - t0) > timeout_ns) {
-            atomicExch(&ctl->abort, 1);
-            ok = 0;
-            break;
+          // the clock at the first poll (a limit shorter than one barrier
+          // ends the solve at its first barrier) and then with the abort
+          // flag every 64th: reading the global timer at every poll spaced
+          // the polls out and lengthened every barrier
+          const unsigned sp = spins++;
+          if (sp == 0 || (sp & 63u) == 63u) {
+            if ((long long)(global_ns() - t0) > timeout_ns) {
+              atomicExch(&ctl->abort, 1);
+              ok = 0;
+              break;
+            }
+            if (sp != 0 && *(volatile int*)&ctl->abort) { ok = 0; break; }
           }
-          if ((++spins & 63u) == 0 && *(volatile int*)&ctl->abort) { ok = 0; break; }
         }
       }
       s_ok = ok;

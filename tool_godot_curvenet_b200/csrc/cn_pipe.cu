@@ -357,7 +357,15 @@ __device__ __noinline__ void ssor_sweeps_global(const PipeSmem<K>* s, const LEnt
   }
 }
 
-template <typename T, int K, int QR, class Team>
+// The CG forms of a launch: FORM selects the code compiled into a kernel
+// (each form keeps the registers of its own loop: one kernel holding all
+// three spilled more in every one of them).
+enum { kFormClassic = 0, kFormPipe = 1, kFormSingle = 2 };
+__host__ __device__ constexpr int form_of(int pipe_mode) {
+  return pipe_mode == 3 ? kFormSingle : (pipe_mode == 1 || pipe_mode == 2) ? kFormPipe : kFormClassic;
+}
+
+template <typename T, int K, int QR, int FORM, class Team>
 __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, unsigned char* dyn) {
   // entries of a row gathered together (K values per neighbour in both forms)
   constexpr int UP = sizeof(T) == 4 ? 8 : 4;
@@ -672,7 +680,7 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
 
   // ---- single-reduction form: the blocks that own the columns of this
   // block's rows (their z is what this block gathers)
-  if (a.pipe_mode == 3) {
+  if constexpr (FORM == kFormSingle) {
     for (int i = t; i < kNbrWords; i += B) s->nbm[i] = 0u;
     __syncthreads();
     const long long rows_per = (long long)Qg * B;
@@ -820,7 +828,7 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
         // the pipelined form falls back to the classic one (for the rest of
         // the solve) when its last inner solve cut the FP64 residual of some
         // column by less than 10x
-        if (refine == 0) s->use_pipe = a.pipe_mode == 1 || a.pipe_mode == 2;
+        if (refine == 0) s->use_pipe = FORM == kFormPipe && (a.pipe_mode == 1 || a.pipe_mode == 2);
         if (s->use_pipe && a.pipe_mode == 2 && refine > 0)
           for (int c = 0; c < K; ++c)
             if (s->rrprev[c] > 0.0 && !(s->sm.sum[c] <= 1e-2 * s->rrprev[c])) s->use_pipe = 0;
@@ -851,7 +859,7 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
     }
 
     bool pipe_failed = false;
-    if (s->use_pipe) {
+    if (FORM == kFormPipe && s->use_pipe) {
     // ---- phase I: w = A u, m = M^-1 w (to m1), gamma = (r, u), delta = (w, u)
     {
       T d2[2 * K];
@@ -990,7 +998,7 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
       ++total_iters;
       if (!team.sync()) { status = CN_TIMEOUT; goto done; }
     }
-    } else if (a.pipe_mode == 3) {
+    } else if (FORM == kFormSingle) {
     // ---- the single-reduction CG, one grid barrier per iteration:
     //   gamma, delta, ||r||^2 of the last phase -> stop?, beta, alpha;
     //   p = z + beta p'; s = w + beta s'; x += alpha p; r -= alpha s;
@@ -1160,12 +1168,16 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
               const unsigned long long t0 = global_ns();
               unsigned spins = 0;
               while (ld_acquire_u32(f) < epoch) {
-                if ((long long)(global_ns() - t0) > a.timeout_ns) {
-                  atomicExch(&a.ctl->abort, 1);
-                  ok = 0;
-                  break;
+                // the clock at the first poll and every 64th (as the grid barrier)
+                const unsigned sp = spins++;
+                if (sp == 0 || (sp & 63u) == 63u) {
+                  if ((long long)(global_ns() - t0) > a.timeout_ns) {
+                    atomicExch(&a.ctl->abort, 1);
+                    ok = 0;
+                    break;
+                  }
+                  if (sp != 0 && *(volatile int*)&a.ctl->abort) { ok = 0; break; }
                 }
-                if ((++spins & 63u) == 0 && *(volatile int*)&a.ctl->abort) { ok = 0; break; }
               }
             }
           }
@@ -1441,32 +1453,32 @@ constexpr int pipe_unroll() { return sizeof(T) == 4 ? 8 : 4; }
 
 // QR = 1: one row per thread, up to 1024 threads; QR = 2: two rows per
 // thread gathered together, up to 512 threads (twice the registers).
-template <typename T, int K, int QR>
+template <typename T, int K, int QR, int FORM>
 __global__ void __launch_bounds__(1024 / QR, 1) k_pipe_grid(SolveArgs a) {
   __shared__ PipeSmem<K> s;
   extern __shared__ __align__(16) unsigned char dyn[];
   GridTeam team{a.ctl, a.timeout_ns, 0u};
-  pipe_body<T, K, QR>(a, team, &s, dyn);
+  pipe_body<T, K, QR, FORM>(a, team, &s, dyn);
 }
 
-template <typename T, int K>
+template <typename T, int K, int FORM>
 __global__ void __launch_bounds__(1024, 1) k_pipe_cta(SolveArgs a) {
   __shared__ PipeSmem<K> s;
   extern __shared__ __align__(16) unsigned char dyn[];
   CtaTeam team;
-  pipe_body<T, K, 1>(a, team, &s, dyn);
+  pipe_body<T, K, 1, FORM>(a, team, &s, dyn);
 }
 
-template <typename T, int K>
-cudaError_t launch_pk(const SolveArgs& a, int block, int grid, int qr, cudaStream_t st) {
+template <typename T, int K, int FORM>
+cudaError_t launch_pkf(const SolveArgs& a, int block, int grid, int qr, cudaStream_t st) {
   const int dyn = a.cache_bytes;
   if (grid <= 1) {
     SolveArgs c = a;
     c.cache_bytes = 0;
-    k_pipe_cta<T, K><<<1, block, 0, st>>>(c);
+    k_pipe_cta<T, K, FORM><<<1, block, 0, st>>>(c);
     return cudaGetLastError();
   }
-  auto kern = qr == 2 ? k_pipe_grid<T, K, 2> : k_pipe_grid<T, K, 1>;
+  auto kern = qr == 2 ? k_pipe_grid<T, K, 2, FORM> : k_pipe_grid<T, K, 1, FORM>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
   if (e != cudaSuccess) return e;
   SolveArgs copy = a;
@@ -1475,14 +1487,32 @@ cudaError_t launch_pk(const SolveArgs& a, int block, int grid, int qr, cudaStrea
 }
 
 template <typename T, int K>
-int max_grid_pk(int block, int dyn, int qr) {
+cudaError_t launch_pk(const SolveArgs& a, int block, int grid, int qr, cudaStream_t st) {
+  switch (form_of(a.pipe_mode)) {
+    case kFormPipe: return launch_pkf<T, K, kFormPipe>(a, block, grid, qr, st);
+    case kFormSingle: return launch_pkf<T, K, kFormSingle>(a, block, grid, qr, st);
+    default: return launch_pkf<T, K, kFormClassic>(a, block, grid, qr, st);
+  }
+}
+
+template <typename T, int K, int FORM>
+int max_grid_pkf(int block, int dyn, int qr) {
   int dev = 0, sms = 0, per = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  auto kern = qr == 2 ? k_pipe_grid<T, K, 2> : k_pipe_grid<T, K, 1>;
+  auto kern = qr == 2 ? k_pipe_grid<T, K, 2, FORM> : k_pipe_grid<T, K, 1, FORM>;
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn) != cudaSuccess) return 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, block, dyn) != cudaSuccess) return 0;
   return sms * per;
+}
+
+template <typename T, int K>
+int max_grid_pk(int block, int dyn, int qr, int pipe_mode) {
+  switch (form_of(pipe_mode)) {
+    case kFormPipe: return max_grid_pkf<T, K, kFormPipe>(block, dyn, qr);
+    case kFormSingle: return max_grid_pkf<T, K, kFormSingle>(block, dyn, qr);
+    default: return max_grid_pkf<T, K, kFormClassic>(block, dyn, qr);
+  }
 }
 
 }  // namespace
@@ -1501,15 +1531,15 @@ cudaError_t launch_pipelined_solve(const SolveArgs& a, int precision, int K, int
   return cudaErrorInvalidValue;
 }
 
-int pipelined_max_grid(int precision, int K, int block, int cache_bytes, int qr) {
+int pipelined_max_grid(int precision, int K, int block, int cache_bytes, int qr, int pipe_mode) {
   if (precision == CN_PREC_MIXED) {
-    if (K == 1) return max_grid_pk<float, 1>(block, cache_bytes, qr);
-    if (K == 3) return max_grid_pk<float, 3>(block, cache_bytes, qr);
-    if (K == 9) return max_grid_pk<float, 9>(block, cache_bytes, qr);
+    if (K == 1) return max_grid_pk<float, 1>(block, cache_bytes, qr, pipe_mode);
+    if (K == 3) return max_grid_pk<float, 3>(block, cache_bytes, qr, pipe_mode);
+    if (K == 9) return max_grid_pk<float, 9>(block, cache_bytes, qr, pipe_mode);
   } else {
-    if (K == 1) return max_grid_pk<double, 1>(block, cache_bytes, qr);
-    if (K == 3) return max_grid_pk<double, 3>(block, cache_bytes, qr);
-    if (K == 9) return max_grid_pk<double, 9>(block, cache_bytes, qr);
+    if (K == 1) return max_grid_pk<double, 1>(block, cache_bytes, qr, pipe_mode);
+    if (K == 3) return max_grid_pk<double, 3>(block, cache_bytes, qr, pipe_mode);
+    if (K == 9) return max_grid_pk<double, 9>(block, cache_bytes, qr, pipe_mode);
   }
   return 0;
 }
