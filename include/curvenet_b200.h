@@ -218,7 +218,10 @@ cn_status cn_solve_deformation(cn_handle h, const double* Fc, const double* Xc, 
  * SparseLinAlg.lean:44-60 with the multi-RHS layout of
  * SlangCodegen/SpmvMulti.lean:78-119.  precision CN_PREC_MIXED: FP32 values
  * and vectors; CN_PREC_FP64: FP64.  k in {1, 3, 9, 24}; d_x, d_y: device
- * pointers, [n_free][k] row-major, 16-byte aligned. */
+ * pointers, [n_free][k] row-major, 16-byte aligned.  FP32 with k = 1 or 3
+ * stages the rows of A through shared memory with bulk asynchronous copies;
+ * its waits are bounded, and should one run out (not expected) the rows it
+ * could not compute come back NaN. */
 cn_status cn_spmv_device(cn_handle h, int32_t k, int32_t precision, const void* d_x, void* d_y);
 
 /* ---------------------------------------------------------------------------

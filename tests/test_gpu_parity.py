@@ -296,9 +296,10 @@ def test_jacobi_mixed_converges_where_fp32_pipelining_drifts(mesh, oracle):
 @pytest.mark.parametrize("k", [1, 3, 9, 24])
 @pytest.mark.parametrize("precision", ["mixed", "fp64"])
 def test_spmv_matches_csr(name, k, precision):
-    """cn_spmv_device against the exported matrix applied on the host (the
-    larger mesh gives every block of the staged kernel several row chunks,
-    so both shared-memory buffers are used)."""
+    """cn_spmv_device against the exported matrix applied on the host, in
+    both kernels: FP32 with k = 1 or 3 runs the staged kernel (row tiles
+    copied to shared memory with bulk copies), the rest the grid-stride
+    kernel."""
     import scipy.sparse as sp
     import torch
     pos, tris, h, _ = workload(name)
@@ -315,6 +316,33 @@ def test_spmv_matches_csr(name, k, precision):
         y = d_y.double().cpu().numpy()
     want = A @ x.astype(np.float32).astype(np.float64) if precision == "mixed" else A @ x
     assert rel_err(y, want) <= (2e-6 if precision == "mixed" else 1e-14)
+
+
+@pytest.mark.slow
+@pytest.mark.parametrize("k", [1, 3])
+def test_spmv_staged_ring_wraps(k):
+    """The staged kernel on the 1.05M-row torus: about 4,100 tiles over the
+    resident blocks, so every block reuses each of its shared-memory stages
+    several times (the mbarrier phases alternate); bit-exact against the
+    grid-stride kernel's summation order is not asked, the host product in
+    FP64 of the FP32 inputs is."""
+    import scipy.sparse as sp
+    import torch
+    pos, tris, h, _ = workload("c5")
+    with CutMeshSolver(pos, tris, h, precond="jacobi") as s:
+        free_of, ptr, col, val = s.export_csr()
+        n = ptr.size - 1
+        A = sp.csr_matrix((val.astype(np.float32).astype(np.float64), col, ptr), shape=(n, n))
+        x = np.random.default_rng(7 + k).normal(size=(n, k)).astype(np.float32)
+        d_x = torch.from_numpy(x).cuda()
+        d_y = torch.full((n, k), float("nan"), dtype=torch.float32, device="cuda")
+        for _ in range(2):  # a second call on the same handle and buffers
+            s.spmv_device(k, d_x.data_ptr(), d_y.data_ptr(), precision="mixed")
+        torch.cuda.synchronize()
+        y = d_y.double().cpu().numpy()
+    want = A @ x.astype(np.float64)
+    assert np.isfinite(y).all()
+    assert rel_err(y, want) <= 2e-6
 
 
 def test_spmv_rejects_bad_arguments():

@@ -63,6 +63,8 @@ struct cn_system {
   int bss_loff_cap = 0, bss_rb = -1, bss_grid = -1;
   int* d_status = nullptr;
   unsigned* d_nbflag = nullptr;  // single-reduction form: per-block publication counts (inside buf)
+  int* d_spmv_err = nullptr;     // raised by the staged SpMV if one of its bounded waits runs out (inside buf)
+  int spmv_ents = -1;            // most entries of A in one SpMV tile (computed on first use)
   // pipelined solve: shared-memory needs of the last (grid, block, precision, k)
   int pipe_grid = -1, pipe_block = -1, pipe_prec = -1, pipe_k = -1;
   size_t pipe_cache = 0, pipe_full = 0;
@@ -131,6 +133,7 @@ void layout_all(cn::Bump& b, cn_system* S) {
   S->d_xout = b.take<double>((size_t)S->H.nv * S->kmax + 1);
   S->d_status = b.take<int>(1);
   S->d_nbflag = b.take<unsigned>((size_t)S->max_grid_alloc);
+  S->d_spmv_err = b.take<int>(1);
 }
 
 void choose_launch(cn_system* S) {
@@ -1386,7 +1389,9 @@ cn_status cn_spmv_device(cn_handle S, int32_t k, int32_t precision, const void* 
   }
   CN_CUDA(cudaSetDevice(S->device));
   const void* val = precision == CN_PREC_MIXED ? (const void*)S->D.A32 : (const void*)S->D.A64;
-  CN_CUDA(cn::launch_spmm(S->H.n, k, precision, S->D.A_ptr, S->D.A_col, val, d_x, d_y, S->stream));
+  if (S->spmv_ents < 0) S->spmv_ents = cn::spmm_tile_entries(S->H.A_ptr.data(), S->H.n);
+  CN_CUDA(cn::launch_spmm(S->H.n, k, precision, S->D.A_ptr, S->D.A_col, val, d_x, d_y, S->spmv_ents,
+                          S->d_spmv_err, S->stream));
   return CN_OK;
 }
 

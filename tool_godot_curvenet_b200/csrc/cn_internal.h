@@ -145,9 +145,15 @@ cudaError_t launch_lbs_matvec(int nv, int precision, const void* rest, const voi
                               const int* idx, const void* w, void* out, cudaStream_t s);
 
 // y = A x on a CSR matrix (cn_spmv.cu); k in {1, 3, 9, 24}, x and y
-// [n][k] in T = float (CN_PREC_MIXED) or double, 16-byte aligned.
+// [n][k] in T = float (CN_PREC_MIXED) or double, 16-byte aligned.  FP32 with
+// k = 1 or 3 stages the CSR through shared memory with bulk copies: ptr, col
+// and val then need 4 elements to spare past their ends, tile_ents is
+// spmm_tile_entries of the host row pointers and err a device int raised if
+// a bounded wait of that kernel runs out (tile_ents < 0 or err == null: the
+// grid-stride kernel).
 cudaError_t launch_spmm(int n, int k, int precision, const int* ptr, const int* col, const void* val,
-                        const void* x, void* y, cudaStream_t s);
+                        const void* x, void* y, int tile_ents, int* err, cudaStream_t s);
+int spmm_tile_entries(const int* hptr, int n);
 
 // The row-cached Jacobi-PCG persistent solve (cn_pipe.cu).  a.cache_bytes of
 // dynamic shared memory hold each block's rows of A and their CG state.

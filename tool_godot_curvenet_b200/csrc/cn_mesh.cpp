@@ -327,8 +327,9 @@ void layout(Bump& b, const MeshHost& H, MeshDev& D) {
   D.hidx = b.take<int>(H.hidx.size());
   D.free_of = b.take<int>(H.free_of.size());
   D.handles = b.take<int>(H.handles.size());
-  D.A_ptr = b.take<int>(H.A_ptr.size());
-  D.A_col = b.take<int>(H.A_col.size());
+  // 4 elements to spare: the staged SpMV's bulk copies round up to 16 bytes
+  D.A_ptr = b.take<int>(H.A_ptr.size() + 4);
+  D.A_col = b.take<int>(H.A_col.size() + 4);
   D.A_src = b.take<int>(H.A_src.size());
   D.A_diag = b.take<int>(H.A_diag.size());
   D.lev_ptr = b.take<int>(H.lev_ptr.size());
@@ -343,8 +344,8 @@ void layout(Bump& b, const MeshHost& H, MeshDev& D) {
   D.U_src = b.take<int>(H.U_src.size());
   D.face_m = b.take<double>(6 * (size_t)H.nt);
   D.K_val = b.take<double>(H.nnzK);
-  D.A64 = b.take<double>(H.nnzA);
-  D.A32 = b.take<float>(H.nnzA);
+  D.A64 = b.take<double>(H.nnzA + 4);
+  D.A32 = b.take<float>(H.nnzA + 4);
   D.L64 = b.take<double>(H.nnzL);
   D.L32 = b.take<float>(H.nnzL);
   D.U64 = b.take<double>(H.nnzL);

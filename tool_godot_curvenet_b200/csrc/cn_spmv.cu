@@ -2,18 +2,41 @@
 // handle (sm_100a), the HBM-bound primitive of SparseLinAlg.lean:44-60 and
 // SlangCodegen/SpmvMulti.lean:78-119 (X row-major n x k).
 //
-// Work item: one 16-byte chunk of one output row (4 FP32 or 2 FP64 columns)
-// when k is a multiple of the chunk, else one whole row; the grid holds the
-// blocks resident on the device at once and walks the items grid-stride
-// (one wave: about 17 % faster than one thread per item at k = 24 in FP64).  Consecutive threads
-// take consecutive chunks, so the store of Y and the gather of a neighbour
-// row of X are contiguous across the threads of a row; the row's column
-// indices and values are the same addresses for those threads (one L1
-// transaction).  Four entries are in flight per thread (indices and values
-// first, then the four gathers, then the multiply-adds): the kernel then fits
-// in 32 registers, so every SM holds 2048 threads, which keeps more loads
-// outstanding than eight entries per thread at 40-48 registers did
-// (k = 24: 46 % -> 56 % of the copy bandwidth).
+// Two kernels, chosen by the width of a row of X:
+//
+// * k_spmm_vec (k a multiple of a 16-byte chunk: FP32 k = 24, FP64 k = 24):
+//   work item = one 16-byte chunk of one output row; the grid holds the
+//   blocks resident on the device at once and walks the items grid-stride
+//   (one wave).  Consecutive threads take consecutive chunks, so the store
+//   of Y and the gather of a neighbour row of X are contiguous across the
+//   threads of a row, and the row's column indices and values are the same
+//   addresses for those threads (one L1 transaction).  Four entries are in
+//   flight per thread (indices and values first, then the four gathers, then
+//   the multiply-adds): 32 registers, 2048 threads per SM, which keeps more
+//   loads outstanding than eight entries per thread at 40-48 registers did.
+//
+// * k_spmm_staged (FP32 k = 1 and 3: rows of X of 4 or 12 bytes): one thread
+//   per row, tiles of kTileRows consecutive rows.  A producer warp per block
+//   copies each tile's row pointers, column indices and values from HBM into
+//   a ring of shared-memory stages with bulk asynchronous copies
+//   (cp.async.bulk, completion counted on the stage's mbarrier), kStages - 1
+//   tiles ahead; the consumer threads then read their row's entries from
+//   shared memory and keep only the gathers of X (up to 8 entries x k values
+//   in flight) on the critical path.  A stage is released to the producer by
+//   an arrive of every consumer warp on the stage's second mbarrier.  Every
+//   wait is bounded (kWaitNs); a wait that runs out (not expected: the
+//   copies are this SM's own) raises *err and fills the rows of the
+//   remaining tiles with NaN, so a failed product cannot pass as a result.
+//   Against the grid-stride kernel it measured 20.5 us against 22.5 us at
+//   FP32 k = 3 on the 1.05M-row torus (65 % of the measured copy bandwidth
+//   against 59 %); for 16-byte chunks (k = 24) the staged form was slower in
+//   every shape tried (one item per tile per thread waits a full memory
+//   round trip per tile).
+//
+// The bulk copies start on 16-byte boundaries: a tile's ranges are rounded
+// down to a 16-byte boundary and up to a multiple of 16 bytes, so a copy can
+// read up to 12 bytes past the last row pointer or entry; the handle's
+// row-pointer, column and value arrays are allocated with 4 elements to spare.
 #include <algorithm>
 
 #include "cn_internal.h"
@@ -47,72 +70,45 @@ __device__ __forceinline__ void fma16(double2& acc, double a, const double2& x) 
 
 constexpr int kU = 4;
 
-// K a multiple of the chunk width: thread = (row, chunk) for RPT items
-// h, h + H, ... (H = items / RPT rounded up), all of whose loads are issued
-// together: the row pointers, then every entry's index and value, then every
-// gather, then the multiply-adds.
-template <typename T, int K, int RPT>
+// K a multiple of the chunk width: thread = (row, chunk) for the items
+// tid, tid + threads, ...; each item's loads are issued together: the row
+// pointers, then every entry's index and value, then every gather, then the
+// multiply-adds.
+template <typename T, int K>
 __global__ void __launch_bounds__(256) k_spmm_vec(int n, const int* __restrict__ ptr, const int* __restrict__ col,
                                                   const T* __restrict__ val, const T* __restrict__ x,
                                                   T* __restrict__ y) {
   using V = typename V16<T>::type;
   constexpr int C = K / V16<T>::W;  // chunks per row
   const long long items = (long long)n * C;
-  const long long H = (items + RPT - 1) / RPT;
   const V* __restrict__ xv = reinterpret_cast<const V*>(x);
-  for (long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x; tid < H;
-       tid += (long long)gridDim.x * blockDim.x) {
-    int row[RPT], ch[RPT], e0[RPT], e1[RPT];
-    bool ok[RPT];
+  for (long long it = (long long)blockIdx.x * blockDim.x + threadIdx.x; it < items;
+       it += (long long)gridDim.x * blockDim.x) {
+    const int row = (int)(it / C), ch = (int)(it - (long long)row * C);
+    const int e0 = __ldg(ptr + row), e1 = __ldg(ptr + row + 1);
+    V acc;
+    if constexpr (sizeof(T) == 4) acc = make_float4(0.f, 0.f, 0.f, 0.f);
+    else acc = make_double2(0.0, 0.0);
+    for (int e = e0; e < e1; e += kU) {
+      int j[kU];
+      T a[kU];
 #pragma unroll
-    for (int q = 0; q < RPT; ++q) {
-      const long long it = tid + q * H;
-      ok[q] = it < items;
-      row[q] = ok[q] ? (int)(it / C) : 0;
-      ch[q] = ok[q] ? (int)(it - (long long)row[q] * C) : 0;
+      for (int u = 0; u < kU; ++u) {
+        const bool g = e + u < e1;
+        j[u] = g ? __ldg(col + e + u) : -1;
+        a[u] = g ? __ldg(val + e + u) : (T)0;
+      }
+      V xs[kU];
+#pragma unroll
+      for (int u = 0; u < kU; ++u) {
+        if (j[u] >= 0) xs[u] = __ldg(xv + (size_t)j[u] * C + ch);
+        else if constexpr (sizeof(T) == 4) xs[u] = make_float4(0.f, 0.f, 0.f, 0.f);
+        else xs[u] = make_double2(0.0, 0.0);
+      }
+#pragma unroll
+      for (int u = 0; u < kU; ++u) fma16(acc, a[u], xs[u]);
     }
-#pragma unroll
-    for (int q = 0; q < RPT; ++q) {
-      e0[q] = ok[q] ? __ldg(ptr + row[q]) : 0;
-      e1[q] = ok[q] ? __ldg(ptr + row[q] + 1) : 0;
-    }
-    V acc[RPT];
-#pragma unroll
-    for (int q = 0; q < RPT; ++q) {
-      if constexpr (sizeof(T) == 4) acc[q] = make_float4(0.f, 0.f, 0.f, 0.f);
-      else acc[q] = make_double2(0.0, 0.0);
-    }
-    int len = 0;
-#pragma unroll
-    for (int q = 0; q < RPT; ++q) len = max(len, e1[q] - e0[q]);
-    for (int e = 0; e < len; e += kU) {
-      int j[RPT][kU];
-      T a[RPT][kU];
-#pragma unroll
-      for (int q = 0; q < RPT; ++q)
-#pragma unroll
-        for (int u = 0; u < kU; ++u) {
-          const bool g = e0[q] + e + u < e1[q];
-          j[q][u] = g ? __ldg(col + e0[q] + e + u) : -1;
-          a[q][u] = g ? __ldg(val + e0[q] + e + u) : (T)0;
-        }
-      V xs[RPT][kU];
-#pragma unroll
-      for (int q = 0; q < RPT; ++q)
-#pragma unroll
-        for (int u = 0; u < kU; ++u) {
-          if (j[q][u] >= 0) xs[q][u] = __ldg(xv + (size_t)j[q][u] * C + ch[q]);
-          else if constexpr (sizeof(T) == 4) xs[q][u] = make_float4(0.f, 0.f, 0.f, 0.f);
-          else xs[q][u] = make_double2(0.0, 0.0);
-        }
-#pragma unroll
-      for (int q = 0; q < RPT; ++q)
-#pragma unroll
-        for (int u = 0; u < kU; ++u) fma16(acc[q], a[q][u], xs[q][u]);
-    }
-#pragma unroll
-    for (int q = 0; q < RPT; ++q)
-      if (ok[q]) reinterpret_cast<V*>(y)[(size_t)row[q] * C + ch[q]] = acc[q];
+    reinterpret_cast<V*>(y)[(size_t)row * C + ch] = acc;
   }
 }
 
@@ -150,29 +146,198 @@ __global__ void __launch_bounds__(256) k_spmm_row(int n, const int* __restrict__
   }
 }
 
-// Blocks of 256 threads resident on the whole device at once: the grid of
-// the grid-stride kernels (one wave, no tail of partly filled waves).
+// ---- the staged kernel: mbarriers and bulk copies (PTX, sm_90 and later)
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long* b, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* b, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(unsigned long long* b) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* b, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ unsigned long long ns_now() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// Wait for the completion of the phase of parity `parity`, bounded by limit_ns.
+__device__ __forceinline__ bool mbar_wait(unsigned long long* b, unsigned parity, long long limit_ns) {
+  if (mbar_try_wait(b, parity)) return true;
+  const unsigned long long t0 = ns_now();
+  for (unsigned i = 1;; ++i) {
+    if (mbar_try_wait(b, parity)) return true;
+    if ((i & 15u) == 0 && (long long)(ns_now() - t0) > limit_ns) return false;
+  }
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
+constexpr int kTileRows = 256;  // rows of a tile = consumer threads of a block
+constexpr int kStages = 3;      // shared-memory stages in the ring
+constexpr int kGather = 8;      // entries of a row whose gathers are in flight together
+constexpr long long kWaitNs = 2000000000LL;
+
+// Stage layout: [row pointers | column indices | values], each 16-byte
+// aligned and sized for `ents`, the most entries any tile holds.
+struct StageGeo {
+  static constexpr int kPtrBytes = ((kTileRows + 8) * 4 + 15) / 16 * 16;
+  __host__ __device__ static int col_bytes(int ents) { return ((ents + 8) * 4 + 15) / 16 * 16; }
+  __host__ __device__ static int val_bytes(int ents) { return ((ents + 8) * 4 + 15) / 16 * 16; }
+  __host__ __device__ static int bytes(int ents) { return kPtrBytes + col_bytes(ents) + val_bytes(ents); }
+};
+
+template <int K>
+__global__ void __launch_bounds__(kTileRows + 32) k_spmm_staged(int n, const int* __restrict__ ptr,
+                                                                const int* __restrict__ col,
+                                                                const float* __restrict__ val,
+                                                                const float* __restrict__ x, float* __restrict__ y,
+                                                                int ntiles, int ents, int* err) {
+  extern __shared__ __align__(128) unsigned char dyn[];
+  __shared__ __align__(8) unsigned long long full[kStages], empty[kStages];
+  constexpr int NW = kTileRows / 32;
+  const int sbytes = StageGeo::bytes(ents);
+  const int t = threadIdx.x, lane = t & 31;
+  if (t == 0) {
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], NW);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (t >= kTileRows) {  // the producer warp: one elected lane issues the copies
+    if (lane == 0) {
+      int i = 0;
+      for (int tile = blockIdx.x; tile < ntiles; ++i, tile += gridDim.x) {
+        const int s = i % kStages;
+        // stage s is free once every consumer warp released its use i - kStages
+        if (i >= kStages && !mbar_wait(&empty[s], ((unsigned)(i / kStages) & 1u) ^ 1u, kWaitNs)) {
+          atomicExch(err, 1);
+          break;
+        }
+        unsigned char* st = dyn + (size_t)s * sbytes;
+        const int r0 = tile * kTileRows, r1 = min(r0 + kTileRows, n);
+        const int e0 = __ldg(ptr + r0), e1 = __ldg(ptr + r1);
+        const int r0a = r0 & ~3, c0 = e0 & ~3;
+        const unsigned pb = (unsigned)(((r1 + 1 - r0a) * 4 + 15) & ~15);
+        const unsigned cb = (unsigned)(((e1 - c0) * 4 + 15) & ~15);
+        mbar_expect_tx(&full[s], pb + 2 * cb);
+        bulk_g2s(st, ptr + r0a, pb, &full[s]);
+        if (cb) {
+          bulk_g2s(st + StageGeo::kPtrBytes, col + c0, cb, &full[s]);
+          bulk_g2s(st + StageGeo::kPtrBytes + StageGeo::col_bytes(ents), val + c0, cb, &full[s]);
+        }
+      }
+      // the copies still in flight land before the block may exit
+      for (int q = max(0, i - kStages); q < i; ++q)
+        if (!mbar_wait(&full[q % kStages], (unsigned)(q / kStages) & 1u, kWaitNs)) atomicExch(err, 1);
+    }
+    return;
+  }
+  bool failed = false;
+  int i = 0;
+  for (int tile = blockIdx.x; tile < ntiles; ++i, tile += gridDim.x) {
+    const int row = tile * kTileRows + t;
+    if (!failed) {
+      const int s = i % kStages;
+      const bool got = mbar_wait(&full[s], (unsigned)(i / kStages) & 1u, kWaitNs);
+      if (!__all_sync(0xffffffffu, got)) {
+        failed = true;
+        if (lane == 0) atomicExch(err, 1);
+      } else {
+        const unsigned char* st = dyn + (size_t)s * sbytes;
+        const int* sp = reinterpret_cast<const int*>(st);
+        const int* sc = reinterpret_cast<const int*>(st + StageGeo::kPtrBytes);
+        const float* sv = reinterpret_cast<const float*>(st + StageGeo::kPtrBytes + StageGeo::col_bytes(ents));
+        const int r0a = (tile * kTileRows) & ~3;
+        const int c0 = sp[tile * kTileRows - r0a] & ~3;
+        const bool ok = row < n;
+        const int eb = ok ? sp[row - r0a] : 0, ee = ok ? sp[row + 1 - r0a] : 0;
+        float acc[K];
+#pragma unroll
+        for (int c = 0; c < K; ++c) acc[c] = 0.f;
+        for (int e = eb; e < ee; e += kGather) {
+          int j[kGather];
+          float a[kGather];
+#pragma unroll
+          for (int u = 0; u < kGather; ++u) {
+            const bool g = e + u < ee;
+            j[u] = g ? sc[e + u - c0] : -1;
+            a[u] = g ? sv[e + u - c0] : 0.f;
+          }
+          float xs[kGather][K];
+#pragma unroll
+          for (int u = 0; u < kGather; ++u)
+#pragma unroll
+            for (int c = 0; c < K; ++c) xs[u][c] = j[u] >= 0 ? __ldg(x + (size_t)j[u] * K + c) : 0.f;
+#pragma unroll
+          for (int u = 0; u < kGather; ++u)
+#pragma unroll
+            for (int c = 0; c < K; ++c) acc[c] += a[u] * xs[u][c];
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[s]);
+        if (ok)
+#pragma unroll
+          for (int c = 0; c < K; ++c) y[(size_t)row * K + c] = acc[c];
+        continue;
+      }
+    }
+    if (row < n)
+#pragma unroll
+      for (int c = 0; c < K; ++c) y[(size_t)row * K + c] = __int_as_float(0x7fc00000);
+  }
+}
+
+// Blocks of `threads` resident on the whole device at once: the grid of the
+// grid-stride and staged kernels (one wave, no tail of partly filled waves).
 template <typename F>
-int resident_blocks(F kern) {
+int resident_blocks(F kern, int threads, size_t smem) {
   int dev = 0, sms = 148, per = 1;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, 256, 0) != cudaSuccess || per < 1) per = 1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, threads, smem) != cudaSuccess || per < 1) per = 1;
   return sms * per;
+}
+
+template <int K>
+cudaError_t launch_staged(int n, const int* ptr, const int* col, const float* val, const float* x, float* y,
+                          int ents, int* err, cudaStream_t s) {
+  const int ntiles = (n + kTileRows - 1) / kTileRows;
+  const size_t smem = (size_t)kStages * StageGeo::bytes(ents);
+  auto kern = k_spmm_staged<K>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  const int slots = resident_blocks(kern, kTileRows + 32, smem);
+  kern<<<std::min(ntiles, slots), kTileRows + 32, smem, s>>>(n, ptr, col, val, x, y, ntiles, ents, err);
+  return cudaGetLastError();
 }
 
 template <typename T, int K>
 cudaError_t launch_k(int n, const int* ptr, const int* col, const T* val, const T* x, T* y, cudaStream_t s) {
   if (n <= 0) return cudaSuccess;
   if constexpr (K % V16<T>::W == 0) {
-    constexpr int RPT = 1;
     const long long items = (long long)n * (K / V16<T>::W);
-    const long long threads = (items + RPT - 1) / RPT;
-    static const int slots = resident_blocks(k_spmm_vec<T, K, RPT>);
-    const long long nb = std::min<long long>((threads + 255) / 256, slots);
-    k_spmm_vec<T, K, RPT><<<(unsigned)nb, 256, 0, s>>>(n, ptr, col, val, x, y);
+    static const int slots = resident_blocks(k_spmm_vec<T, K>, 256, 0);
+    const long long nb = std::min<long long>((items + 255) / 256, slots);
+    k_spmm_vec<T, K><<<(unsigned)nb, 256, 0, s>>>(n, ptr, col, val, x, y);
   } else {
-    static const int slots = resident_blocks(k_spmm_row<T, K>);
+    static const int slots = resident_blocks(k_spmm_row<T, K>, 256, 0);
     const long long nb = std::min<long long>((n + 255) / 256, slots);
     k_spmm_row<T, K><<<(unsigned)nb, 256, 0, s>>>(n, ptr, col, val, x, y);
   }
@@ -193,10 +358,22 @@ cudaError_t launch_t(int n, int k, const int* ptr, const int* col, const T* val,
 
 }  // namespace
 
+int spmm_tile_entries(const int* hptr, int n) {
+  int ents = 0;
+  for (int r0 = 0; r0 < n; r0 += kTileRows) ents = std::max(ents, hptr[std::min(r0 + kTileRows, n)] - hptr[r0]);
+  return ents;
+}
+
 cudaError_t launch_spmm(int n, int k, int precision, const int* ptr, const int* col, const void* val,
-                        const void* x, void* y, cudaStream_t s) {
-  if (precision == CN_PREC_MIXED)
+                        const void* x, void* y, int tile_ents, int* err, cudaStream_t s) {
+  if (precision == CN_PREC_MIXED) {
+    if (n > 0 && (k == 1 || k == 3) && tile_ents >= 0 && err) {
+      const float* v = (const float*)val;
+      return k == 1 ? launch_staged<1>(n, ptr, col, v, (const float*)x, (float*)y, tile_ents, err, s)
+                    : launch_staged<3>(n, ptr, col, v, (const float*)x, (float*)y, tile_ents, err, s);
+    }
     return launch_t<float>(n, k, ptr, col, (const float*)val, (const float*)x, (float*)y, s);
+  }
   return launch_t<double>(n, k, ptr, col, (const double*)val, (const double*)x, (double*)y, s);
 }
 
