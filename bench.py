@@ -166,6 +166,19 @@ def algorithmic_bytes_pipelined(info, stats, k, mixed):
     return stats.iterations * b_iter + (stats.refinements + 1) * b_res + b_rhs
 
 
+def algorithmic_bytes_bssor_pipelined(info, stats, k, mixed):
+    """Bytes the pipelined CG with block SSOR must move: the pipelined
+    Jacobi form's bytes plus, per inner iteration, a read and a write of the
+    two more own-row vectors u = M^-1 r and q = M^-1 s, and the two
+    triangular sweeps of m = M^-1 w over the off-diagonal entries (scaled
+    value and neighbour index) with a read and a write of the sweep vector in
+    each."""
+    n, nnz = info["n_free"], info["nnz_A"]
+    sv = 4 if mixed else 8
+    sweeps = (nnz - n) * (sv + 4) + 4 * n * k * sv
+    return algorithmic_bytes_pipelined(info, stats, k, mixed) + stats.iterations * (4 * n * k * sv + sweeps)
+
+
 def algorithmic_bytes_classic(info, stats, k, mixed):
     """Bytes the two-reduction Jacobi-PCG must move: per inner iteration one
     SpMV (A's values and columns, row pointer, the gathered z and p), a read
@@ -737,7 +750,8 @@ def main():
     st_ic = one("mixed", stats=True, sv=solver_ic)
     st_jac = one("mixed", stats=True, sv=solver_j)
     st_classic = one("mixed", "pipelined", stats=True, sv=solver_j)
-    for s in (st_mixed, st_fp64, st_plain, st_ic, st_jac, st_classic):
+    st_bss2 = one("mixed", "classic", stats=True)
+    for s in (st_mixed, st_fp64, st_plain, st_ic, st_jac, st_classic, st_bss2):
         if s.status != 0:
             raise SystemExit(f"solve failed: status {s.status}")
 
@@ -771,6 +785,7 @@ def main():
     t_ic = timed("mixed", "fused", max(3, args.steps // 3), 2, sv=solver_ic)
     t_jac = timed("mixed", "fused", max(3, args.steps // 3), 2, sv=solver_j)
     t_classic = timed("mixed", "pipelined", max(3, args.steps // 3), 2, sv=solver_j)
+    t_bss2 = timed("mixed", "classic", max(3, args.steps // 3), 2)
 
     # e2e: host (pinned) buffers through cn_solve, H2D of the targets and D2H of
     # the deformed positions inside the timed region
@@ -811,11 +826,12 @@ def main():
     ms_ic = maxred(sum(t_ic) / len(t_ic))
     ms_jac = maxred(sum(t_jac) / len(t_jac))
     ms_classic = maxred(sum(t_classic) / len(t_classic))
+    ms_bss2 = maxred(sum(t_bss2) / len(t_bss2))
     peak, peak_kind = load_peaks()
-    bytes_mixed = algorithmic_bytes_bssor(info, st_mixed, k, True)
+    bytes_mixed = algorithmic_bytes_bssor_pipelined(info, st_mixed, k, True)
     bytes_fp64 = algorithmic_bytes_pipelined(info, st_fp64, k, False)
     ach = bytes_mixed / (ms_mixed * 1e-3) / 1e9
-    traffic, traffic_src = capture_traffic("cn_pipe_solve_bssor_mixed", WORKLOAD, info, st_mixed)
+    traffic, traffic_src = capture_traffic("cn_pipe_solve_bssor_pipelined_mixed", WORKLOAD, info, st_mixed)
     spmv = None
     if not args.no_spmv and rank == 0:
         spmv = spmv_section(torch, local, peak)
@@ -849,7 +865,7 @@ def main():
             "dtype": "f32 inner / f64 residual",
             "data": "synthetic (seeded torus, see tool_godot_curvenet_b200/synth.py config2)",
             "config": {"workload": WORKLOAD, "n_verts": nv, "n_free": info["n_free"], "nnz_A": info["nnz_A"],
-                       "rhs": k, "tol": 1e-8, "precond": "block SSOR (blocks = the rows each CTA owns, DSatur colours inside a block), natural row order; two-reduction CG on the row-cached kernel (rows of A, the CG state and the colour lists in shared memory)",
+                       "rhs": k, "tol": 1e-8, "precond": "block SSOR (blocks = the rows each CTA owns, DSatur colours inside a block), natural row order; pipelined CG (one team barrier per iteration, u = M^-1 r and q = M^-1 s by recurrence) on the row-cached kernel (rows of A, the CG state and the colour lists in shared memory)",
                        "launch": f"grid {info['grid']} x block auto (2 rows per thread)", "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
                        "l2": "flushed (256 MB read) before every timed solve, outside the events"},
             "mixed": {"iterations": st_mixed.iterations, "refinements": st_mixed.refinements,
@@ -868,6 +884,9 @@ def main():
             "jacobi_pipelined_mixed": {"solves_per_s": 1e3 / ms_classic, "ms": ms_classic,
                                        "iterations": st_classic.iterations, "refinements": st_classic.refinements,
                                        "note": "same kernel, pipelined CG in FP32 (one team barrier per iteration; not the default: its recurrences drift on ill-conditioned meshes)"},
+            "bssor_two_reduction_mixed": {"solves_per_s": 1e3 / ms_bss2, "ms": ms_bss2,
+                                          "iterations": st_bss2.iterations, "refinements": st_bss2.refinements,
+                                          "note": "the headline handle with the two-reduction CG (two team barriers per iteration)"},
             "speedup_mixed_vs_fp64_plain": ms_plain / ms_mixed,
             "speedup_mixed_vs_fp64_fused": ms_fp64 / ms_mixed,
             "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
@@ -876,7 +895,7 @@ def main():
                                     "shared-memory colour sweeps; A and the CG state stay in shared memory",
                          "dram_achieved_gbs": (traffic / (ms_mixed * 1e-3) / 1e9) if traffic else None,
                          "dram_frac": (traffic / (ms_mixed * 1e-3) / 1e9 / peak) if traffic else None,
-                         "kernel": f"k_pipe_grid<float,3,2> (row-cached persistent solve, block SSOR, grid {info['grid']})",
+                         "kernel": f"k_pipe_grid<float,3,2,3> (row-cached persistent solve, pipelined CG with block SSOR, grid {info['grid']})",
                          "note": "achieved = the algorithmic bytes of an unfused solve (every iteration streams A, "
                                  "the sweeps and the vectors) / device time; dram_* = the bytes the fused kernel "
                                  "actually moves (ncu) / device time",

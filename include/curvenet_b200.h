@@ -71,14 +71,17 @@ enum { CN_MODE_HARMONIC = 0, CN_MODE_DEFORM = 1, CN_MODE_RHS = 2 };
  * (one team barrier per iteration, falling back to the two-reduction form if
  * an inner solve stops reducing the residual), in mixed precision the
  * two-reduction CG (two barriers per iteration; FP32 pipelined recurrences
- * drift on ill-conditioned meshes).  With IC(0) / HSC: the level-scheduled
- * kernel.  CLASSIC: the two-reduction CG (row-cached kernel with Jacobi).
- * PIPELINED: the pipelined CG without fall-back, both precisions (Jacobi
- * only).  PLAIN: one kernel per primitive, FP64 Jacobi.  SINGLE: the
- * single-reduction CG (Chronopoulos & Gear: alpha and beta from one
- * reduction of (r, z), (z, A z), ||r||^2) on the row-cached kernel, Jacobi
- * or block SSOR: one grid barrier per iteration, z exchanged with the
- * neighbour blocks only. */
+ * drift on ill-conditioned meshes).  With block SSOR: in mixed precision
+ * the pipelined CG keeping u = M^-1 r and q = M^-1 s by recurrence, inner
+ * solves of at most 1e-3 restarted by the FP64 refinement, with the same
+ * fall-back; in FP64 the two-reduction CG.  With IC(0) / HSC: the
+ * level-scheduled kernel.  CLASSIC: the two-reduction CG (row-cached
+ * kernel).  PIPELINED: the pipelined CG without fall-back (Jacobi in both
+ * precisions, block SSOR in mixed precision).  PLAIN: one kernel per
+ * primitive, FP64 Jacobi.  SINGLE: the single-reduction CG (Chronopoulos
+ * & Gear: alpha and beta from one reduction of (r, z), (z, A z), ||r||^2)
+ * on the row-cached kernel, Jacobi or block SSOR: one grid barrier per
+ * iteration, z exchanged with the neighbour blocks only. */
 enum { CN_ALGO_FUSED = 0, CN_ALGO_PLAIN = 1, CN_ALGO_CLASSIC = 2, CN_ALGO_PIPELINED = 3, CN_ALGO_SINGLE = 4 };
 
 typedef struct {
@@ -99,7 +102,7 @@ typedef struct {
 typedef struct {
   int32_t precision;   /* CN_PREC_FP64 or CN_PREC_MIXED */
   int32_t mode;        /* CN_MODE_HARMONIC, CN_MODE_DEFORM (targets) or CN_MODE_RHS */
-  int32_t algo;        /* CN_ALGO_FUSED, CN_ALGO_CLASSIC, CN_ALGO_PIPELINED or CN_ALGO_PLAIN */
+  int32_t algo;        /* CN_ALGO_FUSED, _CLASSIC, _PIPELINED, _SINGLE or _PLAIN */
   double tol;          /* relative residual ||b - A x|| / ||b|| per column */
   int32_t max_iter;    /* inner PCG iterations per refinement step */
   int32_t max_refine;  /* FP64 residual refinements (mixed precision) */

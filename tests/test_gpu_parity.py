@@ -391,12 +391,27 @@ def test_block_ssor_takes_fewer_iterations_than_jacobi():
     assert its["bssor"] < 0.8 * its["jacobi"], its
 
 
-def test_block_ssor_rejects_pipelined_form():
-    pos, tris, h, t = workload("cyl_tiny")
+@pytest.mark.parametrize("name", ["cyl_tiny", "torus_small", "torus_mid"])
+@pytest.mark.parametrize("algo", ["fused", "pipelined", "classic"])
+def test_block_ssor_cg_forms_match_oracle(name, algo, oracle):
+    """Block SSOR in mixed precision in its three CG forms: the default
+    (pipelined, u = M^-1 r and q = M^-1 s by recurrence, falling back to the
+    two-reduction form if an inner solve stalls), the pipelined form alone
+    and the two-reduction form, each to the oracle's answer; the pipelined
+    form is FP32 only."""
+    pos, tris, h, t = workload(name)
+    t = t[:, :3]
+    ref = oracle.System(pos, tris, h)
+    st, xo, _, _ = ref.solve(t, mode=1, tol=1e-13)
+    assert st == 0
     with CutMeshSolver(pos, tris, h, precond="bssor") as s:
-        with pytest.raises(CnError) as e:
-            s.solve(t[:, :3], mode="deform", algo="pipelined")
-        assert e.value.status == L.CN_BAD_INPUT
+        r = s.solve(t, mode="deform", precision="mixed", tol=1e-8, algo=algo, max_iter=20000)
+        assert r.status == 0 and np.all(r.rel_residual <= 1e-8)
+        assert rel_err(r.x, xo) <= MIXED_TOL
+        if algo == "pipelined":
+            with pytest.raises(CnError) as e:
+                s.solve(t, mode="deform", precision="fp64", algo="pipelined")
+            assert e.value.status == L.CN_BAD_INPUT
 
 
 @pytest.mark.parametrize("name", ["cyl_tiny", "c1", "torus_small", "torus_mid", "c3_0"])

@@ -66,7 +66,7 @@ struct cn_system {
   int* d_spmv_err = nullptr;     // raised by the staged SpMV if one of its bounded waits runs out (inside buf)
   int spmv_ents = -1;            // most entries of A in one SpMV tile (computed on first use)
   // pipelined solve: shared-memory needs of the last (grid, block, precision, k)
-  int pipe_grid = -1, pipe_block = -1, pipe_prec = -1, pipe_k = -1;
+  int pipe_grid = -1, pipe_block = -1, pipe_prec = -1, pipe_k = -1, pipe_rec = -1;
   size_t pipe_cache = 0, pipe_full = 0;
   int max_grid_alloc = 0;
   bool shape_set = false;   // cn_set_launch fixed the launch shape
@@ -563,8 +563,9 @@ cn_status cn_solve_device(cn_handle S, int32_t k, const double* d_targets, doubl
   a.ctl = S->d_ctl; a.stats = S->d_stats;
   a.timeout_ns = o.wait_limit_ms > 0.0 ? (long long)(o.wait_limit_ms * 1e6) : 2000000000LL;
   a.m0 = S->d_m[0]; a.m1 = S->d_m[1]; a.m2 = S->d_m[2]; a.pown = S->d_pown; a.dinv64 = S->D.dinv64;
-  if (o.algo == CN_ALGO_PIPELINED && (S->hsc || S->opts.precond != CN_PRECOND_JACOBI)) {
-    set_err("the pipelined form needs the Jacobi preconditioner");
+  if (o.algo == CN_ALGO_PIPELINED &&
+      (!row_cached(S) || (S->opts.precond == CN_PRECOND_BSSOR && o.precision != CN_PREC_MIXED))) {
+    set_err("the pipelined form needs the Jacobi preconditioner, or block SSOR in mixed precision");
     return CN_BAD_INPUT;
   }
   if (o.algo == CN_ALGO_SINGLE && !row_cached(S)) {
@@ -572,14 +573,20 @@ cn_status cn_solve_device(cn_handle S, int32_t k, const double* d_targets, doubl
     return CN_BAD_INPUT;
   }
   if (row_cached(S)) {
-    // FP64: pipelined, falling back to the two-reduction form if an inner
-    // solve stalls; mixed: the two-reduction form (the FP32 pipelined
-    // recurrences drift on ill-conditioned meshes), pipelined on request
-    a.pipe_mode = o.algo == CN_ALGO_PIPELINED ? 1 : o.algo == CN_ALGO_CLASSIC ? 0
-                : o.precision == CN_PREC_FP64 ? 2 : 0;
+    // Jacobi -- FP64: pipelined, falling back to the two-reduction form if
+    // an inner solve stalls; mixed: the two-reduction form (the FP32
+    // pipelined recurrences drift on ill-conditioned meshes), pipelined on
+    // request.  Block SSOR -- mixed: pipelined with u = M^-1 r kept by
+    // recurrence, with the same fall-back; FP64: the two-reduction form.
     const bool bssor = S->opts.precond == CN_PRECOND_BSSOR;
-    if (bssor) a.pipe_mode = 0;  // the pipelined recurrences assume a diagonal M
+    if (!bssor)
+      a.pipe_mode = o.algo == CN_ALGO_PIPELINED ? 1 : o.algo == CN_ALGO_CLASSIC ? 0
+                  : o.precision == CN_PREC_FP64 ? 2 : 0;
+    else
+      a.pipe_mode = o.precision != CN_PREC_MIXED || o.algo == CN_ALGO_CLASSIC ? 0
+                  : o.algo == CN_ALGO_PIPELINED ? 5 : 4;
     if (o.algo == CN_ALGO_SINGLE) a.pipe_mode = 3;
+    int rec = a.pipe_mode == 4 || a.pipe_mode == 5 ? 8 : 6;
     a.nbflag = S->d_nbflag;
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, S->device);
@@ -588,36 +595,55 @@ cn_status cn_solve_device(cn_handle S, int32_t k, const double* d_targets, doubl
              : S->opts.grid > 0 ? S->opts.grid : std::min(sms, std::max(1, (S->H.n + 255) / 256));
     int block = S->block, qr = 1;
     a.cache_bytes = 0;
-    if (grid > 1) {
-      grid = std::min(grid, S->max_grid_alloc);
-      // two rows per thread, gathered together: block = n / (2 grid) rounded
-      // up to a warp (an explicit block above 512 runs one row per thread)
-      if (!S->shape_set && S->opts.block <= 0)
-        block = std::min(512, std::max(128, ((S->H.n + 2 * grid - 1) / (2 * grid) + 31) / 32 * 32));
-      qr = block <= 512 ? 2 : 1;
-      const size_t cap = 220 * 1024;
+    const int grid0 = grid, block0 = block;
+    // The block-SSOR pipelined default needs each block's whole state in
+    // shared memory (its longer records and the lists); where that does not
+    // fit (the 1M-row torus: 14 row slices a block) the two-reduction form
+    // measured faster, so the default falls back to it before the launch.
+    for (int attempt = 0; attempt < 2; ++attempt) {
+      grid = grid0;
+      block = block0;
+      qr = 1;
+      a.cache_bytes = 0;
+      rec = a.pipe_mode == 4 || a.pipe_mode == 5 ? 8 : 6;
       int level = 2;  // 2: row cache and own state in shared memory, 1: row cache only, 0: none
-      for (int tries = 0; tries < 6; ++tries) {
-        if (S->pipe_grid != grid || S->pipe_block != block || S->pipe_prec != o.precision || S->pipe_k != k) {
-          cn::pipelined_smem_need(S->H.A_ptr.data(), S->H.A_col.data(), S->H.n, grid, block, o.precision, k, bssor,
-                                  &S->pipe_cache, &S->pipe_full);
-          S->pipe_grid = grid; S->pipe_block = block; S->pipe_prec = o.precision; S->pipe_k = k;
-        }
-        if (level == 2 && S->pipe_full > cap) level = 1;
-        if (level == 1 && S->pipe_cache > cap) level = 0;
-        a.cache_bytes = level == 2 ? (int)S->pipe_full : level == 1 ? (int)S->pipe_cache : 0;
-        const int mg = cn::pipelined_max_grid(o.precision, k, block, a.cache_bytes, qr, a.pipe_mode);
-        if (mg >= grid) break;
-        if (mg <= 0) {
-          if (level == 0) {
-            set_err("the pipelined solve does not fit on this device (block %d)", block);
-            return CN_CUDA_ERROR;
+      if (grid > 1) {
+        grid = std::min(grid, S->max_grid_alloc);
+        // two rows per thread, gathered together: block = n / (2 grid) rounded
+        // up to a warp (an explicit block above 512 runs one row per thread)
+        if (!S->shape_set && S->opts.block <= 0)
+          block = std::min(512, std::max(128, ((S->H.n + 2 * grid - 1) / (2 * grid) + 31) / 32 * 32));
+        qr = block <= 512 ? 2 : 1;
+        const size_t cap = 220 * 1024;
+        for (int tries = 0; tries < 6; ++tries) {
+          if (S->pipe_grid != grid || S->pipe_block != block || S->pipe_prec != o.precision || S->pipe_k != k ||
+              S->pipe_rec != rec) {
+            cn::pipelined_smem_need(S->H.A_ptr.data(), S->H.A_col.data(), S->H.n, grid, block, o.precision, k, bssor,
+                                    rec, &S->pipe_cache, &S->pipe_full);
+            S->pipe_grid = grid; S->pipe_block = block; S->pipe_prec = o.precision; S->pipe_k = k;
+            S->pipe_rec = rec;
           }
-          --level;
-          continue;
+          if (level == 2 && S->pipe_full > cap) level = 1;
+          if (level == 1 && S->pipe_cache > cap) level = 0;
+          a.cache_bytes = level == 2 ? (int)S->pipe_full : level == 1 ? (int)S->pipe_cache : 0;
+          const int mg = cn::pipelined_max_grid(o.precision, k, block, a.cache_bytes, qr, a.pipe_mode);
+          if (mg >= grid) break;
+          if (mg <= 0) {
+            if (level == 0) {
+              set_err("the pipelined solve does not fit on this device (block %d)", block);
+              return CN_CUDA_ERROR;
+            }
+            --level;
+            continue;
+          }
+          grid = mg;
         }
-        grid = mg;
       }
+      if (a.pipe_mode == 4 && grid > 1 && level < 2) {
+        a.pipe_mode = 0;
+        continue;
+      }
+      break;
     }
     a.bcolor = nullptr;
     a.bncolor = 0;

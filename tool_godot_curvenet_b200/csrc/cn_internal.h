@@ -161,17 +161,21 @@ int spmm_tile_entries(const int* hptr, int n);
 // 2: up to 512).  a.pipe_mode: 0 the classic two-reduction form (two
 // barriers per iteration), 1 the pipelined form, 2 the pipelined form with a
 // fall-back to the classic one when an inner solve stops reducing the FP64
-// residual, 3 the single-reduction form; each form runs in a kernel compiled
-// for it alone (pipe_mode is also needed by pipelined_max_grid).
+// residual, 3 the single-reduction form, 4 the pipelined form with block
+// SSOR (u = M^-1 r and q = M^-1 s kept by recurrence, FP32 only) with the
+// same fall-back as 2, 5 the same without the fall-back; each form runs in a
+// kernel compiled for it alone (pipe_mode is also needed by
+// pipelined_max_grid).
 cudaError_t launch_pipelined_solve(const SolveArgs& a, int precision, int K, int block, int grid, int qr,
                                    cudaStream_t s);
 int pipelined_max_grid(int precision, int K, int block, int cache_bytes, int qr, int pipe_mode);
 // Shared memory of the row-cached solve for this launch shape (the largest
 // block's share), given A's pattern: *cache = the row cache alone, *full =
-// the row cache and the own-row state (and, for block SSOR, the colour
-// lists); SIZE_MAX when a block holds more than kPipeSlices row slices.
+// the row cache and the own-row state of rec_vectors K + 1 values a row
+// (and, for block SSOR, the colour lists); SIZE_MAX when a block holds more
+// than kPipeSlices row slices.
 void pipelined_smem_need(const int* A_ptr, const int* A_col, int n, int grid, int block, int precision, int K,
-                         bool bssor, size_t* cache, size_t* full);
+                         bool bssor, int rec_vectors, size_t* cache, size_t* full);
 // Greedy colouring of the rows inside each block of rb consecutive rows, in
 // row order, over the couplings inside the block (at most 64 colours);
 // returns the number of colours.

@@ -49,6 +49,7 @@
 #include <algorithm>
 #include <set>
 #include <tuple>
+#include <type_traits>
 #include <vector>
 
 #include "cn_pcg_body.cuh"
@@ -261,24 +262,27 @@ __device__ void block_reduce_strided(const A (&v)[N], double* red, double* out, 
   }
 }
 
-// Own-row state in T, one contiguous record of 6K + 1 values per row:
-// quantities r, w, z, s, p, x (K columns each), then 1/A_ii.  An odd record
-// length keeps the shared-memory accesses of a warp on distinct banks.
-enum { kQr = 0, kQw = 1, kQz = 2, kQs = 3, kQp = 4, kQx = 5, kQminv = 6 };
-template <typename T, int K>
+// Own-row state in T, one contiguous record of (6 + EX) K + 1 values per
+// row: quantities r, w, z, s, p, x (K columns each), with EX = 2 also u and
+// q (the pipelined form with block SSOR keeps u = M^-1 r and q = M^-1 s by
+// recurrence), then 1/A_ii.  An odd record length keeps the shared-memory
+// accesses of a warp on distinct banks.
+enum { kQr = 0, kQw = 1, kQz = 2, kQs = 3, kQp = 4, kQx = 5, kQu = 6, kQq = 7 };
+template <typename T, int K, int EX = 0>
 struct OwnRef {
-  static constexpr int kLen = 6 * K + 1;
+  static constexpr int kLen = (6 + EX) * K + 1;
   T* p;
   __device__ __forceinline__ T& operator()(int qy, int c) const { return p[qy * K + c]; }
+  __device__ __forceinline__ T& minv() const { return p[kLen - 1]; }
 };
 
 // One own row's update of a pipelined iteration: z = n + beta z,
 // s = w + beta s, p = M^-1 r + beta p, x += alpha p, r -= alpha s,
 // w -= alpha z; m = M^-1 w to mnext; (r, M^-1 r) and (w, M^-1 r) into d2.
-template <typename T, int K>
-__device__ __forceinline__ void pipe_update(const OwnRef<T, K>& o, int row, const T (&nn)[K], const T (&alpha)[K],
+template <typename T, int K, class O>
+__device__ __forceinline__ void pipe_update(const O& o, int row, const T (&nn)[K], const T (&alpha)[K],
                                             const T (&beta)[K], bool b0, T* __restrict__ mnext, T (&d2)[2 * K]) {
-  const T mi = o(kQminv, 0);
+  const T mi = o.minv();
   T m[K];
 #pragma unroll
   for (int c = 0; c < K; ++c) {
@@ -360,13 +364,19 @@ __device__ __noinline__ void ssor_sweeps_global(const PipeSmem<K>* s, const LEnt
 // The CG forms of a launch: FORM selects the code compiled into a kernel
 // (each form keeps the registers of its own loop: one kernel holding all
 // three spilled more in every one of them).
-enum { kFormClassic = 0, kFormPipe = 1, kFormSingle = 2 };
+enum { kFormClassic = 0, kFormPipe = 1, kFormSingle = 2, kFormPipeSsor = 3 };
 __host__ __device__ constexpr int form_of(int pipe_mode) {
-  return pipe_mode == 3 ? kFormSingle : (pipe_mode == 1 || pipe_mode == 2) ? kFormPipe : kFormClassic;
+  return pipe_mode == 3                      ? kFormSingle
+         : (pipe_mode == 1 || pipe_mode == 2) ? kFormPipe
+         : (pipe_mode == 4 || pipe_mode == 5) ? kFormPipeSsor
+                                              : kFormClassic;
 }
 
 template <typename T, int K, int QR, int FORM, class Team>
 __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, unsigned char* dyn) {
+  // the pipelined form with block SSOR keeps u and q in the own-row records
+  constexpr bool PS = FORM == kFormPipeSsor;
+  using Own = OwnRef<T, K, PS ? 2 : 0>;
   // entries of a row gathered together (K values per neighbour in both forms)
   constexpr int UP = sizeof(T) == 4 ? 8 : 4;
   const T* Aval = (const T*)a.A_val;
@@ -436,7 +446,7 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
       // own-row state, plus for block SSOR the rows' colours and list
       // positions, the colours' neighbour lists and the sweep vector in
       // list order
-      size_t own = align16((size_t)(6 * K + 1) * Qb * B * sizeof(T));
+      size_t own = align16((size_t)Own::kLen * Qb * B * sizeof(T));
       int lents = 0, ncb = 0;
       if (bssor) {
         for (int c = 0; c < kMaxColours; ++c) {
@@ -471,7 +481,7 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
   // 16-byte-padded row per position (consecutive threads of a step touch
   // consecutive rows)
   const int nsl = Qb * B;
-  unsigned char* srowc = (unsigned char*)os + align16((size_t)(6 * K + 1) * nsl * sizeof(T));
+  unsigned char* srowc = (unsigned char*)os + align16((size_t)Own::kLen * nsl * sizeof(T));
   short* spos = (short*)(srowc + align16((size_t)nsl));
   const int lents = s->lents;
   short* const slist = (short*)((unsigned char*)spos + align16((size_t)nsl * sizeof(short)));  // position -> slot
@@ -483,8 +493,8 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
   T* const sv_g = bssor ? (T*)a.bss_v + (size_t)blk0 * MRow<T, K>::W : nullptr;
   T* pown = (T*)a.pown;
   auto own_ref = [&](int q, int row) {
-    OwnRef<T, K> o;
-    o.p = own_s ? os + ((size_t)q * B + t) * OwnRef<T, K>::kLen : pown + (size_t)row * OwnRef<T, K>::kLen;
+    Own o;
+    o.p = own_s ? os + ((size_t)q * B + t) * Own::kLen : pown + (size_t)row * Own::kLen;
     return o;
   };
   if (cached) {
@@ -504,7 +514,7 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
     const int row = row0 + q * R;
     if (row >= n) break;
     const double d = a.dinv64[row];
-    own_ref(q, row)(kQminv, 0) = (T)(d * d);  // dinv = 1 / sqrt(A_ii) (the pivots of the empty factor)
+    own_ref(q, row).minv() = (T)(d * d);  // dinv = 1 / sqrt(A_ii) (the pivots of the empty factor)
   }
   __syncthreads();
   auto row_ref = [&](int q, int row) {
@@ -541,7 +551,7 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
   // makes a row's z final (the top colour going up, the others going down)
   // also writes it to the row's record and to the gathered copy zn, and adds
   // the row's (r, z) and ||r||^2 to d2: no pass over the own rows afterwards.
-  auto ssor_fast_fin = [&](bool fin, T* zn, T* d2) {
+  auto ssor_fast_fin = [&](bool fin, auto rec, T* zn, T* d2) {
     const int nc = s->ncb;
     for (int pass = 0; pass < 2; ++pass) {
       const bool fwd = pass == 0;
@@ -572,13 +582,15 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
           store_m<T, K>(sv, beg + p, x);
           if (fin && (!fwd || c == nc - 1)) {
             const int slot = slist[beg + p];
-            T* o = os + (size_t)slot * OwnRef<T, K>::kLen;
+            if constexpr (decltype(rec)::value) {  // the two-reduction form: z's record and the dots too
+              T* o = os + (size_t)slot * Own::kLen;
 #pragma unroll
-            for (int cc = 0; cc < K; ++cc) {
-              const T r = o[kQr * K + cc];
-              o[kQz * K + cc] = x[cc];
-              d2[cc] += r * x[cc];
-              d2[K + cc] += r * r;
+              for (int cc = 0; cc < K; ++cc) {
+                const T r = o[kQr * K + cc];
+                o[kQz * K + cc] = x[cc];
+                d2[cc] += r * x[cc];
+                d2[K + cc] += r * r;
+              }
             }
             store_m<T, K>(zn, blk0 + slot, x);
           }
@@ -587,7 +599,7 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
       }
     }
   };
-  auto ssor_fast = [&]() { ssor_fast_fin(false, nullptr, nullptr); };
+  auto ssor_fast = [&]() { ssor_fast_fin(false, std::false_type{}, nullptr, nullptr); };
   // The tables in shared memory (beside the own state, when everything fits
   // there) or in the global scratch; the colours of the global case come
   // from a.bcolor, the list positions from a.bss_pos.
@@ -611,6 +623,24 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
   auto sv_load = [&](int slot, T (&x)[K]) {
     if (sm_ssor) load_m<T, K>(sv, spos[slot], x);
     else load_m<T, K>(sv_g, gpos[blk0 + slot], x);
+  };
+  // The pipelined form with block SSOR: the sweeps turn the D^-1 w the own
+  // rows left in the sweep vector into m = M^-1 w and write m to `out` for
+  // the neighbours (in the sweep step that makes a row's m final when the
+  // lists are in shared memory).
+  auto ps_sweeps = [&](T* out) {
+    if (sm_ssor && s->ncb >= 2) {
+      ssor_fast_fin(true, std::false_type{}, out, nullptr);
+      return;
+    }
+    ssor_apply();
+    for (int q = 0; q < Qb; ++q) {
+      const int row = row0 + q * R;
+      if (row >= n) break;
+      T m[K];
+      sv_load(q * B + t, m);
+      store_m<T, K>(out, row, m);
+    }
   };
   if (bssor) {
     if (sm_ssor)
@@ -649,7 +679,7 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
       LEnt<T>* const lbase = sm_ssor ? lent : lent_g;
       LEnt<T>* ll = lbase + s->loff[ci] + p;
       LEnt<T>* lu = lbase + s->uoff[ci] + p;
-      const T mi = own_ref(q, row)(kQminv, 0);
+      const T mi = own_ref(q, row).minv();
       const RowRef<T> rr = row_ref(q, row);
       int nl = 0, nu = 0;
       for (int e = 0; e < rr.len; ++e) {
@@ -669,7 +699,7 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
   // row slices q < QR: gathered together before the partial sums are needed
   bool okq[QR];
   RowRef<T> rrq[QR];
-  OwnRef<T, K> ownq[QR];
+  Own ownq[QR];
 #pragma unroll
   for (int q = 0; q < QR; ++q) {
     const int row = row0 + q * R;
@@ -770,8 +800,8 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
                               for (int c = 0; c < K; ++c) x[c] = a.x64[(size_t)j * K + c];
                             },
                             acc);
-        const OwnRef<T, K> o = own_ref(q, row);
-        const T mi = o(kQminv, 0);
+        const Own o = own_ref(q, row);
+        const T mi = o.minv();
         T u[2 * K];
 #pragma unroll
         for (int c = 0; c < K; ++c) {
@@ -806,7 +836,7 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
         for (int q = 0; q < Qb; ++q) {
           const int row = row0 + q * R;
           if (row >= n) break;
-          const OwnRef<T, K> o = own_ref(q, row);
+          const Own o = own_ref(q, row);
           T m[K];
           if (bssor) {
             sv_load(q * B + t, m);
@@ -815,6 +845,10 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
           } else {
 #pragma unroll
             for (int c = 0; c < K; ++c) m[c] = o(kQz, c);
+          }
+          if constexpr (PS) {  // u = M^-1 r starts the pipelined recurrences
+#pragma unroll
+            for (int c = 0; c < K; ++c) o(kQu, c) = m[c];
           }
           store_m<T, K>(mb0, row, m);
           store_m<T, K>(mb2, row, m);
@@ -828,8 +862,10 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
         // the pipelined form falls back to the classic one (for the rest of
         // the solve) when its last inner solve cut the FP64 residual of some
         // column by less than 10x
-        if (refine == 0) s->use_pipe = FORM == kFormPipe && (a.pipe_mode == 1 || a.pipe_mode == 2);
-        if (s->use_pipe && a.pipe_mode == 2 && refine > 0)
+        if (refine == 0)
+          s->use_pipe = (FORM == kFormPipe && (a.pipe_mode == 1 || a.pipe_mode == 2)) ||
+                        (PS && (a.pipe_mode == 4 || a.pipe_mode == 5));
+        if (s->use_pipe && (a.pipe_mode == 2 || a.pipe_mode == 4) && refine > 0)
           for (int c = 0; c < K; ++c)
             if (s->rrprev[c] > 0.0 && !(s->sm.sum[c] <= 1e-2 * s->rrprev[c])) s->use_pipe = 0;
         for (int c = 0; c < K; ++c) {
@@ -859,7 +895,7 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
     }
 
     bool pipe_failed = false;
-    if (FORM == kFormPipe && s->use_pipe) {
+    if ((FORM == kFormPipe || PS) && s->use_pipe) {
     // ---- phase I: w = A u, m = M^-1 w (to m1), gamma = (r, u), delta = (w, u)
     {
       T d2[2 * K];
@@ -870,18 +906,26 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
         if (row >= n) break;
         T acc[K];
         gather_m<T, K, UP>(row_ref(q, row), mb0, acc);
-        const OwnRef<T, K> o = own_ref(q, row);
-        const T mi = o(kQminv, 0);
+        const Own o = own_ref(q, row);
+        const T mi = o.minv();
         T m[K];
 #pragma unroll
         for (int c = 0; c < K; ++c) {
-          const T r = o(kQr, c), u = mi * r, w = acc[c];
+          const T r = o(kQr, c), w = acc[c];
+          T u;
+          if constexpr (PS) u = o(kQu, c);
+          else u = mi * r;
           o(kQw, c) = w;
           m[c] = mi * w;
           d2[c] += r * u;
           d2[K + c] += w * u;
         }
-        store_m<T, K>(mb1, row, m);
+        if constexpr (PS) sv_store(q * B + t, m);  // the block sweeps start from D^-1 w
+        else store_m<T, K>(mb1, row, m);
+      }
+      if constexpr (PS) {  // m = M^-1 w by the block sweeps, to m1 for the neighbours
+        __syncthreads();
+        ps_sweeps(mb1);
       }
       block_reduce_strided<2 * K, T>(d2, s->red2, pipe_ptr(0) + team.rank(), tsize);
       if (!team.sync()) { status = CN_TIMEOUT; goto done; }
@@ -966,7 +1010,7 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
       }
       __syncthreads();
       if (s->flag == 2) {
-        if (a.pipe_mode == 2) {  // drop this inner solve, continue in the classic form
+        if (a.pipe_mode == 2 || a.pipe_mode == 4) {  // drop this inner solve, continue in the classic form
           pipe_failed = true;
           break;
         }
@@ -984,15 +1028,66 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
       T d2[2 * K];
 #pragma unroll
       for (int c = 0; c < 2 * K; ++c) d2[c] = (T)0;
+      if constexpr (PS) {
+        // block SSOR: z = n + beta z, q = m + beta q, s = w + beta s,
+        // p = u + beta p, x += alpha p, r -= alpha s, u -= alpha q,
+        // w -= alpha z (m = M^-1 w of the last phase, still in the sweep
+        // vector); the sweeps then turn D^-1 w into the next m
+        auto ps_update = [&](const Own& o, int slot, const T (&nn)[K], T (&d)[2 * K]) {
+          const T mi = o.minv();
+          T mo[K], v[K];
+          sv_load(slot, mo);
 #pragma unroll
-      for (int q = 0; q < QR; ++q)
-        if (okq[q]) pipe_update<T, K>(ownq[q], row0 + q * R, nq[q], alpha, beta, b0, mnext, d2);
-      for (int q = QR; q < Qb; ++q) {
-        const int row = row0 + q * R;
-        if (row >= n) break;
-        T nn[K];
-        gather_m<T, K, UP>(row_ref(q, row), mcur, nn);
-        pipe_update<T, K>(own_ref(q, row), row, nn, alpha, beta, b0, mnext, d2);
+          for (int c = 0; c < K; ++c) {
+            const T r0 = o(kQr, c), w0 = o(kQw, c), u0 = o(kQu, c);
+            const T zo = b0 ? (T)0 : o(kQz, c);
+            const T qo = b0 ? (T)0 : o(kQq, c);
+            const T so = b0 ? (T)0 : o(kQs, c);
+            const T po = b0 ? (T)0 : o(kQp, c);
+            const T z = nn[c] + beta[c] * zo;
+            const T qv = mo[c] + beta[c] * qo;
+            const T sx = w0 + beta[c] * so;
+            const T p = u0 + beta[c] * po;
+            const T r = r0 - alpha[c] * sx;
+            const T u = u0 - alpha[c] * qv;
+            const T w = w0 - alpha[c] * z;
+            o(kQx, c) += alpha[c] * p;
+            o(kQz, c) = z;
+            o(kQq, c) = qv;
+            o(kQs, c) = sx;
+            o(kQp, c) = p;
+            o(kQr, c) = r;
+            o(kQu, c) = u;
+            o(kQw, c) = w;
+            v[c] = mi * w;
+            d[c] += r * u;
+            d[K + c] += w * u;
+          }
+          sv_store(slot, v);
+        };
+#pragma unroll
+        for (int q = 0; q < QR; ++q)
+          if (okq[q]) ps_update(ownq[q], q * B + t, nq[q], d2);
+        for (int q = QR; q < Qb; ++q) {
+          const int row = row0 + q * R;
+          if (row >= n) break;
+          T nn[K];
+          gather_m<T, K, UP>(row_ref(q, row), mcur, nn);
+          ps_update(own_ref(q, row), q * B + t, nn, d2);
+        }
+        __syncthreads();
+        ps_sweeps(mnext);
+      } else {
+#pragma unroll
+        for (int q = 0; q < QR; ++q)
+          if (okq[q]) pipe_update<T, K>(ownq[q], row0 + q * R, nq[q], alpha, beta, b0, mnext, d2);
+        for (int q = QR; q < Qb; ++q) {
+          const int row = row0 + q * R;
+          if (row >= n) break;
+          T nn[K];
+          gather_m<T, K, UP>(row_ref(q, row), mcur, nn);
+          pipe_update<T, K>(own_ref(q, row), row, nn, alpha, beta, b0, mnext, d2);
+        }
       }
       block_reduce_strided<2 * K, T>(d2, s->red2, pipe_ptr(g ^ 1) + team.rank(), tsize);
       ++total_iters;
@@ -1022,7 +1117,7 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
         const bool ok1[1] = {true};
         T acc1[1][K];
         gather_rows<T, K, UP, 1>(r1, ok1, mb2, acc1);
-        const OwnRef<T, K> o = own_ref(q, row);
+        const Own o = own_ref(q, row);
 #pragma unroll
         for (int c = 0; c < K; ++c) {
           const T r = o(kQr, c), z = o(kQz, c), w = acc1[0][c];
@@ -1102,8 +1197,8 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
         for (int q = 0; q < Qb; ++q) {
           const int row = row0 + q * R;
           if (row >= n) break;
-          const OwnRef<T, K> o = own_ref(q, row);
-          const T mi = o(kQminv, 0);
+          const Own o = own_ref(q, row);
+          const T mi = o.minv();
           T rec[K];
 #pragma unroll
           for (int c = 0; c < K; ++c) {
@@ -1130,14 +1225,14 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
         }
         if (bssor && sm_ssor && s->ncb >= 2) {  // the sweeps also write the records, zn and the dots
           __syncthreads();
-          ssor_fast_fin(true, zn, d3);
+          ssor_fast_fin(true, std::true_type{}, zn, d3);
         } else if (bssor) {
           __syncthreads();
           ssor_apply();
           for (int q = 0; q < Qb; ++q) {
             const int row = row0 + q * R;
             if (row >= n) break;
-            const OwnRef<T, K> o = own_ref(q, row);
+            const Own o = own_ref(q, row);
             T zf[K];
             sv_load(q * B + t, zf);
 #pragma unroll
@@ -1189,7 +1284,7 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
         // w = A z, (z, w)
         T accq[QR][K];
         gather_rows<T, K, UP, QR>(rrq, okq, zn, accq);
-        auto take_w = [&](const OwnRef<T, K>& o, const T (&acc)[K]) {
+        auto take_w = [&](const Own& o, const T (&acc)[K]) {
 #pragma unroll
           for (int c = 0; c < K; ++c) {
             o(kQw, c) = acc[c];
@@ -1291,7 +1386,7 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
         T d2[2 * K];
 #pragma unroll
         for (int c = 0; c < 2 * K; ++c) d2[c] = (T)0;
-        auto form_p = [&](const OwnRef<T, K>& o, const T (&acc)[K]) {
+        auto form_p = [&](const Own& o, const T (&acc)[K]) {
 #pragma unroll
           for (int c = 0; c < K; ++c) {
             const T z = o(kQz, c);
@@ -1353,8 +1448,8 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
         for (int q = 0; q < Qb; ++q) {
           const int row = row0 + q * R;
           if (row >= n) break;
-          const OwnRef<T, K> o = own_ref(q, row);
-          const T mi = o(kQminv, 0);
+          const Own o = own_ref(q, row);
+          const T mi = o.minv();
           T rec[K];
 #pragma unroll
           for (int c = 0; c < K; ++c) {
@@ -1377,14 +1472,14 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
         }
         if (bssor && sm_ssor && s->ncb >= 2) {  // the sweeps also write the records and the dots
           __syncthreads();
-          ssor_fast_fin(true, rnext, d2);
+          ssor_fast_fin(true, std::true_type{}, rnext, d2);
         } else if (bssor) {  // z = M^-1 r by the block sweeps, then the records and the dots
           __syncthreads();
           ssor_apply();
           for (int q = 0; q < Qb; ++q) {
             const int row = row0 + q * R;
             if (row >= n) break;
-            const OwnRef<T, K> o = own_ref(q, row);
+            const Own o = own_ref(q, row);
             T zf[K];
             if (bssor) sv_load(q * B + t, zf);
             T rec[K];
@@ -1415,7 +1510,7 @@ __device__ void pipe_body(const SolveArgs& a, const Team& team, PipeSmem<K>* s, 
     for (int q = 0; q < Qb; ++q) {
       const int row = row0 + q * R;
       if (row >= n) break;
-      const OwnRef<T, K> o = own_ref(q, row);
+      const Own o = own_ref(q, row);
 #pragma unroll
       for (int c = 0; c < K; ++c) a.x64[(size_t)row * K + c] += (double)o(kQx, c);
     }
@@ -1491,6 +1586,9 @@ cudaError_t launch_pk(const SolveArgs& a, int block, int grid, int qr, cudaStrea
   switch (form_of(a.pipe_mode)) {
     case kFormPipe: return launch_pkf<T, K, kFormPipe>(a, block, grid, qr, st);
     case kFormSingle: return launch_pkf<T, K, kFormSingle>(a, block, grid, qr, st);
+    case kFormPipeSsor:  // FP32 only (the host never asks for it in FP64)
+      if constexpr (sizeof(T) == 4) return launch_pkf<T, K, kFormPipeSsor>(a, block, grid, qr, st);
+      return cudaErrorInvalidValue;
     default: return launch_pkf<T, K, kFormClassic>(a, block, grid, qr, st);
   }
 }
@@ -1511,6 +1609,9 @@ int max_grid_pk(int block, int dyn, int qr, int pipe_mode) {
   switch (form_of(pipe_mode)) {
     case kFormPipe: return max_grid_pkf<T, K, kFormPipe>(block, dyn, qr);
     case kFormSingle: return max_grid_pkf<T, K, kFormSingle>(block, dyn, qr);
+    case kFormPipeSsor:
+      if constexpr (sizeof(T) == 4) return max_grid_pkf<T, K, kFormPipeSsor>(block, dyn, qr);
+      return 0;
     default: return max_grid_pkf<T, K, kFormClassic>(block, dyn, qr);
   }
 }
@@ -1640,7 +1741,7 @@ long long block_list_entries(const int* A_ptr, const int* A_col, const unsigned 
 }
 
 void pipelined_smem_need(const int* A_ptr, const int* A_col, int n, int grid, int block, int precision, int K,
-                         bool bssor, size_t* cache, size_t* full) {
+                         bool bssor, int rec_vectors, size_t* cache, size_t* full) {
   const size_t vs = precision == CN_PREC_MIXED ? sizeof(float) : sizeof(double);
   const long long Qg = ((long long)n + (long long)grid * block - 1) / ((long long)grid * block);
   const long long R = block;
@@ -1676,7 +1777,7 @@ void pipelined_smem_need(const int* A_ptr, const int* A_col, int n, int grid, in
       extra = align16((size_t)Qb * block) + 2 * align16((size_t)Qb * block * sizeof(short)) + align16(lents * 2 * vs) +
               (size_t)Qb * (size_t)block * wpad;
     }
-    wf = std::max(wf, c + align16((size_t)(6 * K + 1) * (size_t)Qb * (size_t)block * vs) + extra);
+    wf = std::max(wf, c + align16((size_t)(rec_vectors * K + 1) * (size_t)Qb * (size_t)block * vs) + extra);
   }
   *cache = wc;
   *full = wf;
