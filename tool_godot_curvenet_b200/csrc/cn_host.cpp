@@ -6,6 +6,8 @@
 #include <cmath>
 #include <cstring>
 #include <numeric>
+#include <map>
+#include <tuple>
 #include <vector>
 
 #include "cn_hsc.h"
@@ -66,8 +68,11 @@ struct cn_system {
   int* d_spmv_err = nullptr;     // raised by the staged SpMV if one of its bounded waits runs out (inside buf)
   int spmv_ents = -1;            // most entries of A in one SpMV tile (computed on first use)
   // pipelined solve: shared-memory needs of the last (grid, block, precision, k)
-  int pipe_grid = -1, pipe_block = -1, pipe_prec = -1, pipe_k = -1, pipe_rec = -1;
-  size_t pipe_cache = 0, pipe_full = 0;
+  // shared memory of the row-cached solve per launch shape (grid, block,
+  // precision, k, record vectors) -> (row cache, full state): the sizing
+  // colours the blocks on the host, so it is kept for every shape a handle
+  // has launched
+  std::map<std::tuple<int, int, int, int, int>, std::pair<size_t, size_t>> pipe_smem;
   int max_grid_alloc = 0;
   bool shape_set = false;   // cn_set_launch fixed the launch shape
   bool have_solution = false;
@@ -616,16 +621,18 @@ cn_status cn_solve_device(cn_handle S, int32_t k, const double* d_targets, doubl
         qr = block <= 512 ? 2 : 1;
         const size_t cap = 220 * 1024;
         for (int tries = 0; tries < 6; ++tries) {
-          if (S->pipe_grid != grid || S->pipe_block != block || S->pipe_prec != o.precision || S->pipe_k != k ||
-              S->pipe_rec != rec) {
+          const auto key = std::make_tuple(grid, block, (int)o.precision, k, rec);
+          auto it = S->pipe_smem.find(key);
+          if (it == S->pipe_smem.end()) {
+            size_t cache = 0, full = 0;
             cn::pipelined_smem_need(S->H.A_ptr.data(), S->H.A_col.data(), S->H.n, grid, block, o.precision, k, bssor,
-                                    rec, &S->pipe_cache, &S->pipe_full);
-            S->pipe_grid = grid; S->pipe_block = block; S->pipe_prec = o.precision; S->pipe_k = k;
-            S->pipe_rec = rec;
+                                    rec, &cache, &full);
+            it = S->pipe_smem.emplace(key, std::make_pair(cache, full)).first;
           }
-          if (level == 2 && S->pipe_full > cap) level = 1;
-          if (level == 1 && S->pipe_cache > cap) level = 0;
-          a.cache_bytes = level == 2 ? (int)S->pipe_full : level == 1 ? (int)S->pipe_cache : 0;
+          const size_t pipe_cache = it->second.first, pipe_full = it->second.second;
+          if (level == 2 && pipe_full > cap) level = 1;
+          if (level == 1 && pipe_cache > cap) level = 0;
+          a.cache_bytes = level == 2 ? (int)pipe_full : level == 1 ? (int)pipe_cache : 0;
           const int mg = cn::pipelined_max_grid(o.precision, k, block, a.cache_bytes, qr, a.pipe_mode);
           if (mg >= grid) break;
           if (mg <= 0) {
