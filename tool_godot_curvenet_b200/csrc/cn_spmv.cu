@@ -5,15 +5,21 @@
 // Two kernels, chosen by the width of a row of X:
 //
 // * k_spmm_vec (k a multiple of a 16-byte chunk: FP32 k = 24, FP64 k = 24):
-//   work item = one 16-byte chunk of one output row; the grid holds the
-//   blocks resident on the device at once and walks the items grid-stride
-//   (one wave).  Consecutive threads take consecutive chunks, so the store
-//   of Y and the gather of a neighbour row of X are contiguous across the
-//   threads of a row, and the row's column indices and values are the same
-//   addresses for those threads (one L1 transaction).  Four entries are in
-//   flight per thread (indices and values first, then the four gathers, then
-//   the multiply-adds): 32 registers, 2048 threads per SM, which keeps more
-//   loads outstanding than eight entries per thread at 40-48 registers did.
+//   work item = three 16-byte chunks of one output row (2 threads a row in
+//   FP32, 4 in FP64); the grid holds the blocks resident on the device at
+//   once and walks the items grid-stride (one wave).  The threads of a row
+//   take interleaved chunks (thread c: chunks c, c + T, c + 2T), so the store
+//   of Y and each gather of a neighbour row of X are contiguous across them,
+//   and the row's column indices and values are the same addresses for those
+//   threads.  Two entries at a time, their 2 x 3 gathers in flight together,
+//   60 registers (1,024 threads per SM; __launch_bounds__(256, 1) lets ptxas
+//   keep them: bounded for occupancy it chose 40 registers and the same
+//   kernel took 74 instead of 61 us).  Against one chunk per thread with
+//   four entries at a time (32 registers, 2,048 threads per SM) on the
+//   1.05M-row torus: FP32 69.6 -> 61.5 us, FP64 129 -> 109 us; fewer threads
+//   each with three independent gathers per entry keep more bytes in flight
+//   per load instruction, and each row's indices are loaded by a third as
+//   many threads.
 //
 // * k_spmm_staged (FP32 k = 1 and 3: rows of X of 4 or 12 bytes): one thread
 //   per row, tiles of kTileRows consecutive rows.  A producer warp per block
@@ -70,45 +76,59 @@ __device__ __forceinline__ void fma16(double2& acc, double a, const double2& x) 
 
 constexpr int kU = 4;
 
-// K a multiple of the chunk width: thread = (row, chunk) for the items
-// tid, tid + threads, ...; each item's loads are issued together: the row
-// pointers, then every entry's index and value, then every gather, then the
-// multiply-adds.
+constexpr int kVecChunks = 3;   // 16-byte chunks of a row per thread
+constexpr int kVecEntries = 2;  // entries of a row gathered together
+
+// K a multiple of kVecChunks chunks: thread = (row, chunk group) for the
+// items tid, tid + threads, ...; each item's loads are issued together: the
+// row pointers, then two entries' indices and values, then their gathers,
+// then the multiply-adds.
 template <typename T, int K>
-__global__ void __launch_bounds__(256) k_spmm_vec(int n, const int* __restrict__ ptr, const int* __restrict__ col,
+__global__ void __launch_bounds__(256, 1) k_spmm_vec(int n, const int* __restrict__ ptr, const int* __restrict__ col,
                                                   const T* __restrict__ val, const T* __restrict__ x,
                                                   T* __restrict__ y) {
   using V = typename V16<T>::type;
   constexpr int C = K / V16<T>::W;  // chunks per row
-  const long long items = (long long)n * C;
+  constexpr int CW = kVecChunks, U = kVecEntries;
+  static_assert(C % CW == 0, "a row's chunks split evenly over its threads");
+  constexpr int CT = C / CW;  // threads per row
+  const long long items = (long long)n * CT;
   const V* __restrict__ xv = reinterpret_cast<const V*>(x);
   for (long long it = (long long)blockIdx.x * blockDim.x + threadIdx.x; it < items;
        it += (long long)gridDim.x * blockDim.x) {
-    const int row = (int)(it / C), ch = (int)(it - (long long)row * C);
+    const int row = (int)(it / CT), tc = (int)(it - (long long)row * CT);
     const int e0 = __ldg(ptr + row), e1 = __ldg(ptr + row + 1);
-    V acc;
-    if constexpr (sizeof(T) == 4) acc = make_float4(0.f, 0.f, 0.f, 0.f);
-    else acc = make_double2(0.0, 0.0);
-    for (int e = e0; e < e1; e += kU) {
-      int j[kU];
-      T a[kU];
+    V acc[CW];
 #pragma unroll
-      for (int u = 0; u < kU; ++u) {
+    for (int w = 0; w < CW; ++w) {
+      if constexpr (sizeof(T) == 4) acc[w] = make_float4(0.f, 0.f, 0.f, 0.f);
+      else acc[w] = make_double2(0.0, 0.0);
+    }
+    for (int e = e0; e < e1; e += U) {
+      int j[U];
+      T a[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
         const bool g = e + u < e1;
         j[u] = g ? __ldg(col + e + u) : -1;
         a[u] = g ? __ldg(val + e + u) : (T)0;
       }
-      V xs[kU];
+      V xs[U][CW];
 #pragma unroll
-      for (int u = 0; u < kU; ++u) {
-        if (j[u] >= 0) xs[u] = __ldg(xv + (size_t)j[u] * C + ch);
-        else if constexpr (sizeof(T) == 4) xs[u] = make_float4(0.f, 0.f, 0.f, 0.f);
-        else xs[u] = make_double2(0.0, 0.0);
-      }
+      for (int u = 0; u < U; ++u)
 #pragma unroll
-      for (int u = 0; u < kU; ++u) fma16(acc, a[u], xs[u]);
+        for (int w = 0; w < CW; ++w) {
+          if (j[u] >= 0) xs[u][w] = __ldg(xv + (size_t)j[u] * C + tc + w * CT);
+          else if constexpr (sizeof(T) == 4) xs[u][w] = make_float4(0.f, 0.f, 0.f, 0.f);
+          else xs[u][w] = make_double2(0.0, 0.0);
+        }
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+#pragma unroll
+        for (int w = 0; w < CW; ++w) fma16(acc[w], a[u], xs[u][w]);
     }
-    reinterpret_cast<V*>(y)[(size_t)row * C + ch] = acc;
+#pragma unroll
+    for (int w = 0; w < CW; ++w) reinterpret_cast<V*>(y)[(size_t)row * C + tc + w * CT] = acc[w];
   }
 }
 
@@ -331,8 +351,8 @@ cudaError_t launch_staged(int n, const int* ptr, const int* col, const float* va
 template <typename T, int K>
 cudaError_t launch_k(int n, const int* ptr, const int* col, const T* val, const T* x, T* y, cudaStream_t s) {
   if (n <= 0) return cudaSuccess;
-  if constexpr (K % V16<T>::W == 0) {
-    const long long items = (long long)n * (K / V16<T>::W);
+  if constexpr (K % (V16<T>::W * kVecChunks) == 0) {
+    const long long items = (long long)n * (K / V16<T>::W / kVecChunks);
     static const int slots = resident_blocks(k_spmm_vec<T, K>, 256, 0);
     const long long nb = std::min<long long>((items + 255) / 256, slots);
     k_spmm_vec<T, K><<<(unsigned)nb, 256, 0, s>>>(n, ptr, col, val, x, y);
