@@ -116,15 +116,18 @@ def test_c2_jacobi_variants_match_oracle(precision, algo):
 
 
 def test_c2_ic0_matches_oracle():
+    """IC(0): mixed precision through the default call (the sweeps without
+    grid barriers) and the level-scheduled kernel (classic), FP64."""
     pos, tris, h, t = workload("c2")
     xo = oracle_solution("c2")
     with CutMeshSolver(pos, tris, h, precond="ic0") as s:
-        r = s.solve(t, mode="deform", precision="mixed", tol=1e-8)
-        _check(r, 1e-8)
-        assert rel_err(r.x, xo) <= STOP_TOL
-        r = s.solve(t, mode="deform", precision="mixed", tol=1e-11, max_refine=30)
-        _check(r, 1e-11)
-        assert rel_err(r.x, xo) <= TIGHT_TOL
+        for algo in ("fused", "classic"):
+            r = s.solve(t, mode="deform", precision="mixed", tol=1e-8, algo=algo)
+            _check(r, 1e-8)
+            assert rel_err(r.x, xo) <= STOP_TOL
+            r = s.solve(t, mode="deform", precision="mixed", tol=1e-11, max_refine=30, algo=algo)
+            _check(r, 1e-11)
+            assert rel_err(r.x, xo) <= TIGHT_TOL
         r = s.solve(t, mode="deform", precision="fp64", tol=1e-13, max_iter=20000)
         _check(r, 1e-13)
         assert rel_err(r.x, xo) <= FP64_TOL

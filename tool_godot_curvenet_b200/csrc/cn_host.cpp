@@ -76,6 +76,12 @@ struct cn_system {
   int max_grid_alloc = 0;
   bool shape_set = false;   // cn_set_launch fixed the launch shape
   bool have_solution = false;
+  // IC(0) sweeps without grid barriers: per-level ELL tables of L, U and A
+  // (own allocations, built at the first such solve)
+  bool icsf_ready = false;
+  std::vector<void*> icsf_mem;
+  int *d_ell_tab = nullptr, *d_ell_cL = nullptr, *d_ell_cU = nullptr, *d_ell_cA = nullptr;
+  float *d_ell_vL = nullptr, *d_ell_vU = nullptr, *d_ell_vA = nullptr;
   // HSC preconditioner tables (own allocations)
   bool hsc = false;
   int hsc_L = 0, hsc_tail = 0, hsc_nc = 0;
@@ -108,6 +114,13 @@ namespace {
 // Jacobi and block SSOR run on the row-cached kernel
 bool row_cached(const cn_system* S) {
   return !S->hsc && (S->opts.precond == CN_PRECOND_JACOBI || S->opts.precond == CN_PRECOND_BSSOR);
+}
+
+// IC(0) in mixed precision on a multi-block grid runs the sweeps without
+// grid barriers (cn_icsf.cu); CLASSIC keeps the level-scheduled kernel
+bool icsf_path(const cn_system* S, const cn_solve_opts& o) {
+  return !S->hsc && S->opts.precond == CN_PRECOND_IC0 && o.precision == CN_PREC_MIXED && S->grid > 1 &&
+         o.algo != CN_ALGO_CLASSIC && o.algo != CN_ALGO_PLAIN && S->H.nlev <= cn::icsf_max_levels();
 }
 
 const char* kStatusText[] = {"ok", "max_iter", "singular_component", "nonpositive_pivot",
@@ -154,6 +167,10 @@ void choose_launch(cn_system* S) {
   }
 }
 
+// Host -> device uploads go on the handle's stream: the stream is
+// non-blocking, and a synchronous cudaMemcpy from pageable memory may return
+// before its DMA lands, so a kernel on the handle's stream could otherwise
+// read the destination before it holds the data.
 template <class Tp>
 cn_status up_new(cn_system* S, Tp** dst, const std::vector<Tp>& h) {
   const size_t bytes = sizeof(Tp) * std::max<size_t>(h.size(), 1);
@@ -162,7 +179,23 @@ cn_status up_new(cn_system* S, Tp** dst, const std::vector<Tp>& h) {
     return CN_CUDA_ERROR;
   }
   S->hsc_mem.push_back(*dst);
-  if (!h.empty() && cudaMemcpy(*dst, h.data(), sizeof(Tp) * h.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+  if (!h.empty() && cudaMemcpyAsync(*dst, h.data(), sizeof(Tp) * h.size(), cudaMemcpyHostToDevice, S->stream) != cudaSuccess) {
+    set_err("upload failed");
+    return CN_CUDA_ERROR;
+  }
+  return CN_OK;
+}
+
+// Upload h into a new device allocation recorded in `mem` (freed with the handle).
+template <class Tp>
+cn_status up_new_list(std::vector<void*>& mem, cudaStream_t stream, Tp** dst, const std::vector<Tp>& h) {
+  const size_t bytes = sizeof(Tp) * std::max<size_t>(h.size(), 1);
+  if (cudaMalloc((void**)dst, bytes) != cudaSuccess) {
+    set_err("device allocation of %zu bytes failed", bytes);
+    return CN_CUDA_ERROR;
+  }
+  mem.push_back(*dst);
+  if (!h.empty() && cudaMemcpyAsync(*dst, h.data(), sizeof(Tp) * h.size(), cudaMemcpyHostToDevice, stream) != cudaSuccess) {
     set_err("upload failed");
     return CN_CUDA_ERROR;
   }
@@ -170,6 +203,74 @@ cn_status up_new(cn_system* S, Tp** dst, const std::vector<Tp>& h) {
 }
 
 std::vector<float> to_f32(const std::vector<double>& v) { return std::vector<float>(v.begin(), v.end()); }
+
+// Per-level ELL tables of L, U and A for the IC(0) solve without grid
+// barriers: for level l (rows lo..hi, m = hi - lo) and matrix X, entry e of
+// the row at position rho at off_X(l) + e * m + rho, width w_X(l) = the
+// longest row of X in the level; columns -1 pad.  The values are gathered on
+// the device from the handle's FP32 L, U and A.
+cn_status setup_icsf(cn_system* S) {
+  const MeshHost& H = S->H;
+  const int nl = H.nlev;
+  std::vector<int> tab((size_t)6 * std::max(nl, 1), 0);
+  long long tot[3] = {0, 0, 0};
+  const std::vector<int>* ptr[3] = {&H.L_ptr, &H.U_ptr, &H.A_ptr};
+  const std::vector<int>* col[3] = {&H.L_col, &H.U_col, &H.A_col};
+  for (int l = 0; l < nl; ++l) {
+    const int lo = H.lev_ptr[l], hi = H.lev_ptr[l + 1];
+    for (int x = 0; x < 3; ++x) {
+      int w = 0;
+      for (int i = lo; i < hi; ++i) w = std::max(w, (*ptr[x])[i + 1] - (*ptr[x])[i]);
+      tab[6 * l + 2 * x] = (int)tot[x];
+      tab[6 * l + 2 * x + 1] = w;
+      tot[x] += (long long)(hi - lo) * w;
+    }
+  }
+  for (int x = 0; x < 3; ++x)
+    if (tot[x] >= (1LL << 31)) {
+      set_err("IC(0) level tables exceed 2^31 entries");
+      return CN_BAD_INPUT;
+    }
+  const float* src[3] = {S->D.L32, S->D.U32, S->D.A32};
+  int* dc[3] = {};
+  float* dv[3] = {};
+  for (int x = 0; x < 3; ++x) {
+    std::vector<int> c((size_t)std::max<long long>(tot[x], 1), -1), e((size_t)std::max<long long>(tot[x], 1), -1);
+    for (int l = 0; l < nl; ++l) {
+      const int lo = H.lev_ptr[l], hi = H.lev_ptr[l + 1], m = hi - lo, off = tab[6 * l + 2 * x];
+      for (int i = lo; i < hi; ++i)
+        for (int k = (*ptr[x])[i]; k < (*ptr[x])[i + 1]; ++k) {
+          const size_t at = (size_t)off + (size_t)(k - (*ptr[x])[i]) * m + (i - lo);
+          c[at] = (*col[x])[k];
+          e[at] = k;
+        }
+    }
+    cn_status st = up_new_list(S->icsf_mem, S->stream, &dc[x], c);
+    if (st != CN_OK) return st;
+    int* d_e = nullptr;
+    if (cudaMalloc((void**)&d_e, sizeof(int) * e.size()) != cudaSuccess ||
+        cudaMalloc((void**)&dv[x], sizeof(float) * e.size()) != cudaSuccess) {
+      if (d_e) cudaFree(d_e);
+      set_err("device allocation of the IC(0) level tables failed");
+      return CN_CUDA_ERROR;
+    }
+    S->icsf_mem.push_back(dv[x]);
+    const bool ok = cudaMemcpyAsync(d_e, e.data(), sizeof(int) * e.size(), cudaMemcpyHostToDevice, S->stream) == cudaSuccess &&
+                    cn::launch_ell_values(d_e, src[x], dv[x], (long long)e.size(), S->stream) == cudaSuccess &&
+                    cudaStreamSynchronize(S->stream) == cudaSuccess;
+    cudaFree(d_e);
+    if (!ok) {
+      set_err("building the IC(0) level tables failed");
+      return CN_CUDA_ERROR;
+    }
+  }
+  cn_status st = up_new_list(S->icsf_mem, S->stream, &S->d_ell_tab, tab);
+  if (st != CN_OK) return st;
+  S->d_ell_cL = dc[0]; S->d_ell_cU = dc[1]; S->d_ell_cA = dc[2];
+  S->d_ell_vL = dv[0]; S->d_ell_vU = dv[1]; S->d_ell_vA = dv[2];
+  S->icsf_ready = true;
+  return CN_OK;
+}
 
 // HSC: read A back, build the hierarchy on the host, move the rows into HSC
 // order, reassemble A in that order and upload the level tables.
@@ -425,6 +526,7 @@ void cn_destroy(cn_handle S) {
   if (S->stream) cudaStreamSynchronize(S->stream);
   if (S->buf) cudaFree(S->buf);
   for (void* p : S->hsc_mem) cudaFree(p);
+  for (void* p : S->icsf_mem) cudaFree(p);
   for (void* p : S->cnet_mem) cudaFree(p);
   for (void* p : {(void*)S->cnet.seg, (void*)S->cnet.ends, (void*)S->d_cnet_posed, (void*)S->d_cnet_F,
                   (void*)S->d_cnet_X})
@@ -496,8 +598,10 @@ cn_status cn_solve_device(cn_handle S, int32_t k, const double* d_targets, doubl
   }
   // The row-cached Jacobi kernel runs k = 9 as three k = 3 solves on column
   // slices: its k = 9 state fits neither shared memory nor registers, and
-  // three k = 3 solves take a third of the time of one k = 9 solve.
-  if (k == 9 && row_cached(S) && o.algo != CN_ALGO_PLAIN && S->d_split_t &&
+  // three k = 3 solves take a third of the time of one k = 9 solve.  The
+  // IC(0) solve without grid barriers does the same (its gathers keep the
+  // words of six neighbour rows in registers).
+  if (k == 9 && (row_cached(S) || icsf_path(S, o)) && o.algo != CN_ALGO_PLAIN && S->d_split_t &&
       o.tol > 0.0 && o.max_iter >= 0 && o.max_refine >= 1) {
     CN_CUDA(cudaSetDevice(S->device));
     const int rows_t = o.mode == CN_MODE_RHS ? S->H.n : S->H.nh;
@@ -573,8 +677,9 @@ cn_status cn_solve_device(cn_handle S, int32_t k, const double* d_targets, doubl
     set_err("the pipelined form needs the Jacobi preconditioner, or block SSOR in mixed precision");
     return CN_BAD_INPUT;
   }
-  if (o.algo == CN_ALGO_SINGLE && !row_cached(S)) {
-    set_err("the single-reduction form runs on Jacobi and block SSOR handles");
+  if (o.algo == CN_ALGO_SINGLE && !row_cached(S) &&
+      !(S->opts.precond == CN_PRECOND_IC0 && !S->hsc && mixed)) {
+    set_err("the single-reduction form runs on Jacobi and block SSOR handles, and on IC(0) handles in mixed precision");
     return CN_BAD_INPUT;
   }
   if (row_cached(S)) {
@@ -663,7 +768,7 @@ cn_status cn_solve_device(cn_handle S, int32_t k, const double* d_targets, doubl
         S->h_bcolor.assign((size_t)std::max(n, 1), 0);
         S->bncolor = cn::block_colours(S->H.A_ptr.data(), S->H.A_col.data(), n, std::max(rb, 1), S->h_bcolor.data());
         if (!S->d_bcolor) CN_CUDA(cudaMalloc((void**)&S->d_bcolor, (size_t)std::max(n, 1)));
-        if (n) CN_CUDA(cudaMemcpy(S->d_bcolor, S->h_bcolor.data(), (size_t)n, cudaMemcpyHostToDevice));
+        if (n) CN_CUDA(cudaMemcpyAsync(S->d_bcolor, S->h_bcolor.data(), (size_t)n, cudaMemcpyHostToDevice, S->stream));
         S->bcolor_rb = rb;
       }
       a.bcolor = S->d_bcolor;
@@ -696,7 +801,7 @@ cn_status cn_solve_device(cn_handle S, int32_t k, const double* d_targets, doubl
           CN_CUDA(cudaMalloc((void**)&S->d_bss_loff, sizeof(long long) * (size_t)(nb + 1)));
           S->bss_loff_cap = nb + 1;
         }
-        CN_CUDA(cudaMemcpy(S->d_bss_loff, off.data(), sizeof(long long) * (size_t)(nb + 1), cudaMemcpyHostToDevice));
+        CN_CUDA(cudaMemcpyAsync(S->d_bss_loff, off.data(), sizeof(long long) * (size_t)(nb + 1), cudaMemcpyHostToDevice, S->stream));
         S->bss_rb = rb;
         S->bss_grid = nb;
       }
@@ -716,6 +821,35 @@ cn_status cn_solve_device(cn_handle S, int32_t k, const double* d_targets, doubl
     return fill_stats(S, k, stats);
   }
   int grid = S->grid;
+  // IC(0) in mixed precision on a multi-block grid: the sweeps without grid
+  // barriers (tagged words) under the single-reduction CG; CLASSIC keeps the
+  // level-scheduled kernel
+  if (icsf_path(S, o)) {
+    if (!S->icsf_ready) {
+      const cn_status st = setup_icsf(S);
+      if (st != CN_OK) return st;
+    }
+    a.ell_tab = S->d_ell_tab;
+    a.ell_cL = S->d_ell_cL; a.ell_vL = S->d_ell_vL;
+    a.ell_cU = S->d_ell_cU; a.ell_vU = S->d_ell_vU;
+    a.ell_cA = S->d_ell_cA; a.ell_vA = S->d_ell_vA;
+    const int block = std::min(S->block, 384);
+    const int mg = cn::icsf_max_grid(k, block);
+    if (mg <= 0) {
+      set_err("the IC(0) solve does not fit on this device (block %d)", block);
+      return CN_CUDA_ERROR;
+    }
+    grid = std::min(std::min(grid, mg), S->max_grid_alloc);
+    a.m0 = S->d_m[0];
+    a.m1 = S->d_m[1];
+    CN_CUDA(cudaMemsetAsync(S->d_ctl, 0, sizeof(Control), S->stream));
+    CN_CUDA(cudaEventRecord(S->ev0, S->stream));
+    CN_CUDA(cn::launch_icsf_solve(a, k, block, grid, S->stream));
+    CN_CUDA(cudaEventRecord(S->ev1, S->stream));
+    S->have_solution = true;
+    if (!stats) return CN_OK;
+    return fill_stats(S, k, stats);
+  }
   if (grid > 1) {
     const int mg = cn::persistent_max_grid(o.precision, k, S->lanes, S->block);
     if (mg <= 0) {
@@ -924,11 +1058,11 @@ cn_status cn_bind_curves(cn_handle S, int32_t n_curves, int32_t n_segments, cons
   CN_CUDA(cudaMalloc((void**)&S->d_dP, sizeof(double) * ncp));
   CN_CUDA(cudaMalloc((void**)&S->d_dw, sizeof(double) * n_curves));
   if (H.nh) {
-    CN_CUDA(cudaMemcpy(S->d_curve_of, curve_of, sizeof(int) * H.nh, cudaMemcpyHostToDevice));
-    CN_CUDA(cudaMemcpy(S->d_tau, tau, sizeof(double) * H.nh, cudaMemcpyHostToDevice));
+    CN_CUDA(cudaMemcpyAsync(S->d_curve_of, curve_of, sizeof(int) * H.nh, cudaMemcpyHostToDevice, S->stream));
+    CN_CUDA(cudaMemcpyAsync(S->d_tau, tau, sizeof(double) * H.nh, cudaMemcpyHostToDevice, S->stream));
   }
-  CN_CUDA(cudaMemcpy(S->d_row_of, row_of.data(), sizeof(int) * H.nv, cudaMemcpyHostToDevice));
-  CN_CUDA(cudaMemcpy(S->d_rest_cp, rest_cp, sizeof(double) * ncp, cudaMemcpyHostToDevice));
+  CN_CUDA(cudaMemcpyAsync(S->d_row_of, row_of.data(), sizeof(int) * H.nv, cudaMemcpyHostToDevice, S->stream));
+  CN_CUDA(cudaMemcpyAsync(S->d_rest_cp, rest_cp, sizeof(double) * ncp, cudaMemcpyHostToDevice, S->stream));
   return CN_OK;
 }
 
@@ -1021,11 +1155,11 @@ static cn_status ensure_deform_tables(cn_handle S) {
   CN_CUDA(cudaMalloc((void**)&S->d_vf_corner, sizeof(int) * std::max<size_t>(H.vf_corner.size(), 1)));
   CN_CUDA(cudaMalloc((void**)&S->d_contrib, sizeof(double) * 9 * std::max(H.nt, 1)));
   CN_CUDA(cudaMalloc((void**)&S->d_Xc, sizeof(double) * 3 * std::max(H.nh, 1)));
-  CN_CUDA(cudaMemcpy(S->d_vf_ptr, H.vf_ptr.data(), sizeof(int) * H.vf_ptr.size(), cudaMemcpyHostToDevice));
+  CN_CUDA(cudaMemcpyAsync(S->d_vf_ptr, H.vf_ptr.data(), sizeof(int) * H.vf_ptr.size(), cudaMemcpyHostToDevice, S->stream));
   if (!H.vf_face.empty()) {
-    CN_CUDA(cudaMemcpy(S->d_vf_face, H.vf_face.data(), sizeof(int) * H.vf_face.size(), cudaMemcpyHostToDevice));
-    CN_CUDA(cudaMemcpy(S->d_vf_corner, H.vf_corner.data(), sizeof(int) * H.vf_corner.size(),
-                       cudaMemcpyHostToDevice));
+    CN_CUDA(cudaMemcpyAsync(S->d_vf_face, H.vf_face.data(), sizeof(int) * H.vf_face.size(), cudaMemcpyHostToDevice, S->stream));
+    CN_CUDA(cudaMemcpyAsync(S->d_vf_corner, H.vf_corner.data(), sizeof(int) * H.vf_corner.size(),
+                            cudaMemcpyHostToDevice, S->stream));
   }
   return CN_OK;
 }
@@ -1103,7 +1237,7 @@ static cn_status cnet_upload_bytes(cn_system* S, void** dst, const void* h, size
   void* d = nullptr;
   CN_CUDA(cudaMalloc(&d, std::max<size_t>(bytes, 8)));
   S->cnet_mem.push_back(d);
-  if (bytes) CN_CUDA(cudaMemcpy(d, h, bytes, cudaMemcpyHostToDevice));
+  if (bytes) CN_CUDA(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, S->stream));
   *dst = d;
   return CN_OK;
 }

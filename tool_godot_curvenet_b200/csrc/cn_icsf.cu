@@ -1,0 +1,701 @@
+// cn_icsf.cu -- IC(0)-preconditioned CG with synchronisation-free triangular
+// sweeps (sm_100a): the mixed-precision solve of an IC(0) handle.
+//
+// Same problem, right-hand sides, FP64 residual refinement and output as the
+// level-scheduled persistent solve (cn_pcg.cu), and the same preconditioner:
+// M = L~ L~^T with the handle's IC(0) factor (IncompleteCholesky.lean:30-101),
+// applied as a forward sweep y = L~^-1 r and a backward sweep u = L~^-T y
+// over the levels of the factor's lower-triangular graph.
+//
+// The level-scheduled kernel separates the levels by grid barriers (2 x
+// levels per iteration).  Here no barrier separates them: every value a
+// sweep publishes is stored together with the number of the preconditioner
+// application it belongs to, one 64-bit word per column (the FP32 bits in
+// the low half, the application number in the high half), and a row's
+// thread reads its neighbours' words until every one carries the current
+// number.  A naturally aligned 64-bit access is single-copy atomic, so a word
+// with the current number holds the current value; no fence or flag orders
+// the value and its number.  Each thread walks its own rows level by level
+// (ascending in the forward sweep, descending in the backward one), and a
+// row only waits for rows of lower (higher) levels, so by induction over the
+// levels every wait ends (the launch is cooperative: all blocks co-resident).
+//
+// The CG is the single-reduction form of Chronopoulos & Gear ("s-step
+// iterative methods for symmetric linear systems", J. Comput. Appl. Math.
+// 25, 1989):
+//
+//   u = M^-1 r ; w = A u                       (sweeps and product, no barrier)
+//   gamma = (r, u), delta = (w, u), ||r||^2    one reduction -> ONE grid barrier
+//   beta = gamma / gamma' ; alpha = gamma / (delta - beta gamma / alpha')
+//   p = u + beta p ; s = w + beta s ; x += alpha p ; r -= alpha s
+//
+// and the update of a row is done by its thread in the forward sweep, just
+// before the row's y, so an iteration is: the forward sweep (with the
+// update), the backward sweep, the product w = A u, the partial sums, one grid
+// barrier.  A word of application a is overwritten only in application a + 1,
+// which starts after a grid barrier that every reader of application a has
+// passed, so no reader sees a value replaced too early.
+//
+// Ownership: the rows of level l are cut into one chunk of ceil(size / grid)
+// consecutive rows per block; inside block b's chunk, position q goes to
+// thread (q + o_l) mod blockDim, o_l the sum of the lower levels' chunk sizes
+// (consecutive levels start on different warps, so a warp whose rows wait
+// does not hold back the next level's rows).  Rows of a level are in vertex
+// order, so block b's chunks of all levels cover about the same part of the
+// mesh and most of a row's neighbours are rows of the same block.
+//
+// Every wait is bounded: it reads the global timer at its first poll and every
+// 64th and the shared abort flag every 64th; a wait that runs out raises the
+// abort flag, the others leave at their next check, and the solve ends with
+// CN_TIMEOUT at the next block-uniform check.
+#include <algorithm>
+
+#include "cn_pcg_body.cuh"
+
+namespace cn {
+namespace {
+
+using namespace pcg;
+
+constexpr int kIcsfMaxLev = 256;
+
+// Words of a row: K columns padded to an even count (whole 16-byte pairs).
+template <int K>
+struct TRow {
+  static constexpr int W = (K + 1) & ~1;
+};
+
+__device__ __forceinline__ unsigned long long tag_word(float v, unsigned app) {
+  return ((unsigned long long)app << 32) | (unsigned long long)__float_as_uint(v);
+}
+
+__device__ __forceinline__ void ld_pair(const unsigned long long* p, unsigned long long& a, unsigned long long& b) {
+  asm volatile("ld.relaxed.gpu.global.v2.u64 {%0, %1}, [%2];" : "=l"(a), "=l"(b) : "l"(p));
+}
+
+__device__ __forceinline__ void ld_one(const unsigned long long* p, unsigned long long& a) {
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(a) : "l"(p));
+}
+
+__device__ __forceinline__ void st_pair(unsigned long long* p, unsigned long long a, unsigned long long b) {
+  asm volatile("st.relaxed.gpu.global.v2.u64 [%0], {%1, %2};" ::"l"(p), "l"(a), "l"(b) : "memory");
+}
+
+template <int K>
+__device__ __forceinline__ void publish(unsigned long long* words, int row, const float (&v)[K], unsigned app) {
+  constexpr int W = TRow<K>::W;
+  unsigned long long* p = words + (size_t)row * W;
+#pragma unroll
+  for (int i = 0; i < W / 2; ++i) {
+    const unsigned long long a = tag_word(2 * i < K ? v[2 * i] : 0.f, app);
+    const unsigned long long b = tag_word(2 * i + 1 < K ? v[2 * i + 1] : 0.f, app);
+    st_pair(p + 2 * i, a, b);
+  }
+}
+
+// The bounded wait of one thread in one phase.
+struct Spin {
+  Control* ctl;
+  long long limit_ns;
+  unsigned long long t0;
+  unsigned n;
+  bool dead;
+  // false: stop waiting (limit reached, or another wait raised the abort flag)
+  __device__ __forceinline__ bool poll() {
+    if (dead) return false;
+    const unsigned k = n++;
+    if (k == 0) {
+      t0 = global_ns();
+    } else if ((k & 63u) == 63u) {
+      if (*(volatile int*)&ctl->abort) {
+        dead = true;
+        return false;
+      }
+      if ((long long)(global_ns() - t0) > limit_ns) {
+        atomicExch(&ctl->abort, 1);
+        dead = true;
+        return false;
+      }
+    }
+    return true;
+  }
+};
+
+// The K words of a row (pairs, then the last one alone when K is odd).
+template <int K>
+__device__ __forceinline__ void load_row_words(const unsigned long long* p, unsigned long long (&x)[K]) {
+#pragma unroll
+  for (int i = 0; i + 1 < K; i += 2) ld_pair(p + i, x[i], x[i + 1]);
+  if (K & 1) ld_one(p + K - 1, x[K - 1]);
+}
+
+template <int K>
+__device__ __forceinline__ bool row_ready(const unsigned long long (&x)[K], unsigned app) {
+  bool ok = true;
+#pragma unroll
+  for (int c = 0; c < K; ++c) ok = ok && (unsigned)(x[c] >> 32) == app;
+  return ok;
+}
+
+// Reads the row's words again until every one carries `app` (or the wait
+// gives up).
+template <int K>
+__device__ __forceinline__ void wait_row(const unsigned long long* p, unsigned long long (&x)[K], unsigned app,
+                                         Spin& sp) {
+  while (!row_ready<K>(x, app) && sp.poll()) load_row_words<K>(p, x);
+}
+
+// Rows of level l owned by this thread: block b's chunk of the level,
+// positions q = (t - o) mod B, q + B, ... below the chunk's row count.
+struct LevelRows {
+  int base, cnt, q0;
+};
+
+__device__ __forceinline__ LevelRows level_rows(const int* lev, const int* loff, int l) {
+  const int lo = lev[l], hi = lev[l + 1];
+  const int G = gridDim.x, B = blockDim.x;
+  const int cs = (hi - lo + G - 1) / G;
+  LevelRows r;
+  r.base = lo + blockIdx.x * cs;
+  r.cnt = min(cs, hi - r.base);
+  int q0 = ((int)threadIdx.x - loff[l] % B) % B;
+  if (q0 < 0) q0 += B;
+  r.q0 = q0;
+  return r;
+}
+
+template <int K>
+struct IcsfSmem {
+  double red[kMaxWarps * 3 * K];
+  double sum[3 * K];
+  double bb[K], stop[K], gprev[K], aprev[K], alpha[K], beta[K];
+  int active[K];
+  int flag;
+  int abort;
+  int lev[kIcsfMaxLev + 1];
+  int loff[kIcsfMaxLev];  // ownership offset of each level: chunk sizes of the lower levels
+  int tab[6 * kIcsfMaxLev];  // per level: first entry and width of the L, U and A tables
+};
+
+// The first kPre entries of a row's ELL table (column -1: none), copied by
+// the thread into its slots of a shared-memory buffer with cp.async (no
+// registers held while the copy is in flight): slot u of thread t at u * B + t
+// (columns), then the values.  A row of level l is at position rho = row -
+// first row of the level, its entry e at tab_off + e * level_size + rho
+// (consecutive rows of a level are consecutive words: a warp's loads
+// coalesce).  Two buffers: the rows of the current level and those of the
+// next one, prefetched while the current level runs.
+constexpr int kPre = 12;   // entries per row copied ahead
+constexpr int kChunk = 6;  // entries whose words are in flight together
+
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+struct EllBuf {
+  int* c;    // kPre x blockDim.x
+  float* v;  // kPre x blockDim.x
+};
+
+__device__ __forceinline__ EllBuf ell_buf(unsigned char* dyn, int b) {
+  const int B = blockDim.x;
+  EllBuf e;
+  e.c = (int*)(dyn + (size_t)b * kPre * B * 8);
+  e.v = (float*)(e.c + kPre * B);
+  return e;
+}
+
+// Start the copy of the row at position rho of level l (which: 0 L, 1 U,
+// 2 A; rho < 0: no row) into this thread's slots of buffer e.
+template <class Sm>
+__device__ __forceinline__ void ell_issue(const Sm& s, int l, int which, int rho, const int* __restrict__ cg,
+                                          const float* __restrict__ vg, const EllBuf& e) {
+  const int t = threadIdx.x, B = blockDim.x;
+  const int off = s.tab[6 * l + 2 * which], w = rho >= 0 ? s.tab[6 * l + 2 * which + 1] : 0;
+  const int m = s.lev[l + 1] - s.lev[l];
+#pragma unroll
+  for (int u = 0; u < kPre; ++u) {
+    if (u < w) {
+      cp_async4(e.c + u * B + t, cg + off + u * m + rho);
+      cp_async4(e.v + u * B + t, vg + off + u * m + rho);
+    } else {
+      e.c[u * B + t] = -1;
+    }
+  }
+  cp_async_commit();
+}
+
+// The position of this thread's first row of level l, or -1.
+template <class Sm>
+__device__ __forceinline__ int first_rho(const Sm& s, int l) {
+  const LevelRows lr = level_rows(s.lev, s.loff, l);
+  return lr.q0 < lr.cnt ? lr.base + lr.q0 - s.lev[l] : -1;
+}
+
+// acc[c] = sum over the row's entries of val * word(col, c), every word read
+// until it carries `app`: chunks of kChunk entries whose words are all in
+// flight before the first wait; the first kPre entries from the thread's
+// buffer slots (copies complete), the rest from the table.  Sums in entry
+// order.
+template <int K, class Sm>
+__device__ __forceinline__ void gather_ell(const EllBuf& e, const Sm& s, int l, int which, int rho,
+                                           const int* __restrict__ cg, const float* __restrict__ vg,
+                                           const unsigned long long* words, unsigned app, Spin& sp,
+                                           float (&acc)[K]) {
+  constexpr int W = TRow<K>::W;
+  const int t = threadIdx.x, B = blockDim.x;
+  const int w = s.tab[6 * l + 2 * which + 1];
+  const int off = s.tab[6 * l + 2 * which], m = s.lev[l + 1] - s.lev[l];
+#pragma unroll
+  for (int c = 0; c < K; ++c) acc[c] = 0.f;
+  for (int e0 = 0; e0 < w; e0 += kChunk) {
+    int j[kChunk];
+    float v[kChunk];
+    unsigned long long x[kChunk][K];
+#pragma unroll
+    for (int u = 0; u < kChunk; ++u) {
+      const int k = e0 + u;
+      if (k < kPre) {
+        j[u] = e.c[k * B + t];
+        v[u] = e.v[k * B + t];
+      } else {
+        j[u] = k < w && rho >= 0 ? __ldg(cg + off + k * m + rho) : -1;
+        v[u] = j[u] >= 0 ? __ldg(vg + off + k * m + rho) : 0.f;
+      }
+      if (j[u] >= 0) load_row_words<K>(words + (size_t)j[u] * W, x[u]);
+    }
+#pragma unroll
+    for (int u = 0; u < kChunk; ++u) {
+      if (j[u] >= 0) {
+        wait_row<K>(words + (size_t)j[u] * W, x[u], app, sp);
+#pragma unroll
+        for (int c = 0; c < K; ++c) acc[c] += v[u] * __uint_as_float((unsigned)x[u][c]);
+      }
+    }
+  }
+}
+
+// Sum the V values of every block's partials (V-wide records) in block order;
+// result in sum[0..V).
+template <int V>
+__device__ void team_sum_wide(const double* part, int size, double* red, double* sum) {
+  double v[V];
+#pragma unroll
+  for (int c = 0; c < V; ++c) v[c] = 0.0;
+  for (int i = threadIdx.x; i < size * V; i += blockDim.x) {
+    const double x = __ldcg(part + i);
+    const int ci = i % V;
+#pragma unroll
+    for (int c = 0; c < V; ++c)
+      if (c == ci) v[c] += x;
+  }
+  block_reduce_store<V>(v, red, sum);
+}
+
+template <int K>
+__global__ void __launch_bounds__(384, 1) k_icsf(SolveArgs a) {
+  __shared__ IcsfSmem<K> s;
+  extern __shared__ __align__(16) unsigned char dyn[];  // the two ELL buffers
+  GridTeam team{a.ctl, a.timeout_ns, 0u};
+  const float* dinv = (const float*)a.dinv;
+  float* r = (float*)a.r;
+  float* u = (float*)a.z;   // M^-1 r of the own rows
+  float* w = (float*)a.y;   // A u of the own rows
+  float* p = (float*)a.p0;
+  float* sv = (float*)a.Ap; // s = A p
+  float* xin = (float*)a.xin;
+  unsigned long long* yw = (unsigned long long*)a.m0;  // forward-sweep words
+  unsigned long long* uw = (unsigned long long*)a.m1;  // backward-sweep words
+  constexpr int W = TRow<K>::W;
+  const int n = a.n, nlev = a.nlev;
+  const int row0 = blockIdx.x * blockDim.x + threadIdx.x, rstride = gridDim.x * blockDim.x;
+  const int tsize = gridDim.x;
+  double* part = a.partials;
+  int status = CN_OK, total_iters = 0, refinements = 0;
+  unsigned app = 0;
+  Spin sp{a.ctl, a.timeout_ns, 0ull, 0u, false};
+
+  for (int i = threadIdx.x; i <= nlev; i += blockDim.x) s.lev[i] = a.lev_ptr[i];
+  for (int i = threadIdx.x; i < 6 * nlev; i += blockDim.x) s.tab[i] = a.ell_tab[i];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int o = 0;
+    for (int l = 0; l < nlev; ++l) {
+      s.loff[l] = o;
+      o += (s.lev[l + 1] - s.lev[l] + (int)gridDim.x - 1) / (int)gridDim.x;
+    }
+  }
+  __syncthreads();
+  // every word starts with application number 0 (applications count from 1)
+  for (size_t i = row0; i < (size_t)n * W; i += rstride) {
+    yw[i] = 0ull;
+    uw[i] = 0ull;
+  }
+
+  // ---- right-hand side (HarmonicSolve.lean:51-66 / DeformSolve.lean:123-135)
+  {
+    double bb[K];
+#pragma unroll
+    for (int c = 0; c < K; ++c) bb[c] = 0.0;
+    for (int row = row0; row < n; row += rstride) {
+      double acc[K];
+#pragma unroll
+      for (int c = 0; c < K; ++c) acc[c] = 0.0;
+      const int v = a.free_of[row];
+      if (a.mode != CN_MODE_RHS) {
+        const bool deform = a.mode == CN_MODE_DEFORM;
+        gather_row<K, 1, 4>(a.K_ptr[v], a.K_ptr[v + 1], 0, a.K_col, a.K_val,
+                            [&](int uu, double* d) {
+                              const int h = a.hidx[uu];
+#pragma unroll
+                              for (int c = 0; c < K; ++c) {
+                                const double rest = deform ? a.pos[3 * uu + c % 3] : 0.0;
+                                d[c] = h >= 0 ? a.targets[(size_t)h * K + c] - rest : -rest;
+                              }
+                            },
+                            acc);
+      }
+#pragma unroll
+      for (int c = 0; c < K; ++c) {
+        const double b = a.mode == CN_MODE_RHS ? a.targets[(size_t)row * K + c] : -acc[c];
+        a.b64[(size_t)row * K + c] = b;
+        bb[c] += b * b;
+        if (!a.warm) a.x64[(size_t)row * K + c] = a.x0 ? a.x0[(size_t)v * K + c] : 0.0;
+      }
+    }
+    block_reduce_store<K>(bb, s.red, part + (size_t)blockIdx.x * K);
+    if (!team.sync()) { status = CN_TIMEOUT; goto done; }
+    team_sum_wide<K>(part, tsize, s.red, s.sum);
+    if (threadIdx.x < K) s.bb[threadIdx.x] = s.sum[threadIdx.x];
+    __syncthreads();
+  }
+
+  for (int refine = 0;; ++refine) {
+    // ---- FP64 residual r = b - A x (stays FP64)
+    {
+      double rr[K];
+#pragma unroll
+      for (int c = 0; c < K; ++c) rr[c] = 0.0;
+      for (int row = row0; row < n; row += rstride) {
+        double acc[K];
+#pragma unroll
+        for (int c = 0; c < K; ++c) acc[c] = 0.0;
+        gather_row<K, 1, 4>(a.A_ptr[row], a.A_ptr[row + 1], 0, a.A_col, a.A_val64,
+                            [&](int j, double* x) {
+#pragma unroll
+                              for (int c = 0; c < K; ++c) x[c] = a.x64[(size_t)j * K + c];
+                            },
+                            acc);
+#pragma unroll
+        for (int c = 0; c < K; ++c) {
+          const double rv = a.b64[(size_t)row * K + c] - acc[c];
+          r[(size_t)row * K + c] = (float)rv;
+          xin[(size_t)row * K + c] = 0.f;
+          rr[c] += rv * rv;
+        }
+      }
+      double* pslot = part + (size_t)tsize * K;
+      block_reduce_store<K>(rr, s.red, pslot + (size_t)blockIdx.x * K);
+      if (!team.sync()) { status = CN_TIMEOUT; goto done; }
+      team_sum_wide<K>(pslot, tsize, s.red, s.sum);
+      if (threadIdx.x == 0) {
+        int any = 0, bad = 0;
+        for (int c = 0; c < K; ++c) {
+          const double rr64 = s.sum[c], bb = s.bb[c];
+          const double rel = bb > 0.0 ? sqrt(rr64 / bb) : sqrt(rr64);
+          if (c < 32) a.stats->rel_residual[c] = rel;
+          if (!(rel == rel)) bad = 1;
+          const int act = rel > a.tol;
+          s.active[c] = act;
+          any |= act;
+          const double want = bb > 0.0 ? 0.5 * a.tol * sqrt(bb / (rr64 > 0.0 ? rr64 : 1.0)) : 0.0;
+          const double tau = fmax(a.inner_tol, want);
+          s.stop[c] = tau * tau * rr64;
+          s.alpha[c] = 0.0;
+          s.beta[c] = 0.0;
+        }
+        s.flag = bad ? 2 : (any ? 1 : 0);
+      }
+      __syncthreads();
+      if (s.flag == 2) { status = CN_NAN; break; }
+      if (s.flag == 0) { status = CN_OK; break; }
+      if (refine >= a.max_refine) { status = CN_MAX_ITER; break; }
+      refinements = refine + 1;
+    }
+
+    // ---- inner single-reduction PCG in FP32
+    int it = 0;
+    bool first = true;
+    for (;;) {
+      float al[K], be[K];
+#pragma unroll
+      for (int c = 0; c < K; ++c) {
+        al[c] = (float)s.alpha[c];
+        be[c] = (float)s.beta[c];
+      }
+      ++app;
+      sp.n = 0;
+      // forward sweep y = L~^-1 r, the update of each row first; the top
+      // level's u = y / L_ii is final and goes straight to the u words.  The
+      // ELL entries of this thread's first row of the next level are loaded
+      // while this level runs.
+      {
+        ell_issue(s, 0, 0, first_rho(s, 0), a.ell_cL, a.ell_vL, ell_buf(dyn, 0));
+        for (int l = 0; l < nlev; ++l) {
+          const LevelRows lr = level_rows(s.lev, s.loff, l);
+          const bool top = l == nlev - 1;
+          const EllBuf cur = ell_buf(dyn, l & 1);
+          cp_async_wait_all();
+          if (!top) ell_issue(s, l + 1, 0, first_rho(s, l + 1), a.ell_cL, a.ell_vL, ell_buf(dyn, (l + 1) & 1));
+          for (int q = lr.q0; q < lr.cnt; q += blockDim.x) {
+            const int row = lr.base + q;
+            if (q != lr.q0) {
+              ell_issue(s, l, 0, row - s.lev[l], a.ell_cL, a.ell_vL, cur);
+              cp_async_wait_all();
+            }
+            float rv[K];
+            if (!first) {
+#pragma unroll
+              for (int c = 0; c < K; ++c) {
+                const size_t ix = (size_t)row * K + c;
+                // beta = 0 (an inner solve's first update, or an inactive
+                // column): p = u, s = w, whatever the previous p, s hold
+                const float pv = be[c] == 0.f ? u[ix] : u[ix] + be[c] * p[ix];
+                const float svv = be[c] == 0.f ? w[ix] : w[ix] + be[c] * sv[ix];
+                p[ix] = pv;
+                sv[ix] = svv;
+                xin[ix] += al[c] * pv;
+                rv[c] = r[ix] - al[c] * svv;
+                r[ix] = rv[c];
+              }
+            } else {
+#pragma unroll
+              for (int c = 0; c < K; ++c) rv[c] = r[(size_t)row * K + c];
+            }
+            const float di = dinv[row];
+            float acc[K];
+            gather_ell<K>(cur, s, l, 0, row - s.lev[l], a.ell_cL, a.ell_vL, yw, app, sp, acc);
+            float yv[K];
+#pragma unroll
+            for (int c = 0; c < K; ++c) yv[c] = (rv[c] - acc[c]) * di;
+            if (top) {
+              float uv[K];
+#pragma unroll
+              for (int c = 0; c < K; ++c) {
+                uv[c] = yv[c] * di;
+                u[(size_t)row * K + c] = uv[c];
+              }
+              publish<K>(uw, row, uv, app);
+            } else {
+              publish<K>(yw, row, yv, app);
+            }
+          }
+          // the block's rows of this level are published before any of its
+          // rows of the next level reads them; rows of other blocks carry
+          // their application number
+          __syncthreads();
+        }
+      }
+      // backward sweep u = L~^-T y, levels nlev-2 .. 0 (own y from the words)
+      {
+        if (nlev >= 2) ell_issue(s, nlev - 2, 1, first_rho(s, nlev - 2), a.ell_cU, a.ell_vU, ell_buf(dyn, nlev & 1));
+        for (int l = nlev - 2; l >= 0; --l) {
+          const LevelRows lr = level_rows(s.lev, s.loff, l);
+          const EllBuf cur = ell_buf(dyn, l & 1);
+          cp_async_wait_all();
+          if (l > 0) ell_issue(s, l - 1, 1, first_rho(s, l - 1), a.ell_cU, a.ell_vU, ell_buf(dyn, (l - 1) & 1));
+          for (int q = lr.q0; q < lr.cnt; q += blockDim.x) {
+            const int row = lr.base + q;
+            if (q != lr.q0) {
+              ell_issue(s, l, 1, row - s.lev[l], a.ell_cU, a.ell_vU, cur);
+              cp_async_wait_all();
+            }
+            // the row's own y (this thread's word) before the waits
+            unsigned long long yx[K];
+            load_row_words<K>(yw + (size_t)row * W, yx);
+            const float di = dinv[row];
+            float acc[K];
+            gather_ell<K>(cur, s, l, 1, row - s.lev[l], a.ell_cU, a.ell_vU, uw, app, sp, acc);
+            float uv[K];
+#pragma unroll
+            for (int c = 0; c < K; ++c) {
+              uv[c] = (__uint_as_float((unsigned)yx[c]) - acc[c]) * di;
+              u[(size_t)row * K + c] = uv[c];
+            }
+            publish<K>(uw, row, uv, app);
+          }
+          __syncthreads();
+        }
+      }
+      // w = A u and the partial sums (r, u), (w, u), ||r||^2
+      double ga[K], de[K], rr[K];
+#pragma unroll
+      for (int c = 0; c < K; ++c) { ga[c] = 0.0; de[c] = 0.0; rr[c] = 0.0; }
+      for (int l = 0; l < nlev; ++l) {
+        const LevelRows lr = level_rows(s.lev, s.loff, l);
+        for (int q = lr.q0; q < lr.cnt; q += blockDim.x) {
+          const int row = lr.base + q;
+          const EllBuf cur = ell_buf(dyn, 0);
+          ell_issue(s, l, 2, row - s.lev[l], a.ell_cA, a.ell_vA, cur);
+          cp_async_wait_all();
+          float acc[K];
+          gather_ell<K>(cur, s, l, 2, row - s.lev[l], a.ell_cA, a.ell_vA, uw, app, sp, acc);
+#pragma unroll
+          for (int c = 0; c < K; ++c) {
+            const size_t ix = (size_t)row * K + c;
+            w[ix] = acc[c];
+            const double uu = (double)u[ix], rv = (double)r[ix];
+            ga[c] += rv * uu;
+            de[c] += (double)acc[c] * uu;
+            rr[c] += rv * rv;
+          }
+        }
+      }
+      {
+        double v[3 * K];
+#pragma unroll
+        for (int c = 0; c < K; ++c) { v[c] = ga[c]; v[K + c] = de[c]; v[2 * K + c] = rr[c]; }
+        // partials alternate between two 3K-wide tables by iteration parity
+        double* pslot = part + (size_t)tsize * K * (2 + 3 * (app & 1u));
+        block_reduce_store<3 * K>(v, s.red, pslot + (size_t)blockIdx.x * 3 * K);
+        // a wait of this iteration that gave up (here or in another block)
+        // ends the solve; the decision is the block's, read once
+        if (threadIdx.x == 0) s.abort = *(volatile int*)&a.ctl->abort;
+        __syncthreads();
+        if (s.abort) { status = CN_TIMEOUT; goto done; }
+        if (!team.sync()) { status = CN_TIMEOUT; goto done; }
+        team_sum_wide<3 * K>(pslot, tsize, s.red, s.sum);
+      }
+      if (threadIdx.x == 0) {
+        int any = 0, bad = 0;
+        for (int c = 0; c < K; ++c) {
+          const double g = s.sum[c], d = s.sum[K + c], rrv = s.sum[2 * K + c];
+          if (!(g == g) || !(d == d) || !(rrv == rrv)) bad = 1;
+          if (!first && s.active[c] && rrv < s.stop[c]) s.active[c] = 0;
+          double be2 = 0.0, al2 = 0.0;
+          if (s.active[c]) {
+            be2 = first || s.gprev[c] == 0.0 ? 0.0 : g / s.gprev[c];
+            const double den = first ? d : d - be2 * g / s.aprev[c];
+            // SparseLinAlg.lean:118 stops on pAp == 0; a non-positive
+            // curvature ends this column's inner solve (the next FP64
+            // residual decides whether it restarts)
+            if (den > 0.0) al2 = g / den;
+            else s.active[c] = 0;
+          }
+          if (!s.active[c]) { be2 = 0.0; al2 = 0.0; }
+          s.beta[c] = be2;
+          s.alpha[c] = al2;
+          s.gprev[c] = g;
+          if (al2 != 0.0) s.aprev[c] = al2;
+          any |= s.active[c];
+        }
+        s.flag = bad ? 2 : (any ? 1 : 0);
+      }
+      __syncthreads();
+      if (s.flag == 2) { status = CN_NAN; goto done; }
+      if (s.flag == 0 || it >= a.max_iter) break;
+      // the update of the next forward sweep is this iteration
+      ++it;
+      ++total_iters;
+      first = false;
+    }
+    // ---- x64 += xin (FP64 accumulation of the correction), own rows
+    {
+      for (int l = 0; l < nlev; ++l) {
+        const LevelRows lr = level_rows(s.lev, s.loff, l);
+        for (int q = lr.q0; q < lr.cnt; q += blockDim.x) {
+          const int row = lr.base + q;
+#pragma unroll
+          for (int c = 0; c < K; ++c) {
+            const size_t ix = (size_t)row * K + c;
+            a.x64[ix] += (double)xin[ix];
+          }
+        }
+      }
+    }
+    if (!team.sync()) { status = CN_TIMEOUT; goto done; }
+  }
+
+  // ---- output: free rows, then the handle overlay (DeformSolve.lean:108-109)
+  if (a.x_out) {
+    for (int row = row0; row < n; row += rstride) {
+      const int v = a.free_of[row];
+#pragma unroll
+      for (int c = 0; c < K; ++c) a.x_out[(size_t)v * K + c] = a.x64[(size_t)row * K + c];
+    }
+    for (int h = row0; h < a.nh; h += rstride) {
+      const int v = a.handles[h];
+#pragma unroll
+      for (int c = 0; c < K; ++c)
+        a.x_out[(size_t)v * K + c] = a.mode == CN_MODE_RHS ? 0.0 : a.targets[(size_t)h * K + c];
+    }
+  }
+
+done:
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    a.stats->status = status;
+    a.stats->iterations = total_iters;
+    a.stats->refinements = refinements;
+  }
+}
+
+inline size_t ell_smem(int block) { return (size_t)2 * kPre * block * 8; }
+
+template <int K>
+cudaError_t launch_k(const SolveArgs& a, int block, int grid, cudaStream_t st) {
+  const cudaError_t e =
+      cudaFuncSetAttribute(k_icsf<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ell_smem(block));
+  if (e != cudaSuccess) return e;
+  SolveArgs copy = a;
+  void* args[] = {&copy};
+  return cudaLaunchCooperativeKernel((const void*)k_icsf<K>, dim3(grid), dim3(block), args, ell_smem(block), st);
+}
+
+template <int K>
+int max_grid_k(int block) {
+  int dev = 0, sms = 0, per = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (cudaFuncSetAttribute(k_icsf<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ell_smem(block)) !=
+      cudaSuccess)
+    return 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_icsf<K>, block, ell_smem(block));
+  return sms * per;
+}
+
+__global__ void k_ell_values(const int* __restrict__ idx, const float* __restrict__ src, float* __restrict__ dst,
+                             long long count) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count; i += (long long)gridDim.x * blockDim.x) {
+    const int e = idx[i];
+    dst[i] = e >= 0 ? src[e] : 0.f;
+  }
+}
+
+}  // namespace
+
+int icsf_max_levels() { return kIcsfMaxLev; }
+
+cudaError_t launch_ell_values(const int* idx, const float* src, float* dst, long long count, cudaStream_t s) {
+  if (count <= 0) return cudaSuccess;
+  const int blocks = (int)std::min<long long>((count + 255) / 256, 148 * 16);
+  k_ell_values<<<blocks, 256, 0, s>>>(idx, src, dst, count);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_icsf_solve(const SolveArgs& a, int K, int block, int grid, cudaStream_t s) {
+  if (a.nlev > kIcsfMaxLev || grid < 1 || block > 384) return cudaErrorInvalidValue;
+  if (K == 1) return launch_k<1>(a, block, grid, s);
+  if (K == 3) return launch_k<3>(a, block, grid, s);
+  return cudaErrorInvalidValue;
+}
+
+int icsf_max_grid(int K, int block) {
+  if (K == 1) return max_grid_k<1>(block);
+  if (K == 3) return max_grid_k<3>(block);
+  return 0;
+}
+
+}  // namespace cn
