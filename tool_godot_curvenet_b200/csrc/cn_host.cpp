@@ -76,12 +76,6 @@ struct cn_system {
   int max_grid_alloc = 0;
   bool shape_set = false;   // cn_set_launch fixed the launch shape
   bool have_solution = false;
-  // IC(0) sweeps without grid barriers: per-level ELL tables of L, U and A
-  // (own allocations, built at the first such solve)
-  bool icsf_ready = false;
-  std::vector<void*> icsf_mem;
-  int *d_ell_tab = nullptr, *d_ell_cL = nullptr, *d_ell_cU = nullptr, *d_ell_cA = nullptr;
-  float *d_ell_vL = nullptr, *d_ell_vU = nullptr, *d_ell_vA = nullptr;
   // HSC preconditioner tables (own allocations)
   bool hsc = false;
   int hsc_L = 0, hsc_tail = 0, hsc_nc = 0;
@@ -186,91 +180,7 @@ cn_status up_new(cn_system* S, Tp** dst, const std::vector<Tp>& h) {
   return CN_OK;
 }
 
-// Upload h into a new device allocation recorded in `mem` (freed with the handle).
-template <class Tp>
-cn_status up_new_list(std::vector<void*>& mem, cudaStream_t stream, Tp** dst, const std::vector<Tp>& h) {
-  const size_t bytes = sizeof(Tp) * std::max<size_t>(h.size(), 1);
-  if (cudaMalloc((void**)dst, bytes) != cudaSuccess) {
-    set_err("device allocation of %zu bytes failed", bytes);
-    return CN_CUDA_ERROR;
-  }
-  mem.push_back(*dst);
-  if (!h.empty() && cudaMemcpyAsync(*dst, h.data(), sizeof(Tp) * h.size(), cudaMemcpyHostToDevice, stream) != cudaSuccess) {
-    set_err("upload failed");
-    return CN_CUDA_ERROR;
-  }
-  return CN_OK;
-}
-
 std::vector<float> to_f32(const std::vector<double>& v) { return std::vector<float>(v.begin(), v.end()); }
-
-// Per-level ELL tables of L, U and A for the IC(0) solve without grid
-// barriers: for level l (rows lo..hi, m = hi - lo) and matrix X, entry e of
-// the row at position rho at off_X(l) + e * m + rho, width w_X(l) = the
-// longest row of X in the level; columns -1 pad.  The values are gathered on
-// the device from the handle's FP32 L, U and A.
-cn_status setup_icsf(cn_system* S) {
-  const MeshHost& H = S->H;
-  const int nl = H.nlev;
-  std::vector<int> tab((size_t)6 * std::max(nl, 1), 0);
-  long long tot[3] = {0, 0, 0};
-  const std::vector<int>* ptr[3] = {&H.L_ptr, &H.U_ptr, &H.A_ptr};
-  const std::vector<int>* col[3] = {&H.L_col, &H.U_col, &H.A_col};
-  for (int l = 0; l < nl; ++l) {
-    const int lo = H.lev_ptr[l], hi = H.lev_ptr[l + 1];
-    for (int x = 0; x < 3; ++x) {
-      int w = 0;
-      for (int i = lo; i < hi; ++i) w = std::max(w, (*ptr[x])[i + 1] - (*ptr[x])[i]);
-      tab[6 * l + 2 * x] = (int)tot[x];
-      tab[6 * l + 2 * x + 1] = w;
-      tot[x] += (long long)(hi - lo) * w;
-    }
-  }
-  for (int x = 0; x < 3; ++x)
-    if (tot[x] >= (1LL << 31)) {
-      set_err("IC(0) level tables exceed 2^31 entries");
-      return CN_BAD_INPUT;
-    }
-  const float* src[3] = {S->D.L32, S->D.U32, S->D.A32};
-  int* dc[3] = {};
-  float* dv[3] = {};
-  for (int x = 0; x < 3; ++x) {
-    std::vector<int> c((size_t)std::max<long long>(tot[x], 1), -1), e((size_t)std::max<long long>(tot[x], 1), -1);
-    for (int l = 0; l < nl; ++l) {
-      const int lo = H.lev_ptr[l], hi = H.lev_ptr[l + 1], m = hi - lo, off = tab[6 * l + 2 * x];
-      for (int i = lo; i < hi; ++i)
-        for (int k = (*ptr[x])[i]; k < (*ptr[x])[i + 1]; ++k) {
-          const size_t at = (size_t)off + (size_t)(k - (*ptr[x])[i]) * m + (i - lo);
-          c[at] = (*col[x])[k];
-          e[at] = k;
-        }
-    }
-    cn_status st = up_new_list(S->icsf_mem, S->stream, &dc[x], c);
-    if (st != CN_OK) return st;
-    int* d_e = nullptr;
-    if (cudaMalloc((void**)&d_e, sizeof(int) * e.size()) != cudaSuccess ||
-        cudaMalloc((void**)&dv[x], sizeof(float) * e.size()) != cudaSuccess) {
-      if (d_e) cudaFree(d_e);
-      set_err("device allocation of the IC(0) level tables failed");
-      return CN_CUDA_ERROR;
-    }
-    S->icsf_mem.push_back(dv[x]);
-    const bool ok = cudaMemcpyAsync(d_e, e.data(), sizeof(int) * e.size(), cudaMemcpyHostToDevice, S->stream) == cudaSuccess &&
-                    cn::launch_ell_values(d_e, src[x], dv[x], (long long)e.size(), S->stream) == cudaSuccess &&
-                    cudaStreamSynchronize(S->stream) == cudaSuccess;
-    cudaFree(d_e);
-    if (!ok) {
-      set_err("building the IC(0) level tables failed");
-      return CN_CUDA_ERROR;
-    }
-  }
-  cn_status st = up_new_list(S->icsf_mem, S->stream, &S->d_ell_tab, tab);
-  if (st != CN_OK) return st;
-  S->d_ell_cL = dc[0]; S->d_ell_cU = dc[1]; S->d_ell_cA = dc[2];
-  S->d_ell_vL = dv[0]; S->d_ell_vU = dv[1]; S->d_ell_vA = dv[2];
-  S->icsf_ready = true;
-  return CN_OK;
-}
 
 // HSC: read A back, build the hierarchy on the host, move the rows into HSC
 // order, reassemble A in that order and upload the level tables.
@@ -526,7 +436,6 @@ void cn_destroy(cn_handle S) {
   if (S->stream) cudaStreamSynchronize(S->stream);
   if (S->buf) cudaFree(S->buf);
   for (void* p : S->hsc_mem) cudaFree(p);
-  for (void* p : S->icsf_mem) cudaFree(p);
   for (void* p : S->cnet_mem) cudaFree(p);
   for (void* p : {(void*)S->cnet.seg, (void*)S->cnet.ends, (void*)S->d_cnet_posed, (void*)S->d_cnet_F,
                   (void*)S->d_cnet_X})
@@ -599,8 +508,8 @@ cn_status cn_solve_device(cn_handle S, int32_t k, const double* d_targets, doubl
   // The row-cached Jacobi kernel runs k = 9 as three k = 3 solves on column
   // slices: its k = 9 state fits neither shared memory nor registers, and
   // three k = 3 solves take a third of the time of one k = 9 solve.  The
-  // IC(0) solve without grid barriers does the same (its gathers keep the
-  // words of six neighbour rows in registers).
+  // IC(0) solve without grid barriers does the same (its k = 9 gathers would
+  // hold 36 words of the neighbour rows in registers).
   if (k == 9 && (row_cached(S) || icsf_path(S, o)) && o.algo != CN_ALGO_PLAIN && S->d_split_t &&
       o.tol > 0.0 && o.max_iter >= 0 && o.max_refine >= 1) {
     CN_CUDA(cudaSetDevice(S->device));
@@ -825,15 +734,7 @@ cn_status cn_solve_device(cn_handle S, int32_t k, const double* d_targets, doubl
   // barriers (tagged words) under the single-reduction CG; CLASSIC keeps the
   // level-scheduled kernel
   if (icsf_path(S, o)) {
-    if (!S->icsf_ready) {
-      const cn_status st = setup_icsf(S);
-      if (st != CN_OK) return st;
-    }
-    a.ell_tab = S->d_ell_tab;
-    a.ell_cL = S->d_ell_cL; a.ell_vL = S->d_ell_vL;
-    a.ell_cU = S->d_ell_cU; a.ell_vU = S->d_ell_vU;
-    a.ell_cA = S->d_ell_cA; a.ell_vA = S->d_ell_vA;
-    const int block = std::min(S->block, 384);
+    const int block = std::min(S->block, 512);
     const int mg = cn::icsf_max_grid(k, block);
     if (mg <= 0) {
       set_err("the IC(0) solve does not fit on this device (block %d)", block);

@@ -48,8 +48,6 @@
 // 64th and the shared abort flag every 64th; a wait that runs out raises the
 // abort flag, the others leave at their next check, and the solve ends with
 // CN_TIMEOUT at the next block-uniform check.
-#include <algorithm>
-
 #include "cn_pcg_body.cuh"
 
 namespace cn {
@@ -71,10 +69,6 @@ __device__ __forceinline__ unsigned long long tag_word(float v, unsigned app) {
 
 __device__ __forceinline__ void ld_pair(const unsigned long long* p, unsigned long long& a, unsigned long long& b) {
   asm volatile("ld.relaxed.gpu.global.v2.u64 {%0, %1}, [%2];" : "=l"(a), "=l"(b) : "l"(p));
-}
-
-__device__ __forceinline__ void ld_one(const unsigned long long* p, unsigned long long& a) {
-  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(a) : "l"(p));
 }
 
 __device__ __forceinline__ void st_pair(unsigned long long* p, unsigned long long a, unsigned long long b) {
@@ -121,28 +115,51 @@ struct Spin {
   }
 };
 
-// The K words of a row (pairs, then the last one alone when K is odd).
-template <int K>
-__device__ __forceinline__ void load_row_words(const unsigned long long* p, unsigned long long (&x)[K]) {
+// acc[c] = sum over the row's entries e0..e1 of val[e] * word(col[e], c),
+// every word read until it carries `app`.  U entries at a time: their indices
+// and values, then all their words, then the waits and the multiply-adds in
+// entry order.
+template <int K, int U>
+__device__ __forceinline__ void gather_tagged(int e0, int e1, const int* __restrict__ col,
+                                              const float* __restrict__ val, const unsigned long long* words,
+                                              unsigned app, Spin& sp, float (&acc)[K]) {
+  constexpr int W = TRow<K>::W;
 #pragma unroll
-  for (int i = 0; i + 1 < K; i += 2) ld_pair(p + i, x[i], x[i + 1]);
-  if (K & 1) ld_one(p + K - 1, x[K - 1]);
-}
-
-template <int K>
-__device__ __forceinline__ bool row_ready(const unsigned long long (&x)[K], unsigned app) {
-  bool ok = true;
+  for (int c = 0; c < K; ++c) acc[c] = 0.f;
+  for (int e = e0; e < e1; e += U) {
+    int j[U];
+    float v[U];
 #pragma unroll
-  for (int c = 0; c < K; ++c) ok = ok && (unsigned)(x[c] >> 32) == app;
-  return ok;
-}
-
-// Reads the row's words again until every one carries `app` (or the wait
-// gives up).
-template <int K>
-__device__ __forceinline__ void wait_row(const unsigned long long* p, unsigned long long (&x)[K], unsigned app,
-                                         Spin& sp) {
-  while (!row_ready<K>(x, app) && sp.poll()) load_row_words<K>(p, x);
+    for (int u = 0; u < U; ++u) {
+      const bool ok = e + u < e1;
+      j[u] = ok ? __ldg(col + e + u) : -1;
+      v[u] = ok ? __ldg(val + e + u) : 0.f;
+    }
+    unsigned long long x[U][W];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (j[u] >= 0) {
+#pragma unroll
+        for (int i = 0; i < W / 2; ++i) ld_pair(words + (size_t)j[u] * W + 2 * i, x[u][2 * i], x[u][2 * i + 1]);
+      } else {
+#pragma unroll
+        for (int i = 0; i < W; ++i) x[u][i] = (unsigned long long)app << 32;
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      for (;;) {
+        bool ready = true;
+#pragma unroll
+        for (int c = 0; c < K; ++c) ready = ready && (unsigned)(x[u][c] >> 32) == app;
+        if (ready || !sp.poll()) break;
+#pragma unroll
+        for (int i = 0; i < W / 2; ++i) ld_pair(words + (size_t)j[u] * W + 2 * i, x[u][2 * i], x[u][2 * i + 1]);
+      }
+#pragma unroll
+      for (int c = 0; c < K; ++c) acc[c] += v[u] * __uint_as_float((unsigned)x[u][c]);
+    }
+  }
 }
 
 // Rows of level l owned by this thread: block b's chunk of the level,
@@ -174,109 +191,7 @@ struct IcsfSmem {
   int abort;
   int lev[kIcsfMaxLev + 1];
   int loff[kIcsfMaxLev];  // ownership offset of each level: chunk sizes of the lower levels
-  int tab[6 * kIcsfMaxLev];  // per level: first entry and width of the L, U and A tables
 };
-
-// The first kPre entries of a row's ELL table (column -1: none), copied by
-// the thread into its slots of a shared-memory buffer with cp.async (no
-// registers held while the copy is in flight): slot u of thread t at u * B + t
-// (columns), then the values.  A row of level l is at position rho = row -
-// first row of the level, its entry e at tab_off + e * level_size + rho
-// (consecutive rows of a level are consecutive words: a warp's loads
-// coalesce).  Two buffers: the rows of the current level and those of the
-// next one, prefetched while the current level runs.
-constexpr int kPre = 12;   // entries per row copied ahead
-constexpr int kChunk = 6;  // entries whose words are in flight together
-
-__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
-  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(sa), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
-
-struct EllBuf {
-  int* c;    // kPre x blockDim.x
-  float* v;  // kPre x blockDim.x
-};
-
-__device__ __forceinline__ EllBuf ell_buf(unsigned char* dyn, int b) {
-  const int B = blockDim.x;
-  EllBuf e;
-  e.c = (int*)(dyn + (size_t)b * kPre * B * 8);
-  e.v = (float*)(e.c + kPre * B);
-  return e;
-}
-
-// Start the copy of the row at position rho of level l (which: 0 L, 1 U,
-// 2 A; rho < 0: no row) into this thread's slots of buffer e.
-template <class Sm>
-__device__ __forceinline__ void ell_issue(const Sm& s, int l, int which, int rho, const int* __restrict__ cg,
-                                          const float* __restrict__ vg, const EllBuf& e) {
-  const int t = threadIdx.x, B = blockDim.x;
-  const int off = s.tab[6 * l + 2 * which], w = rho >= 0 ? s.tab[6 * l + 2 * which + 1] : 0;
-  const int m = s.lev[l + 1] - s.lev[l];
-#pragma unroll
-  for (int u = 0; u < kPre; ++u) {
-    if (u < w) {
-      cp_async4(e.c + u * B + t, cg + off + u * m + rho);
-      cp_async4(e.v + u * B + t, vg + off + u * m + rho);
-    } else {
-      e.c[u * B + t] = -1;
-    }
-  }
-  cp_async_commit();
-}
-
-// The position of this thread's first row of level l, or -1.
-template <class Sm>
-__device__ __forceinline__ int first_rho(const Sm& s, int l) {
-  const LevelRows lr = level_rows(s.lev, s.loff, l);
-  return lr.q0 < lr.cnt ? lr.base + lr.q0 - s.lev[l] : -1;
-}
-
-// acc[c] = sum over the row's entries of val * word(col, c), every word read
-// until it carries `app`: chunks of kChunk entries whose words are all in
-// flight before the first wait; the first kPre entries from the thread's
-// buffer slots (copies complete), the rest from the table.  Sums in entry
-// order.
-template <int K, class Sm>
-__device__ __forceinline__ void gather_ell(const EllBuf& e, const Sm& s, int l, int which, int rho,
-                                           const int* __restrict__ cg, const float* __restrict__ vg,
-                                           const unsigned long long* words, unsigned app, Spin& sp,
-                                           float (&acc)[K]) {
-  constexpr int W = TRow<K>::W;
-  const int t = threadIdx.x, B = blockDim.x;
-  const int w = s.tab[6 * l + 2 * which + 1];
-  const int off = s.tab[6 * l + 2 * which], m = s.lev[l + 1] - s.lev[l];
-#pragma unroll
-  for (int c = 0; c < K; ++c) acc[c] = 0.f;
-  for (int e0 = 0; e0 < w; e0 += kChunk) {
-    int j[kChunk];
-    float v[kChunk];
-    unsigned long long x[kChunk][K];
-#pragma unroll
-    for (int u = 0; u < kChunk; ++u) {
-      const int k = e0 + u;
-      if (k < kPre) {
-        j[u] = e.c[k * B + t];
-        v[u] = e.v[k * B + t];
-      } else {
-        j[u] = k < w && rho >= 0 ? __ldg(cg + off + k * m + rho) : -1;
-        v[u] = j[u] >= 0 ? __ldg(vg + off + k * m + rho) : 0.f;
-      }
-      if (j[u] >= 0) load_row_words<K>(words + (size_t)j[u] * W, x[u]);
-    }
-#pragma unroll
-    for (int u = 0; u < kChunk; ++u) {
-      if (j[u] >= 0) {
-        wait_row<K>(words + (size_t)j[u] * W, x[u], app, sp);
-#pragma unroll
-        for (int c = 0; c < K; ++c) acc[c] += v[u] * __uint_as_float((unsigned)x[u][c]);
-      }
-    }
-  }
-}
 
 // Sum the V values of every block's partials (V-wide records) in block order;
 // result in sum[0..V).
@@ -296,10 +211,12 @@ __device__ void team_sum_wide(const double* part, int size, double* red, double*
 }
 
 template <int K>
-__global__ void __launch_bounds__(384, 1) k_icsf(SolveArgs a) {
+__global__ void __launch_bounds__(512) k_icsf(SolveArgs a) {
   __shared__ IcsfSmem<K> s;
-  extern __shared__ __align__(16) unsigned char dyn[];  // the two ELL buffers
   GridTeam team{a.ctl, a.timeout_ns, 0u};
+  const float* Aval = (const float*)a.A_val;
+  const float* Lval = (const float*)a.L_val;
+  const float* Uval = (const float*)a.U_val;
   const float* dinv = (const float*)a.dinv;
   float* r = (float*)a.r;
   float* u = (float*)a.z;   // M^-1 r of the own rows
@@ -310,6 +227,10 @@ __global__ void __launch_bounds__(384, 1) k_icsf(SolveArgs a) {
   unsigned long long* yw = (unsigned long long*)a.m0;  // forward-sweep words
   unsigned long long* uw = (unsigned long long*)a.m1;  // backward-sweep words
   constexpr int W = TRow<K>::W;
+  // entries whose words are in flight together: rows of L and U hold ~3
+  // entries, rows of A ~7
+  constexpr int kUL = K <= 3 ? 4 : 2;
+  constexpr int kUA = K <= 3 ? 8 : 2;
   const int n = a.n, nlev = a.nlev;
   const int row0 = blockIdx.x * blockDim.x + threadIdx.x, rstride = gridDim.x * blockDim.x;
   const int tsize = gridDim.x;
@@ -319,7 +240,6 @@ __global__ void __launch_bounds__(384, 1) k_icsf(SolveArgs a) {
   Spin sp{a.ctl, a.timeout_ns, 0ull, 0u, false};
 
   for (int i = threadIdx.x; i <= nlev; i += blockDim.x) s.lev[i] = a.lev_ptr[i];
-  for (int i = threadIdx.x; i < 6 * nlev; i += blockDim.x) s.tab[i] = a.ell_tab[i];
   __syncthreads();
   if (threadIdx.x == 0) {
     int o = 0;
@@ -438,97 +358,77 @@ __global__ void __launch_bounds__(384, 1) k_icsf(SolveArgs a) {
       }
       ++app;
       sp.n = 0;
+
       // forward sweep y = L~^-1 r, the update of each row first; the top
-      // level's u = y / L_ii is final and goes straight to the u words.  The
-      // ELL entries of this thread's first row of the next level are loaded
-      // while this level runs.
-      {
-        ell_issue(s, 0, 0, first_rho(s, 0), a.ell_cL, a.ell_vL, ell_buf(dyn, 0));
-        for (int l = 0; l < nlev; ++l) {
-          const LevelRows lr = level_rows(s.lev, s.loff, l);
-          const bool top = l == nlev - 1;
-          const EllBuf cur = ell_buf(dyn, l & 1);
-          cp_async_wait_all();
-          if (!top) ell_issue(s, l + 1, 0, first_rho(s, l + 1), a.ell_cL, a.ell_vL, ell_buf(dyn, (l + 1) & 1));
-          for (int q = lr.q0; q < lr.cnt; q += blockDim.x) {
-            const int row = lr.base + q;
-            if (q != lr.q0) {
-              ell_issue(s, l, 0, row - s.lev[l], a.ell_cL, a.ell_vL, cur);
-              cp_async_wait_all();
+      // level's u = y / L_ii is final and goes straight to the u words
+      for (int l = 0; l < nlev; ++l) {
+        const LevelRows lr = level_rows(s.lev, s.loff, l);
+        const bool top = l == nlev - 1;
+        for (int q = lr.q0; q < lr.cnt; q += blockDim.x) {
+          const int row = lr.base + q;
+          float rv[K];
+          if (!first) {
+#pragma unroll
+            for (int c = 0; c < K; ++c) {
+              const size_t ix = (size_t)row * K + c;
+              // beta = 0 (an inner solve's first update, or an inactive
+              // column): p = u, s = w, whatever the previous p, s hold
+              const float pv = be[c] == 0.f ? u[ix] : u[ix] + be[c] * p[ix];
+              const float svv = be[c] == 0.f ? w[ix] : w[ix] + be[c] * sv[ix];
+              p[ix] = pv;
+              sv[ix] = svv;
+              xin[ix] += al[c] * pv;
+              rv[c] = r[ix] - al[c] * svv;
+              r[ix] = rv[c];
             }
-            float rv[K];
-            if (!first) {
+          } else {
 #pragma unroll
-              for (int c = 0; c < K; ++c) {
-                const size_t ix = (size_t)row * K + c;
-                // beta = 0 (an inner solve's first update, or an inactive
-                // column): p = u, s = w, whatever the previous p, s hold
-                const float pv = be[c] == 0.f ? u[ix] : u[ix] + be[c] * p[ix];
-                const float svv = be[c] == 0.f ? w[ix] : w[ix] + be[c] * sv[ix];
-                p[ix] = pv;
-                sv[ix] = svv;
-                xin[ix] += al[c] * pv;
-                rv[c] = r[ix] - al[c] * svv;
-                r[ix] = rv[c];
-              }
-            } else {
-#pragma unroll
-              for (int c = 0; c < K; ++c) rv[c] = r[(size_t)row * K + c];
-            }
-            const float di = dinv[row];
-            float acc[K];
-            gather_ell<K>(cur, s, l, 0, row - s.lev[l], a.ell_cL, a.ell_vL, yw, app, sp, acc);
-            float yv[K];
-#pragma unroll
-            for (int c = 0; c < K; ++c) yv[c] = (rv[c] - acc[c]) * di;
-            if (top) {
-              float uv[K];
-#pragma unroll
-              for (int c = 0; c < K; ++c) {
-                uv[c] = yv[c] * di;
-                u[(size_t)row * K + c] = uv[c];
-              }
-              publish<K>(uw, row, uv, app);
-            } else {
-              publish<K>(yw, row, yv, app);
-            }
+            for (int c = 0; c < K; ++c) rv[c] = r[(size_t)row * K + c];
           }
-          // the block's rows of this level are published before any of its
-          // rows of the next level reads them; rows of other blocks carry
-          // their application number
-          __syncthreads();
-        }
-      }
-      // backward sweep u = L~^-T y, levels nlev-2 .. 0 (own y from the words)
-      {
-        if (nlev >= 2) ell_issue(s, nlev - 2, 1, first_rho(s, nlev - 2), a.ell_cU, a.ell_vU, ell_buf(dyn, nlev & 1));
-        for (int l = nlev - 2; l >= 0; --l) {
-          const LevelRows lr = level_rows(s.lev, s.loff, l);
-          const EllBuf cur = ell_buf(dyn, l & 1);
-          cp_async_wait_all();
-          if (l > 0) ell_issue(s, l - 1, 1, first_rho(s, l - 1), a.ell_cU, a.ell_vU, ell_buf(dyn, (l - 1) & 1));
-          for (int q = lr.q0; q < lr.cnt; q += blockDim.x) {
-            const int row = lr.base + q;
-            if (q != lr.q0) {
-              ell_issue(s, l, 1, row - s.lev[l], a.ell_cU, a.ell_vU, cur);
-              cp_async_wait_all();
-            }
-            // the row's own y (this thread's word) before the waits
-            unsigned long long yx[K];
-            load_row_words<K>(yw + (size_t)row * W, yx);
-            const float di = dinv[row];
-            float acc[K];
-            gather_ell<K>(cur, s, l, 1, row - s.lev[l], a.ell_cU, a.ell_vU, uw, app, sp, acc);
+          float acc[K];
+          gather_tagged<K, kUL>(a.L_ptr[row], a.L_ptr[row + 1], a.L_col, Lval, yw, app, sp, acc);
+          const float di = dinv[row];
+          float yv[K];
+#pragma unroll
+          for (int c = 0; c < K; ++c) yv[c] = (rv[c] - acc[c]) * di;
+          if (top) {
             float uv[K];
 #pragma unroll
             for (int c = 0; c < K; ++c) {
-              uv[c] = (__uint_as_float((unsigned)yx[c]) - acc[c]) * di;
+              uv[c] = yv[c] * di;
               u[(size_t)row * K + c] = uv[c];
             }
             publish<K>(uw, row, uv, app);
+          } else {
+            publish<K>(yw, row, yv, app);
           }
-          __syncthreads();
         }
+        // the block's rows of this level are published before any of its
+        // rows of the next level reads them; rows of other blocks carry
+        // their application number
+        __syncthreads();
+      }
+      // backward sweep u = L~^-T y, levels nlev-2 .. 0 (own y from the words)
+      for (int l = nlev - 2; l >= 0; --l) {
+        const LevelRows lr = level_rows(s.lev, s.loff, l);
+        for (int q = lr.q0; q < lr.cnt; q += blockDim.x) {
+          const int row = lr.base + q;
+          // the row's own y (this thread's word) before the waits
+          unsigned long long yx[W];
+#pragma unroll
+          for (int i = 0; i < W / 2; ++i) ld_pair(yw + (size_t)row * W + 2 * i, yx[2 * i], yx[2 * i + 1]);
+          const float di = dinv[row];
+          float acc[K];
+          gather_tagged<K, kUL>(a.U_ptr[row], a.U_ptr[row + 1], a.U_col, Uval, uw, app, sp, acc);
+          float uv[K];
+#pragma unroll
+          for (int c = 0; c < K; ++c) {
+            uv[c] = (__uint_as_float((unsigned)yx[c]) - acc[c]) * di;
+            u[(size_t)row * K + c] = uv[c];
+          }
+          publish<K>(uw, row, uv, app);
+        }
+        __syncthreads();
       }
       // w = A u and the partial sums (r, u), (w, u), ||r||^2
       double ga[K], de[K], rr[K];
@@ -538,11 +438,8 @@ __global__ void __launch_bounds__(384, 1) k_icsf(SolveArgs a) {
         const LevelRows lr = level_rows(s.lev, s.loff, l);
         for (int q = lr.q0; q < lr.cnt; q += blockDim.x) {
           const int row = lr.base + q;
-          const EllBuf cur = ell_buf(dyn, 0);
-          ell_issue(s, l, 2, row - s.lev[l], a.ell_cA, a.ell_vA, cur);
-          cp_async_wait_all();
           float acc[K];
-          gather_ell<K>(cur, s, l, 2, row - s.lev[l], a.ell_cA, a.ell_vA, uw, app, sp, acc);
+          gather_tagged<K, kUA>(a.A_ptr[row], a.A_ptr[row + 1], a.A_col, Aval, uw, app, sp, acc);
 #pragma unroll
           for (int c = 0; c < K; ++c) {
             const size_t ix = (size_t)row * K + c;
@@ -642,16 +539,11 @@ done:
   }
 }
 
-inline size_t ell_smem(int block) { return (size_t)2 * kPre * block * 8; }
-
 template <int K>
 cudaError_t launch_k(const SolveArgs& a, int block, int grid, cudaStream_t st) {
-  const cudaError_t e =
-      cudaFuncSetAttribute(k_icsf<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ell_smem(block));
-  if (e != cudaSuccess) return e;
   SolveArgs copy = a;
   void* args[] = {&copy};
-  return cudaLaunchCooperativeKernel((const void*)k_icsf<K>, dim3(grid), dim3(block), args, ell_smem(block), st);
+  return cudaLaunchCooperativeKernel((const void*)k_icsf<K>, dim3(grid), dim3(block), args, 0, st);
 }
 
 template <int K>
@@ -659,34 +551,16 @@ int max_grid_k(int block) {
   int dev = 0, sms = 0, per = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  if (cudaFuncSetAttribute(k_icsf<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ell_smem(block)) !=
-      cudaSuccess)
-    return 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_icsf<K>, block, ell_smem(block));
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_icsf<K>, block, 0);
   return sms * per;
-}
-
-__global__ void k_ell_values(const int* __restrict__ idx, const float* __restrict__ src, float* __restrict__ dst,
-                             long long count) {
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count; i += (long long)gridDim.x * blockDim.x) {
-    const int e = idx[i];
-    dst[i] = e >= 0 ? src[e] : 0.f;
-  }
 }
 
 }  // namespace
 
 int icsf_max_levels() { return kIcsfMaxLev; }
 
-cudaError_t launch_ell_values(const int* idx, const float* src, float* dst, long long count, cudaStream_t s) {
-  if (count <= 0) return cudaSuccess;
-  const int blocks = (int)std::min<long long>((count + 255) / 256, 148 * 16);
-  k_ell_values<<<blocks, 256, 0, s>>>(idx, src, dst, count);
-  return cudaGetLastError();
-}
-
 cudaError_t launch_icsf_solve(const SolveArgs& a, int K, int block, int grid, cudaStream_t s) {
-  if (a.nlev > kIcsfMaxLev || grid < 1 || block > 384) return cudaErrorInvalidValue;
+  if (a.nlev > kIcsfMaxLev || grid < 1 || block > 512) return cudaErrorInvalidValue;
   if (K == 1) return launch_k<1>(a, block, grid, s);
   if (K == 3) return launch_k<3>(a, block, grid, s);
   return cudaErrorInvalidValue;

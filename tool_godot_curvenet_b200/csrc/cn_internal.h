@@ -92,17 +92,6 @@ struct SolveArgs {
   void* bss_lent;
   const long long* bss_loff;
   double* partials;        // [kSlots][grid][K]
-  // IC(0) sweeps without grid barriers (cn_icsf.cu): per level, ELL tables of
-  // L, U and A over the level's rows (entry e of the row at position rho of
-  // level l at tab_off + e * level_size + rho; column -1: padding) and the
-  // table nlev x [L first entry, L width, U ..., A ...]
-  const int* ell_tab;
-  const int* ell_cL;
-  const float* ell_vL;
-  const int* ell_cU;
-  const float* ell_vU;
-  const int* ell_cA;
-  const float* ell_vA;
   // HSC preconditioner (hsc != 0): rows are in HSC order; F_l = positions
   // [hsc_off[l], hsc_off[l + 1]); the coarse set starts at hsc_off[hsc_L];
   // levels >= hsc_tail (and the coarse solve) run in block 0 alone.
@@ -143,12 +132,10 @@ int persistent_max_grid(int precision, int K, int lanes, int block);
 
 // The mixed-precision IC(0) solve with synchronisation-free sweeps
 // (cn_icsf.cu): tagged words of the forward and backward sweeps in a.m0 and
-// a.m1 ([rows][round_up(K, 2)] 64-bit words each), the ELL tables in a.ell_*;
-// K = 1 or 3; at most icsf_max_levels() levels; a cooperative launch of
-// `grid` blocks of `block` threads (block <= 512).
+// a.m1 ([rows][round_up(K, 2)] 64-bit words each); K = 1 or 3; at most
+// icsf_max_levels() levels; a cooperative launch of `grid` blocks of `block`
+// threads (block <= 512).
 cudaError_t launch_icsf_solve(const SolveArgs& a, int K, int block, int grid, cudaStream_t s);
-// dst[i] = src[idx[i]] (0 where idx[i] < 0): the values of the ELL tables.
-cudaError_t launch_ell_values(const int* idx, const float* src, float* dst, long long count, cudaStream_t s);
 int icsf_max_grid(int K, int block);
 int icsf_max_levels();
 
