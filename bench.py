@@ -652,8 +652,9 @@ def c4_section(local, reps=20):
 
 def c5_section(torch, local, peak, steps=3):
     """The large-scale workload (torus 1024 x 1024 = 1.05M vertices, 16 seams,
-    1% handles, U(-0.5, 0.5), 3 RHS, 1e-8): IC(0), HSC, block SSOR and Jacobi
-    in mixed precision and IC(0) in FP64 -- iterations, build and solve time,
+    1% handles, U(-0.5, 0.5), 3 RHS, 1e-8): IC(0) (sweeps without grid
+    barriers, and the level-scheduled kernel), HSC, block SSOR and Jacobi in
+    mixed precision and IC(0) in FP64 -- iterations, build and solve time,
     and for IC(0) the achieved bandwidth of its algorithmic bytes (SpMV, the
     two triangular sweeps, 9 vector passes per iteration).  The vectors and
     the factor exceed L2; L2 is flushed before every timed solve as well."""
@@ -667,22 +668,24 @@ def c5_section(torch, local, peak, steps=3):
     flush = torch.ones(64 << 20, dtype=torch.float32, device=dev)
     out = {"workload": "torus1024x1024_16seams_1pct_handles_3rhs", "n_verts": int(pos.shape[0]), "tol": 1e-8,
            "l2": "flushed (256 MB read) before every timed solve"}
-    for precond, precision in [("ic0", "mixed"), ("hsc", "mixed"), ("bssor", "mixed"), ("jacobi", "mixed"),
-                               ("ic0", "fp64")]:
+    for precond, precision, algo in [("ic0", "mixed", "fused"), ("ic0", "mixed", "classic"), ("hsc", "mixed", "fused"),
+                                     ("bssor", "mixed", "fused"), ("jacobi", "mixed", "fused"),
+                                     ("ic0", "fp64", "fused")]:
         t0 = time.perf_counter()
         with CutMeshSolver(pos, tris, h, device=local, precond=precond) as s:
             build_s = time.perf_counter() - t0
             info = s.info()
             st, ms = time_device_solves(torch, s, local, 3, d_t.data_ptr(), d_x.data_ptr(), steps, 1, flush,
-                                        mode="deform", precision=precision, tol=1e-8, max_iter=20000)
+                                        mode="deform", precision=precision, algo=algo, tol=1e-8, max_iter=20000)
             row = {"ms": statistics.mean(ms), "iterations": st.iterations, "refinements": st.refinements,
                    "max_rel_residual": st.max_rel_residual, "build_s": build_s}
             if precond == "ic0":
                 byts = algorithmic_bytes(info, st, 3, precision == "mixed")
                 row.update(algorithmic_bytes=byts, achieved_gbs=byts / (row["ms"] * 1e-3) / 1e9,
                            frac=byts / (row["ms"] * 1e-3) / 1e9 / peak, n_levels=info["n_levels"])
-            out[f"{precond}_{precision}"] = row
-        if precond == "ic0" and precision == "mixed":
+            key = f"{precond}_{precision}" if algo == "fused" else f"{precond}_level_scheduled_{precision}"
+            out[key] = row
+        if precond == "ic0" and precision == "mixed" and algo == "fused":
             out["n_free"], out["nnz_A"] = info["n_free"], info["nnz_A"]
     return out
 
@@ -748,10 +751,11 @@ def main():
     st_fp64 = one("fp64", stats=True, sv=solver_j)
     st_plain = one("fp64", "plain", stats=True, sv=solver_j)
     st_ic = one("mixed", stats=True, sv=solver_ic)
+    st_ic_ls = one("mixed", "classic", stats=True, sv=solver_ic)
     st_jac = one("mixed", stats=True, sv=solver_j)
     st_classic = one("mixed", "pipelined", stats=True, sv=solver_j)
     st_bss2 = one("mixed", "classic", stats=True)
-    for s in (st_mixed, st_fp64, st_plain, st_ic, st_jac, st_classic, st_bss2):
+    for s in (st_mixed, st_fp64, st_plain, st_ic, st_ic_ls, st_jac, st_classic, st_bss2):
         if s.status != 0:
             raise SystemExit(f"solve failed: status {s.status}")
 
@@ -783,6 +787,7 @@ def main():
     t_fp64 = timed("fp64", "fused", max(3, args.steps // 3), 2, sv=solver_j)
     t_plain = timed("fp64", "plain", 3, 1, sv=solver_j)
     t_ic = timed("mixed", "fused", max(3, args.steps // 3), 2, sv=solver_ic)
+    t_ic_ls = timed("mixed", "classic", max(3, args.steps // 3), 2, sv=solver_ic)
     t_jac = timed("mixed", "fused", max(3, args.steps // 3), 2, sv=solver_j)
     t_classic = timed("mixed", "pipelined", max(3, args.steps // 3), 2, sv=solver_j)
     t_bss2 = timed("mixed", "classic", max(3, args.steps // 3), 2)
@@ -824,6 +829,7 @@ def main():
     ms_plain = maxred(sum(t_plain) / len(t_plain))
     ms_e2e = maxred(sum(e2e_ms) / len(e2e_ms))
     ms_ic = maxred(sum(t_ic) / len(t_ic))
+    ms_ic_ls = maxred(sum(t_ic_ls) / len(t_ic_ls))
     ms_jac = maxred(sum(t_jac) / len(t_jac))
     ms_classic = maxred(sum(t_classic) / len(t_classic))
     ms_bss2 = maxred(sum(t_bss2) / len(t_bss2))
@@ -879,8 +885,14 @@ def main():
             "fp64_plain": {"solves_per_s": 1e3 / ms_plain, "ms": ms_plain, "iterations": st_plain.iterations,
                            "note": "Jacobi-PCG, one kernel per primitive, dots folded on the host each iteration"},
             "ic0_mixed": {"solves_per_s": 1e3 / ms_ic, "ms": ms_ic, "iterations": st_ic.iterations,
-                          "n_levels": info_ic["n_levels"],
-                          "note": "IC(0) in greedy-colour order, classic CG: 2 x n_levels team barriers per iteration"},
+                          "refinements": st_ic.refinements, "n_levels": info_ic["n_levels"],
+                          "note": "IC(0) in greedy-colour order, sweeps without grid barriers (values carry their "
+                                  "application number; block barriers per level), single-reduction CG: one grid "
+                                  "barrier per iteration"},
+            "ic0_level_scheduled_mixed": {"solves_per_s": 1e3 / ms_ic_ls, "ms": ms_ic_ls,
+                                          "iterations": st_ic_ls.iterations, "refinements": st_ic_ls.refinements,
+                                          "note": "the same handle on the level-scheduled kernel, classic CG: "
+                                                  "2 x n_levels grid barriers per iteration"},
             "jacobi_pipelined_mixed": {"solves_per_s": 1e3 / ms_classic, "ms": ms_classic,
                                        "iterations": st_classic.iterations, "refinements": st_classic.refinements,
                                        "note": "same kernel, pipelined CG in FP32 (one team barrier per iteration; not the default: its recurrences drift on ill-conditioned meshes)"},
