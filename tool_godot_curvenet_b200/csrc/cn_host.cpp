@@ -110,10 +110,35 @@ bool row_cached(const cn_system* S) {
   return !S->hsc && (S->opts.precond == CN_PRECOND_JACOBI || S->opts.precond == CN_PRECOND_BSSOR);
 }
 
+// Launch shape of an IC(0) solve: the handle's (explicit, tuned, or one
+// block for a small system), or, left automatic on a system of at least 1,024
+// free rows, a grid sized by the system and the kernel: about 600 rows a
+// block for the sweeps without grid barriers (at most 7/8 of the SMs; fewer
+// blocks keep more of a level's rows in each), about 120 for the
+// level-scheduled kernel (all SMs); 256 threads a block below 20,000 rows.
+// Measured on B200 across 2k-130k-row tori and cylinders: one block took
+// 1.3-5x longer than these grids from 2k rows on.
+void ic0_shape(const cn_system* S, const cn_solve_opts& o, int* grid, int* block) {
+  *grid = S->grid;
+  *block = S->block;
+  if (S->hsc || S->opts.precond != CN_PRECOND_IC0 || S->shape_set || S->opts.grid > 0 || S->opts.block > 0 ||
+      S->H.n < 1024)
+    return;
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, S->device);
+  const bool sync_free = o.precision == CN_PREC_MIXED && o.algo != CN_ALGO_CLASSIC;
+  const int per = sync_free ? 600 : 120;
+  const int cap = sync_free ? std::max(8, sms * 7 / 8) : sms;
+  *grid = std::min(cap, std::max(8, S->H.n / per));
+  *block = S->H.n >= 20000 ? 512 : 256;
+}
+
 // IC(0) in mixed precision on a multi-block grid runs the sweeps without
 // grid barriers (cn_icsf.cu); CLASSIC keeps the level-scheduled kernel
 bool icsf_path(const cn_system* S, const cn_solve_opts& o) {
-  return !S->hsc && S->opts.precond == CN_PRECOND_IC0 && o.precision == CN_PREC_MIXED && S->grid > 1 &&
+  int grid = 0, block = 0;
+  ic0_shape(S, o, &grid, &block);
+  return !S->hsc && S->opts.precond == CN_PRECOND_IC0 && o.precision == CN_PREC_MIXED && grid > 1 &&
          o.algo != CN_ALGO_CLASSIC && o.algo != CN_ALGO_PLAIN && S->H.nlev <= cn::icsf_max_levels();
 }
 
@@ -729,12 +754,13 @@ cn_status cn_solve_device(cn_handle S, int32_t k, const double* d_targets, doubl
     if (!stats) return CN_OK;
     return fill_stats(S, k, stats);
   }
-  int grid = S->grid;
+  int grid = S->grid, lblock = S->block;
+  ic0_shape(S, o, &grid, &lblock);
   // IC(0) in mixed precision on a multi-block grid: the sweeps without grid
   // barriers (tagged words) under the single-reduction CG; CLASSIC keeps the
   // level-scheduled kernel
   if (icsf_path(S, o)) {
-    const int block = std::min(S->block, 512);
+    const int block = std::min(lblock, 512);
     const int mg = cn::icsf_max_grid(k, block);
     if (mg <= 0) {
       set_err("the IC(0) solve does not fit on this device (block %d)", block);
@@ -752,9 +778,9 @@ cn_status cn_solve_device(cn_handle S, int32_t k, const double* d_targets, doubl
     return fill_stats(S, k, stats);
   }
   if (grid > 1) {
-    const int mg = cn::persistent_max_grid(o.precision, k, S->lanes, S->block);
+    const int mg = cn::persistent_max_grid(o.precision, k, S->lanes, lblock);
     if (mg <= 0) {
-      set_err("the persistent solve does not fit on this device (lanes %d, block %d)", S->lanes, S->block);
+      set_err("the persistent solve does not fit on this device (lanes %d, block %d)", S->lanes, lblock);
       return CN_CUDA_ERROR;
     }
     grid = std::min(std::min(grid, mg), S->max_grid_alloc);
@@ -767,7 +793,7 @@ cn_status cn_solve_device(cn_handle S, int32_t k, const double* d_targets, doubl
   }
   CN_CUDA(cudaMemsetAsync(S->d_ctl, 0, sizeof(Control), S->stream));
   CN_CUDA(cudaEventRecord(S->ev0, S->stream));
-  CN_CUDA(cn::launch_persistent_solve(a, o.precision, k, S->lanes, S->block, grid, S->stream));
+  CN_CUDA(cn::launch_persistent_solve(a, o.precision, k, S->lanes, lblock, grid, S->stream));
   CN_CUDA(cudaEventRecord(S->ev1, S->stream));
   S->have_solution = true;
   if (!stats) return CN_OK;
