@@ -113,11 +113,12 @@ bool row_cached(const cn_system* S) {
 // Launch shape of an IC(0) solve: the handle's (explicit, tuned, or one
 // block for a small system), or, left automatic on a system of at least 1,024
 // free rows, a grid sized by the system and the kernel: about 600 rows a
-// block for the sweeps without grid barriers (at most 7/8 of the SMs; fewer
-// blocks keep more of a level's rows in each), about 120 for the
-// level-scheduled kernel (all SMs); 256 threads a block below 20,000 rows.
-// Measured on B200 across 2k-130k-row tori and cylinders: one block took
-// 1.3-5x longer than these grids from 2k rows on.
+// block for the sweeps without grid barriers (below 300,000 rows at most 7/8
+// of the SMs: fewer blocks keep more of a level's rows in each; the
+// 1.05M-row torus wants every SM), about 120 for the level-scheduled kernel
+// (all SMs); 256 threads a block below 20,000 rows.  Measured on B200 across
+// 2k-1M-row tori and cylinders: one block took 1.3-5x longer than these
+// grids from 2k rows on.
 void ic0_shape(const cn_system* S, const cn_solve_opts& o, int* grid, int* block) {
   *grid = S->grid;
   *block = S->block;
@@ -128,7 +129,7 @@ void ic0_shape(const cn_system* S, const cn_solve_opts& o, int* grid, int* block
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, S->device);
   const bool sync_free = o.precision == CN_PREC_MIXED && o.algo != CN_ALGO_CLASSIC;
   const int per = sync_free ? 600 : 120;
-  const int cap = sync_free ? std::max(8, sms * 7 / 8) : sms;
+  const int cap = sync_free && S->H.n < 300000 ? std::max(8, sms * 7 / 8) : sms;
   *grid = std::min(cap, std::max(8, S->H.n / per));
   *block = S->H.n >= 20000 ? 512 : 256;
 }
