@@ -86,3 +86,19 @@ def test_single_reduction_on_ic0_needs_mixed_precision():
     with CutMeshSolver(pos, tris, h, precond="ic0") as s:
         with pytest.raises(CnError):
             s.solve(t[:, :3], mode="deform", precision="fp64", algo="single")
+
+
+@pytest.mark.parametrize("kw", [{"grid": 8, "block": 256}, {"grid": 148, "block": 512}, {}])
+def test_sync_free_ic0_repeats_bit_for_bit(kw):
+    """Twenty solves of one system on one handle give the same bits and the
+    same iteration count every time: every value a sweep reads is the one of
+    the current application (a stale or torn read would change the result of
+    some solve), and the reductions sum in a fixed order."""
+    pos, tris, h, t = workload("torus_small")
+    t = t[:, :3]
+    with CutMeshSolver(pos, tris, h, precond="ic0", **kw) as s:
+        r0 = s.solve(t, mode="deform", precision="mixed", tol=1e-8)
+        for _ in range(19):
+            r = s.solve(t, mode="deform", precision="mixed", tol=1e-8)
+            assert r.iterations == r0.iterations and r.refinements == r0.refinements
+            assert np.array_equal(r.x, r0.x)
