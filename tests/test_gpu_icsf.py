@@ -6,11 +6,11 @@ single-reduction CG.
 Reference semantics: SparseLinAlg.lean:104-163 (PCG) with the IC(0) apply of
 IncompleteCholesky.lean:83-101.  Checked against the oracle's FP64 IC(0)-PCG
 to 1e-13 and against the level-scheduled kernel on the same handle
-(algo="classic").  Bars: mixed precision stopped at 1e-8 within 1e-6 of the
-oracle (the mixed bar of the other parity tests); mixed precision driven to
-1e-11 by the FP64 refinement within 1e-8; the iteration count within 10 % (or
-8) of the level-scheduled kernel's (same preconditioner, same stopping rule,
-a different CG recurrence)."""
+(algo="classic").  Bars: FP64 to 1e-13 within 1e-9 of the oracle; mixed
+precision stopped at 1e-8 within 1e-6 (the mixed bar of the other parity
+tests); mixed precision driven to 1e-11 by the FP64 refinement within 1e-8;
+the iteration count within 10 % (or 8) of the level-scheduled kernel's (same
+preconditioner, same stopping rule, a different CG recurrence)."""
 import numpy as np
 import pytest
 
@@ -20,6 +20,7 @@ from tool_godot_curvenet_b200 import _lib as L
 
 pytestmark = pytest.mark.gpu
 
+FP64_TOL = 1e-9
 MIXED_TOL = 1e-6
 TIGHT_TOL = 1e-8
 
@@ -50,8 +51,13 @@ def test_sync_free_ic0_matches_oracle_and_level_scheduled(name, kw, k, oracle):
         rs = s.solve(t, mode="harmonic", precision="mixed", tol=1e-8, max_iter=20000, algo="single")
         rt = s.solve(t, mode="harmonic", precision="mixed", tol=1e-11, max_iter=20000)
         rc = s.solve(t, mode="harmonic", precision="mixed", tol=1e-8, max_iter=20000, algo="classic")
-    for r in (rf, rs, rt, rc):
+        # FP64 takes the sweeps without grid barriers by default from 50,000
+        # rows on; SINGLE asks for them on any size
+        r64 = s.solve(t, mode="harmonic", precision="fp64", tol=1e-13, max_iter=20000, algo="single")
+    for r in (rf, rs, rt, rc, r64):
         assert r.status == L.CN_OK
+    assert np.all(r64.rel_residual <= 1e-13)
+    assert rel_err(r64.x, xo) <= FP64_TOL
     assert np.all(rf.rel_residual <= 1e-8) and np.all(rt.rel_residual <= 1e-11)
     assert rel_err(rf.x, xo) <= MIXED_TOL
     assert rel_err(rt.x, xo) <= TIGHT_TOL
@@ -81,11 +87,23 @@ def test_sync_free_ic0_deform_mode_repeatable(oracle):
         assert np.array_equal(r.x, rs[0].x)
 
 
-def test_single_reduction_on_ic0_needs_mixed_precision():
+def test_sync_free_ic0_fp64_matches_level_scheduled(oracle):
+    """FP64 (two words a value: the high and the low half, each with the
+    application number; SINGLE asks for it below the 50,000 rows where FP64
+    takes it by default) against the level-scheduled FP64 kernel and the
+    oracle, deform mode on the 18k-vertex torus, twice (bit for bit)."""
     pos, tris, h, t = workload("torus_mid")
+    t = t[:, :3]
+    st, xo, _, _ = oracle.System(pos, tris, h).solve(t, mode=1, tol=1e-13)
     with CutMeshSolver(pos, tris, h, precond="ic0") as s:
-        with pytest.raises(CnError):
-            s.solve(t[:, :3], mode="deform", precision="fp64", algo="single")
+        rs = s.solve(t, mode="deform", precision="fp64", tol=1e-13, max_iter=20000, algo="single")
+        rs2 = s.solve(t, mode="deform", precision="fp64", tol=1e-13, max_iter=20000, algo="single")
+        rc = s.solve(t, mode="deform", precision="fp64", tol=1e-13, max_iter=20000, algo="classic")
+    for r in (rs, rs2, rc):
+        assert r.status == L.CN_OK and np.all(r.rel_residual <= 1e-13)
+        assert rel_err(r.x, xo) <= FP64_TOL
+    assert np.array_equal(rs.x, rs2.x)
+    assert abs(rs.iterations - rc.iterations) <= max(8, 0.1 * rc.iterations)
 
 
 @pytest.mark.parametrize("kw", [{"grid": 8, "block": 256}, {"grid": 148, "block": 512}, {}])

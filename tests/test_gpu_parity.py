@@ -443,9 +443,6 @@ def test_single_reduction_form_matches_oracle(name, precond, k, oracle):
 
 def test_single_reduction_rejected_on_level_scheduled_handles():
     pos, tris, h, t = workload("c1")
-    with CutMeshSolver(pos, tris, h, precond="ic0") as s:
-        with pytest.raises(CnError):
-            s.solve(t, mode="deform", precision="fp64", algo="single")
     with CutMeshSolver(pos, tris, h, precond="hsc") as s:
         with pytest.raises(CnError):
             s.solve(t, mode="deform", precision="mixed", algo="single")

@@ -110,6 +110,18 @@ bool row_cached(const cn_system* S) {
   return !S->hsc && (S->opts.precond == CN_PRECOND_JACOBI || S->opts.precond == CN_PRECOND_BSSOR);
 }
 
+// The IC(0) solve without grid barriers in the sweeps (cn_icsf.cu) is used
+// for IC(0) handles unless CLASSIC asks for the level-scheduled kernel: in
+// mixed precision always, in FP64 from 50,000 free rows on or when SINGLE
+// asks for it (on B200 the FP64 form, two words a value, beat the
+// level-scheduled kernel on the 130k-row torus by 9 % and lost by 3-12 % on
+// 5k-18k-row meshes).
+bool icsf_wanted(const cn_system* S, const cn_solve_opts& o) {
+  return !S->hsc && S->opts.precond == CN_PRECOND_IC0 && o.algo != CN_ALGO_CLASSIC && o.algo != CN_ALGO_PLAIN &&
+         S->H.nlev <= cn::icsf_max_levels() &&
+         (o.precision == CN_PREC_MIXED || S->H.n >= 50000 || o.algo == CN_ALGO_SINGLE);
+}
+
 // Launch shape of an IC(0) solve: the handle's (explicit, tuned, or one
 // block for a small system), or, left automatic on a system of at least 1,024
 // free rows, a grid sized by the system and the kernel: about 600 rows a
@@ -127,20 +139,18 @@ void ic0_shape(const cn_system* S, const cn_solve_opts& o, int* grid, int* block
     return;
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, S->device);
-  const bool sync_free = o.precision == CN_PREC_MIXED && o.algo != CN_ALGO_CLASSIC;
+  const bool sync_free = icsf_wanted(S, o);
   const int per = sync_free ? 600 : 120;
   const int cap = sync_free && S->H.n < 300000 ? std::max(8, sms * 7 / 8) : sms;
   *grid = std::min(cap, std::max(8, S->H.n / per));
   *block = S->H.n >= 20000 ? 512 : 256;
 }
 
-// IC(0) in mixed precision on a multi-block grid runs the sweeps without
-// grid barriers (cn_icsf.cu); CLASSIC keeps the level-scheduled kernel
+// ... on a multi-block grid
 bool icsf_path(const cn_system* S, const cn_solve_opts& o) {
   int grid = 0, block = 0;
   ic0_shape(S, o, &grid, &block);
-  return !S->hsc && S->opts.precond == CN_PRECOND_IC0 && o.precision == CN_PREC_MIXED && grid > 1 &&
-         o.algo != CN_ALGO_CLASSIC && o.algo != CN_ALGO_PLAIN && S->H.nlev <= cn::icsf_max_levels();
+  return icsf_wanted(S, o) && grid > 1;
 }
 
 const char* kStatusText[] = {"ok", "max_iter", "singular_component", "nonpositive_pivot",
@@ -612,9 +622,8 @@ cn_status cn_solve_device(cn_handle S, int32_t k, const double* d_targets, doubl
     set_err("the pipelined form needs the Jacobi preconditioner, or block SSOR in mixed precision");
     return CN_BAD_INPUT;
   }
-  if (o.algo == CN_ALGO_SINGLE && !row_cached(S) &&
-      !(S->opts.precond == CN_PRECOND_IC0 && !S->hsc && mixed)) {
-    set_err("the single-reduction form runs on Jacobi and block SSOR handles, and on IC(0) handles in mixed precision");
+  if (o.algo == CN_ALGO_SINGLE && !row_cached(S) && !(S->opts.precond == CN_PRECOND_IC0 && !S->hsc)) {
+    set_err("the single-reduction form runs on Jacobi, block SSOR and IC(0) handles");
     return CN_BAD_INPUT;
   }
   if (row_cached(S)) {
@@ -757,12 +766,12 @@ cn_status cn_solve_device(cn_handle S, int32_t k, const double* d_targets, doubl
   }
   int grid = S->grid, lblock = S->block;
   ic0_shape(S, o, &grid, &lblock);
-  // IC(0) in mixed precision on a multi-block grid: the sweeps without grid
-  // barriers (tagged words) under the single-reduction CG; CLASSIC keeps the
-  // level-scheduled kernel
+  // IC(0) on a multi-block grid: the sweeps without grid barriers (tagged
+  // words) under the single-reduction CG (icsf_wanted: mixed precision, or
+  // FP64 on a large system); otherwise the level-scheduled kernel
   if (icsf_path(S, o)) {
     const int block = std::min(lblock, 512);
-    const int mg = cn::icsf_max_grid(k, block);
+    const int mg = cn::icsf_max_grid(o.precision, k, block);
     if (mg <= 0) {
       set_err("the IC(0) solve does not fit on this device (block %d)", block);
       return CN_CUDA_ERROR;
@@ -772,7 +781,7 @@ cn_status cn_solve_device(cn_handle S, int32_t k, const double* d_targets, doubl
     a.m1 = S->d_m[1];
     CN_CUDA(cudaMemsetAsync(S->d_ctl, 0, sizeof(Control), S->stream));
     CN_CUDA(cudaEventRecord(S->ev0, S->stream));
-    CN_CUDA(cn::launch_icsf_solve(a, k, block, grid, S->stream));
+    CN_CUDA(cn::launch_icsf_solve(a, o.precision, k, block, grid, S->stream));
     CN_CUDA(cudaEventRecord(S->ev1, S->stream));
     S->have_solution = true;
     if (!stats) return CN_OK;

@@ -60,16 +60,6 @@ using namespace pcg;
 
 constexpr int kIcsfMaxLev = 256;
 
-// Words of a row: K columns padded to an even count (whole 16-byte pairs).
-template <int K>
-struct TRow {
-  static constexpr int W = (K + 1) & ~1;
-};
-
-__device__ __forceinline__ unsigned long long tag_word(float v, unsigned app) {
-  return ((unsigned long long)app << 32) | (unsigned long long)__float_as_uint(v);
-}
-
 __device__ __forceinline__ void ld_pair(const unsigned long long* p, unsigned long long& a, unsigned long long& b) {
   asm volatile("ld.relaxed.gpu.global.v2.u64 {%0, %1}, [%2];" : "=l"(a), "=l"(b) : "l"(p));
 }
@@ -78,16 +68,67 @@ __device__ __forceinline__ void st_pair(unsigned long long* p, unsigned long lon
   asm volatile("st.relaxed.gpu.global.v2.u64 [%0], {%1, %2};" ::"l"(p), "l"(a), "l"(b) : "memory");
 }
 
+__device__ __forceinline__ unsigned long long tag_bits(unsigned bits, unsigned app) {
+  return ((unsigned long long)app << 32) | (unsigned long long)bits;
+}
+
+// The words of a row.  FP32: one word per column (value bits, number),
+// K padded to an even count so a row is whole 16-byte pairs.  FP64: two
+// words per column, the high and the low half of the value each with the
+// number; a reader takes a column when both carry the current number (each
+// half is written once per application, so both then come from it).
+template <typename T, int K>
+struct Words;
+
 template <int K>
-__device__ __forceinline__ void publish(unsigned long long* words, int row, const float (&v)[K], unsigned app) {
-  constexpr int W = TRow<K>::W;
-  unsigned long long* p = words + (size_t)row * W;
+struct Words<float, K> {
+  static constexpr int W = (K + 1) & ~1;  // words of a row
+  static constexpr int N = W;             // words read
+  static constexpr int R = K;             // words whose numbers are checked
+  __device__ __forceinline__ static void load(const unsigned long long* p, unsigned long long (&x)[N]) {
 #pragma unroll
-  for (int i = 0; i < W / 2; ++i) {
-    const unsigned long long a = tag_word(2 * i < K ? v[2 * i] : 0.f, app);
-    const unsigned long long b = tag_word(2 * i + 1 < K ? v[2 * i + 1] : 0.f, app);
-    st_pair(p + 2 * i, a, b);
+    for (int i = 0; i < W; i += 2) ld_pair(p + i, x[i], x[i + 1]);
   }
+  __device__ __forceinline__ static float value(const unsigned long long (&x)[N], int c) { return __uint_as_float((unsigned)x[c]); }
+  __device__ __forceinline__ static void publish(unsigned long long* p, const float (&v)[K], unsigned app) {
+#pragma unroll
+    for (int i = 0; i < W / 2; ++i)
+      st_pair(p + 2 * i, tag_bits(__float_as_uint(2 * i < K ? v[2 * i] : 0.f), app),
+              tag_bits(__float_as_uint(2 * i + 1 < K ? v[2 * i + 1] : 0.f), app));
+  }
+};
+
+template <int K>
+struct Words<double, K> {
+  static constexpr int W = 2 * K;
+  static constexpr int N = 2 * K;
+  static constexpr int R = 2 * K;
+  __device__ __forceinline__ static void load(const unsigned long long* p, unsigned long long (&x)[N]) {
+#pragma unroll
+    for (int c = 0; c < K; ++c) ld_pair(p + 2 * c, x[2 * c], x[2 * c + 1]);
+  }
+  __device__ __forceinline__ static double value(const unsigned long long (&x)[N], int c) {
+    return __hiloint2double((int)(unsigned)x[2 * c], (int)(unsigned)x[2 * c + 1]);
+  }
+  __device__ __forceinline__ static void publish(unsigned long long* p, const double (&v)[K], unsigned app) {
+#pragma unroll
+    for (int c = 0; c < K; ++c)
+      st_pair(p + 2 * c, tag_bits((unsigned)__double2hiint(v[c]), app), tag_bits((unsigned)__double2loint(v[c]), app));
+  }
+};
+
+template <typename T, int K>
+__device__ __forceinline__ void publish(unsigned long long* words, int row, const T (&v)[K], unsigned app) {
+  Words<T, K>::publish(words + (size_t)row * Words<T, K>::W, v, app);
+}
+
+// the first R words of x carry `app`
+template <int R, int N>
+__device__ __forceinline__ bool words_ready(const unsigned long long (&x)[N], unsigned app) {
+  bool ok = true;
+#pragma unroll
+  for (int i = 0; i < R; ++i) ok = ok && (unsigned)(x[i] >> 32) == app;
+  return ok;
 }
 
 // The bounded wait of one thread in one phase.
@@ -122,45 +163,41 @@ struct Spin {
 // every word read until it carries `app`.  U entries at a time: their indices
 // and values, then all their words, then the waits and the multiply-adds in
 // entry order.
-template <int K, int U>
-__device__ __forceinline__ void gather_tagged(int e0, int e1, const int* __restrict__ col,
-                                              const float* __restrict__ val, const unsigned long long* words,
-                                              unsigned app, Spin& sp, float (&acc)[K]) {
-  constexpr int W = TRow<K>::W;
+template <typename T, int K, int U>
+__device__ __forceinline__ void gather_tagged(int e0, int e1, const int* __restrict__ col, const T* __restrict__ val,
+                                              const unsigned long long* words, unsigned app, Spin& sp,
+                                              T (&acc)[K]) {
+  using Wd = Words<T, K>;
+  constexpr int W = Wd::W, N = Wd::N;
 #pragma unroll
-  for (int c = 0; c < K; ++c) acc[c] = 0.f;
+  for (int c = 0; c < K; ++c) acc[c] = (T)0;
   for (int e = e0; e < e1; e += U) {
     int j[U];
-    float v[U];
+    T v[U];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       const bool ok = e + u < e1;
       j[u] = ok ? __ldg(col + e + u) : -1;
-      v[u] = ok ? __ldg(val + e + u) : 0.f;
+      v[u] = ok ? __ldg(val + e + u) : (T)0;
     }
-    unsigned long long x[U][W];
+    unsigned long long x[U][N];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       if (j[u] >= 0) {
-#pragma unroll
-        for (int i = 0; i < W / 2; ++i) ld_pair(words + (size_t)j[u] * W + 2 * i, x[u][2 * i], x[u][2 * i + 1]);
+        Wd::load(words + (size_t)j[u] * W, x[u]);
       } else {
 #pragma unroll
-        for (int i = 0; i < W; ++i) x[u][i] = (unsigned long long)app << 32;
+        for (int i = 0; i < N; ++i) x[u][i] = (unsigned long long)app << 32;  // no entry: ready, value 0
       }
     }
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       for (;;) {
-        bool ready = true;
-#pragma unroll
-        for (int c = 0; c < K; ++c) ready = ready && (unsigned)(x[u][c] >> 32) == app;
-        if (ready || !sp.poll()) break;
-#pragma unroll
-        for (int i = 0; i < W / 2; ++i) ld_pair(words + (size_t)j[u] * W + 2 * i, x[u][2 * i], x[u][2 * i + 1]);
+        if (words_ready<Wd::R>(x[u], app) || !sp.poll()) break;
+        Wd::load(words + (size_t)j[u] * W, x[u]);
       }
 #pragma unroll
-      for (int c = 0; c < K; ++c) acc[c] += v[u] * __uint_as_float((unsigned)x[u][c]);
+      for (int c = 0; c < K; ++c) acc[c] += v[u] * Wd::value(x[u], c);
     }
   }
 }
@@ -213,27 +250,28 @@ __device__ void team_sum_wide(const double* part, int size, double* red, double*
   block_reduce_store<V>(v, red, sum);
 }
 
-template <int K>
+template <typename T, int K>
 __global__ void __launch_bounds__(512) k_icsf(SolveArgs a) {
   __shared__ IcsfSmem<K> s;
   GridTeam team{a.ctl, a.timeout_ns, 0u};
-  const float* Aval = (const float*)a.A_val;
-  const float* Lval = (const float*)a.L_val;
-  const float* Uval = (const float*)a.U_val;
-  const float* dinv = (const float*)a.dinv;
-  float* r = (float*)a.r;
-  float* u = (float*)a.z;   // M^-1 r of the own rows
-  float* w = (float*)a.y;   // A u of the own rows
-  float* p = (float*)a.p0;
-  float* sv = (float*)a.Ap; // s = A p
-  float* xin = (float*)a.xin;
+  const T* Aval = (const T*)a.A_val;
+  const T* Lval = (const T*)a.L_val;
+  const T* Uval = (const T*)a.U_val;
+  const T* dinv = (const T*)a.dinv;
+  T* r = (T*)a.r;
+  T* u = (T*)a.z;   // M^-1 r of the own rows
+  T* w = (T*)a.y;   // A u of the own rows
+  T* p = (T*)a.p0;
+  T* sv = (T*)a.Ap; // s = A p
+  T* xin = (T*)a.xin;
   unsigned long long* yw = (unsigned long long*)a.m0;  // forward-sweep words
   unsigned long long* uw = (unsigned long long*)a.m1;  // backward-sweep words
-  constexpr int W = TRow<K>::W;
+  using Wd = Words<T, K>;
+  constexpr int W = Wd::W;
   // entries whose words are in flight together: rows of L and U hold ~3
-  // entries, rows of A ~7
-  constexpr int kUL = K <= 3 ? 4 : 2;
-  constexpr int kUA = K <= 3 ? 8 : 2;
+  // entries, rows of A ~7 (FP64: twice the words an entry)
+  constexpr int kUL = K <= 3 && sizeof(T) == 4 ? 4 : 2;
+  constexpr int kUA = K <= 3 ? (sizeof(T) == 4 ? 8 : 4) : 2;
   const int n = a.n, nlev = a.nlev;
   const int row0 = blockIdx.x * blockDim.x + threadIdx.x, rstride = gridDim.x * blockDim.x;
   const int tsize = gridDim.x;
@@ -315,8 +353,8 @@ __global__ void __launch_bounds__(512) k_icsf(SolveArgs a) {
 #pragma unroll
         for (int c = 0; c < K; ++c) {
           const double rv = a.b64[(size_t)row * K + c] - acc[c];
-          r[(size_t)row * K + c] = (float)rv;
-          xin[(size_t)row * K + c] = 0.f;
+          r[(size_t)row * K + c] = (T)rv;
+          xin[(size_t)row * K + c] = (T)0;
           rr[c] += rv * rv;
         }
       }
@@ -353,11 +391,11 @@ __global__ void __launch_bounds__(512) k_icsf(SolveArgs a) {
     int it = 0;
     bool first = true;
     for (;;) {
-      float al[K], be[K];
+      T al[K], be[K];
 #pragma unroll
       for (int c = 0; c < K; ++c) {
-        al[c] = (float)s.alpha[c];
-        be[c] = (float)s.beta[c];
+        al[c] = (T)s.alpha[c];
+        be[c] = (T)s.beta[c];
       }
       ++app;
       sp.n = 0;
@@ -369,15 +407,15 @@ __global__ void __launch_bounds__(512) k_icsf(SolveArgs a) {
         const bool top = l == nlev - 1;
         for (int q = lr.q0; q < lr.cnt; q += blockDim.x) {
           const int row = lr.base + q;
-          float rv[K];
+          T rv[K];
           if (!first) {
 #pragma unroll
             for (int c = 0; c < K; ++c) {
               const size_t ix = (size_t)row * K + c;
               // beta = 0 (an inner solve's first update, or an inactive
               // column): p = u, s = w, whatever the previous p, s hold
-              const float pv = be[c] == 0.f ? u[ix] : u[ix] + be[c] * p[ix];
-              const float svv = be[c] == 0.f ? w[ix] : w[ix] + be[c] * sv[ix];
+              const T pv = be[c] == (T)0 ? u[ix] : u[ix] + be[c] * p[ix];
+              const T svv = be[c] == (T)0 ? w[ix] : w[ix] + be[c] * sv[ix];
               p[ix] = pv;
               sv[ix] = svv;
               xin[ix] += al[c] * pv;
@@ -388,22 +426,22 @@ __global__ void __launch_bounds__(512) k_icsf(SolveArgs a) {
 #pragma unroll
             for (int c = 0; c < K; ++c) rv[c] = r[(size_t)row * K + c];
           }
-          float acc[K];
-          gather_tagged<K, kUL>(a.L_ptr[row], a.L_ptr[row + 1], a.L_col, Lval, yw, app, sp, acc);
-          const float di = dinv[row];
-          float yv[K];
+          T acc[K];
+          gather_tagged<T, K, kUL>(a.L_ptr[row], a.L_ptr[row + 1], a.L_col, Lval, yw, app, sp, acc);
+          const T di = dinv[row];
+          T yv[K];
 #pragma unroll
           for (int c = 0; c < K; ++c) yv[c] = (rv[c] - acc[c]) * di;
           if (top) {
-            float uv[K];
+            T uv[K];
 #pragma unroll
             for (int c = 0; c < K; ++c) {
               uv[c] = yv[c] * di;
               u[(size_t)row * K + c] = uv[c];
             }
-            publish<K>(uw, row, uv, app);
+            publish<T, K>(uw, row, uv, app);
           } else {
-            publish<K>(yw, row, yv, app);
+            publish<T, K>(yw, row, yv, app);
           }
         }
         // the block's rows of this level are published before any of its
@@ -416,20 +454,19 @@ __global__ void __launch_bounds__(512) k_icsf(SolveArgs a) {
         const LevelRows lr = level_rows(s.lev, s.loff, l);
         for (int q = lr.q0; q < lr.cnt; q += blockDim.x) {
           const int row = lr.base + q;
-          // the row's own y (this thread's word) before the waits
-          unsigned long long yx[W];
-#pragma unroll
-          for (int i = 0; i < W / 2; ++i) ld_pair(yw + (size_t)row * W + 2 * i, yx[2 * i], yx[2 * i + 1]);
-          const float di = dinv[row];
-          float acc[K];
-          gather_tagged<K, kUL>(a.U_ptr[row], a.U_ptr[row + 1], a.U_col, Uval, uw, app, sp, acc);
-          float uv[K];
+          // the row's own y (this thread's words) before the waits
+          unsigned long long yx[Wd::N];
+          Wd::load(yw + (size_t)row * W, yx);
+          const T di = dinv[row];
+          T acc[K];
+          gather_tagged<T, K, kUL>(a.U_ptr[row], a.U_ptr[row + 1], a.U_col, Uval, uw, app, sp, acc);
+          T uv[K];
 #pragma unroll
           for (int c = 0; c < K; ++c) {
-            uv[c] = (__uint_as_float((unsigned)yx[c]) - acc[c]) * di;
+            uv[c] = (Wd::value(yx, c) - acc[c]) * di;
             u[(size_t)row * K + c] = uv[c];
           }
-          publish<K>(uw, row, uv, app);
+          publish<T, K>(uw, row, uv, app);
         }
         __syncthreads();
       }
@@ -441,8 +478,8 @@ __global__ void __launch_bounds__(512) k_icsf(SolveArgs a) {
         const LevelRows lr = level_rows(s.lev, s.loff, l);
         for (int q = lr.q0; q < lr.cnt; q += blockDim.x) {
           const int row = lr.base + q;
-          float acc[K];
-          gather_tagged<K, kUA>(a.A_ptr[row], a.A_ptr[row + 1], a.A_col, Aval, uw, app, sp, acc);
+          T acc[K];
+          gather_tagged<T, K, kUA>(a.A_ptr[row], a.A_ptr[row + 1], a.A_col, Aval, uw, app, sp, acc);
 #pragma unroll
           for (int c = 0; c < K; ++c) {
             const size_t ix = (size_t)row * K + c;
@@ -542,19 +579,19 @@ done:
   }
 }
 
-template <int K>
+template <typename T, int K>
 cudaError_t launch_k(const SolveArgs& a, int block, int grid, cudaStream_t st) {
   SolveArgs copy = a;
   void* args[] = {&copy};
-  return cudaLaunchCooperativeKernel((const void*)k_icsf<K>, dim3(grid), dim3(block), args, 0, st);
+  return cudaLaunchCooperativeKernel((const void*)k_icsf<T, K>, dim3(grid), dim3(block), args, 0, st);
 }
 
-template <int K>
+template <typename T, int K>
 int max_grid_k(int block) {
   int dev = 0, sms = 0, per = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_icsf<K>, block, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_icsf<T, K>, block, 0);
   return sms * per;
 }
 
@@ -562,16 +599,26 @@ int max_grid_k(int block) {
 
 int icsf_max_levels() { return kIcsfMaxLev; }
 
-cudaError_t launch_icsf_solve(const SolveArgs& a, int K, int block, int grid, cudaStream_t s) {
+cudaError_t launch_icsf_solve(const SolveArgs& a, int precision, int K, int block, int grid, cudaStream_t s) {
   if (a.nlev > kIcsfMaxLev || grid < 1 || block > 512) return cudaErrorInvalidValue;
-  if (K == 1) return launch_k<1>(a, block, grid, s);
-  if (K == 3) return launch_k<3>(a, block, grid, s);
+  if (precision == CN_PREC_MIXED) {
+    if (K == 1) return launch_k<float, 1>(a, block, grid, s);
+    if (K == 3) return launch_k<float, 3>(a, block, grid, s);
+  } else {
+    if (K == 1) return launch_k<double, 1>(a, block, grid, s);
+    if (K == 3) return launch_k<double, 3>(a, block, grid, s);
+  }
   return cudaErrorInvalidValue;
 }
 
-int icsf_max_grid(int K, int block) {
-  if (K == 1) return max_grid_k<1>(block);
-  if (K == 3) return max_grid_k<3>(block);
+int icsf_max_grid(int precision, int K, int block) {
+  if (precision == CN_PREC_MIXED) {
+    if (K == 1) return max_grid_k<float, 1>(block);
+    if (K == 3) return max_grid_k<float, 3>(block);
+  } else {
+    if (K == 1) return max_grid_k<double, 1>(block);
+    if (K == 3) return max_grid_k<double, 3>(block);
+  }
   return 0;
 }
 

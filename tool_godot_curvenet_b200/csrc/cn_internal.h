@@ -130,13 +130,13 @@ cudaError_t launch_persistent_solve(const SolveArgs& a, int precision, int K, in
 // Largest co-resident grid of the persistent solve for this configuration.
 int persistent_max_grid(int precision, int K, int lanes, int block);
 
-// The mixed-precision IC(0) solve with synchronisation-free sweeps
-// (cn_icsf.cu): tagged words of the forward and backward sweeps in a.m0 and
-// a.m1 ([rows][round_up(K, 2)] 64-bit words each); K = 1 or 3; at most
-// icsf_max_levels() levels; a cooperative launch of `grid` blocks of `block`
-// threads (block <= 512).
-cudaError_t launch_icsf_solve(const SolveArgs& a, int K, int block, int grid, cudaStream_t s);
-int icsf_max_grid(int K, int block);
+// The IC(0) solve with synchronisation-free sweeps (cn_icsf.cu): tagged
+// words of the forward and backward sweeps in a.m0 and a.m1 (FP32:
+// round_up(K, 2) 64-bit words a row, FP64: 2K); precision CN_PREC_MIXED
+// (FP32 inner solve) or CN_PREC_FP64; K = 1 or 3; at most icsf_max_levels()
+// levels; a cooperative launch of `grid` blocks of `block` threads (block <= 512).
+cudaError_t launch_icsf_solve(const SolveArgs& a, int precision, int K, int block, int grid, cudaStream_t s);
+int icsf_max_grid(int precision, int K, int block);
 int icsf_max_levels();
 
 // dst[r * kd + d0 + c] = src[r * ks + s0 + c] for r < rows, c < ncols (cn_ddm.cu).
