@@ -1,5 +1,6 @@
 // cn_icsf.cu -- IC(0)-preconditioned CG with synchronisation-free triangular
-// sweeps (sm_100a): the mixed-precision solve of an IC(0) handle.
+// sweeps (sm_100a): the solve of an IC(0) handle in mixed precision (FP32
+// inner solve) and, for large systems, in FP64.
 //
 // Same problem, right-hand sides, FP64 residual refinement and output as the
 // level-scheduled persistent solve (cn_pcg.cu), and the same preconditioner:
@@ -11,7 +12,8 @@
 // levels per iteration).  Here no grid barrier separates them: every value a
 // sweep publishes is stored together with the number of the preconditioner
 // application it belongs to, one 64-bit word per column (the FP32 bits in
-// the low half, the application number in the high half), and a row's
+// the low half, the application number in the high half; FP64: two words,
+// one per half of the double), and a row's
 // thread reads its neighbours' words until every one carries the current
 // number.  A naturally aligned 64-bit access is single-copy atomic, so a word
 // with the current number holds the current value; no fence or flag orders
