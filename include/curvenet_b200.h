@@ -74,8 +74,8 @@ enum { CN_MODE_HARMONIC = 0, CN_MODE_DEFORM = 1, CN_MODE_RHS = 2 };
  * drift on ill-conditioned meshes).  With block SSOR: in mixed precision
  * the pipelined CG keeping u = M^-1 r and q = M^-1 s by recurrence, inner
  * solves of at most 1e-3 restarted by the FP64 refinement, with the same
- * fall-back; in FP64 the two-reduction CG.  With IC(0) on a multi-block
- * grid, in mixed precision and in FP64 from 50,000 free rows on: the
+ * fall-back; in FP64 the two-reduction CG.  With IC(0) and k = 1 or 3 on a
+ * multi-block grid, in mixed precision and in FP64 from 50,000 free rows on: the
  * triangular sweeps without grid barriers (every published value carries
  * the number of the preconditioner application it belongs to; block
  * barriers between levels) under the single-reduction CG, one grid barrier
@@ -88,7 +88,7 @@ enum { CN_MODE_HARMONIC = 0, CN_MODE_DEFORM = 1, CN_MODE_RHS = 2 };
  * & Gear: alpha and beta from one reduction of (r, z), (z, A z), ||r||^2)
  * on the row-cached kernel, Jacobi or block SSOR: one grid barrier per
  * iteration, z exchanged with the neighbour blocks only; on IC(0) handles
- * the sweeps without grid barriers in either precision. */
+ * (k = 1, 3) the sweeps without grid barriers in either precision. */
 enum { CN_ALGO_FUSED = 0, CN_ALGO_PLAIN = 1, CN_ALGO_CLASSIC = 2, CN_ALGO_PIPELINED = 3, CN_ALGO_SINGLE = 4 };
 
 typedef struct {

@@ -111,14 +111,16 @@ bool row_cached(const cn_system* S) {
 }
 
 // The IC(0) solve without grid barriers in the sweeps (cn_icsf.cu) is used
-// for IC(0) handles unless CLASSIC asks for the level-scheduled kernel: in
-// mixed precision always, in FP64 from 50,000 free rows on or when SINGLE
-// asks for it (on B200 the FP64 form, two words a value, beat the
-// level-scheduled kernel on the 130k-row torus by 9 % and lost by 3-12 % on
-// 5k-18k-row meshes).
-bool icsf_wanted(const cn_system* S, const cn_solve_opts& o) {
-  return !S->hsc && S->opts.precond == CN_PRECOND_IC0 && o.algo != CN_ALGO_CLASSIC && o.algo != CN_ALGO_PLAIN &&
-         S->H.nlev <= cn::icsf_max_levels() &&
+// for IC(0) solves of k = 1 or 3 columns unless CLASSIC asks for the
+// level-scheduled kernel: in mixed precision always, in FP64 from 50,000
+// free rows on or when SINGLE asks for it (on B200 the FP64 form, two words
+// a value, beat the level-scheduled kernel on the 130k-row torus by 9 % and
+// lost by 3-12 % on 5k-18k-row meshes).  k = 9 stays on the level-scheduled
+// kernel in one launch: both are bound by latency, and three k = 3 solves
+// would take about three times one.
+bool icsf_wanted(const cn_system* S, int k, const cn_solve_opts& o) {
+  return !S->hsc && S->opts.precond == CN_PRECOND_IC0 && (k == 1 || k == 3) && o.algo != CN_ALGO_CLASSIC &&
+         o.algo != CN_ALGO_PLAIN && S->H.nlev <= cn::icsf_max_levels() &&
          (o.precision == CN_PREC_MIXED || S->H.n >= 50000 || o.algo == CN_ALGO_SINGLE);
 }
 
@@ -131,7 +133,7 @@ bool icsf_wanted(const cn_system* S, const cn_solve_opts& o) {
 // (all SMs); 256 threads a block below 20,000 rows.  Measured on B200 across
 // 2k-1M-row tori and cylinders: one block took 1.3-5x longer than these
 // grids from 2k rows on.
-void ic0_shape(const cn_system* S, const cn_solve_opts& o, int* grid, int* block) {
+void ic0_shape(const cn_system* S, int k, const cn_solve_opts& o, int* grid, int* block) {
   *grid = S->grid;
   *block = S->block;
   if (S->hsc || S->opts.precond != CN_PRECOND_IC0 || S->shape_set || S->opts.grid > 0 || S->opts.block > 0 ||
@@ -139,7 +141,7 @@ void ic0_shape(const cn_system* S, const cn_solve_opts& o, int* grid, int* block
     return;
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, S->device);
-  const bool sync_free = icsf_wanted(S, o);
+  const bool sync_free = icsf_wanted(S, k, o);
   const int per = sync_free ? 600 : 120;
   const int cap = sync_free && S->H.n < 300000 ? std::max(8, sms * 7 / 8) : sms;
   *grid = std::min(cap, std::max(8, S->H.n / per));
@@ -147,10 +149,10 @@ void ic0_shape(const cn_system* S, const cn_solve_opts& o, int* grid, int* block
 }
 
 // ... on a multi-block grid
-bool icsf_path(const cn_system* S, const cn_solve_opts& o) {
+bool icsf_path(const cn_system* S, int k, const cn_solve_opts& o) {
   int grid = 0, block = 0;
-  ic0_shape(S, o, &grid, &block);
-  return icsf_wanted(S, o) && grid > 1;
+  ic0_shape(S, k, o, &grid, &block);
+  return icsf_wanted(S, k, o) && grid > 1;
 }
 
 const char* kStatusText[] = {"ok", "max_iter", "singular_component", "nonpositive_pivot",
@@ -543,10 +545,8 @@ cn_status cn_solve_device(cn_handle S, int32_t k, const double* d_targets, doubl
   }
   // The row-cached Jacobi kernel runs k = 9 as three k = 3 solves on column
   // slices: its k = 9 state fits neither shared memory nor registers, and
-  // three k = 3 solves take a third of the time of one k = 9 solve.  The
-  // IC(0) solve without grid barriers does the same (its k = 9 gathers would
-  // hold 36 words of the neighbour rows in registers).
-  if (k == 9 && (row_cached(S) || icsf_path(S, o)) && o.algo != CN_ALGO_PLAIN && S->d_split_t &&
+  // three k = 3 solves take a third of the time of one k = 9 solve.
+  if (k == 9 && row_cached(S) && o.algo != CN_ALGO_PLAIN && S->d_split_t &&
       o.tol > 0.0 && o.max_iter >= 0 && o.max_refine >= 1) {
     CN_CUDA(cudaSetDevice(S->device));
     const int rows_t = o.mode == CN_MODE_RHS ? S->H.n : S->H.nh;
@@ -765,11 +765,11 @@ cn_status cn_solve_device(cn_handle S, int32_t k, const double* d_targets, doubl
     return fill_stats(S, k, stats);
   }
   int grid = S->grid, lblock = S->block;
-  ic0_shape(S, o, &grid, &lblock);
+  ic0_shape(S, k, o, &grid, &lblock);
   // IC(0) on a multi-block grid: the sweeps without grid barriers (tagged
   // words) under the single-reduction CG (icsf_wanted: mixed precision, or
   // FP64 on a large system); otherwise the level-scheduled kernel
-  if (icsf_path(S, o)) {
+  if (icsf_path(S, k, o)) {
     const int block = std::min(lblock, 512);
     const int mg = cn::icsf_max_grid(o.precision, k, block);
     if (mg <= 0) {
