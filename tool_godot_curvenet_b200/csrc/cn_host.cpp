@@ -112,46 +112,70 @@ bool row_cached(const cn_system* S) {
 
 // The IC(0) solve without grid barriers in the sweeps (cn_icsf.cu) is used
 // for IC(0) solves of k = 1 or 3 columns unless CLASSIC asks for the
-// level-scheduled kernel: in mixed precision always, in FP64 from 50,000
-// free rows on or when SINGLE asks for it (on B200 the FP64 form, two words
-// a value, beat the level-scheduled kernel on the 130k-row torus by 9 % and
-// lost by 3-12 % on 5k-18k-row meshes).  k = 9 stays on the level-scheduled
-// kernel in one launch: both are bound by latency, and three k = 3 solves
-// would take about three times one.
+// level-scheduled kernel: in mixed precision below 500,000 free rows, in
+// FP64 from 50,000 to 500,000, and whenever SINGLE asks for it.  Measured on
+// B200: the FP64 form (two words a value) beat the level-scheduled kernel on
+// the 130k-row torus by 9 % and lost by 3-12 % on 5k-18k-row meshes; on the
+// 1.05M-row torus the level-scheduled kernel with 1,024-thread blocks beat
+// both forms (mixed 30.2 ms against 46.1 ms, FP64 46.7 against 64 ms).
+// k = 9 stays on the level-scheduled kernel in one launch: both are bound by
+// latency, and three k = 3 solves would take about three times one.
+constexpr int kLargeRows = 500000;
+
 bool icsf_wanted(const cn_system* S, int k, const cn_solve_opts& o) {
-  return !S->hsc && S->opts.precond == CN_PRECOND_IC0 && (k == 1 || k == 3) && o.algo != CN_ALGO_CLASSIC &&
-         o.algo != CN_ALGO_PLAIN && S->H.nlev <= cn::icsf_max_levels() &&
-         (o.precision == CN_PREC_MIXED || S->H.n >= 50000 || o.algo == CN_ALGO_SINGLE);
+  if (S->hsc || S->opts.precond != CN_PRECOND_IC0 || (k != 1 && k != 3) || o.algo == CN_ALGO_CLASSIC ||
+      o.algo == CN_ALGO_PLAIN || S->H.nlev > cn::icsf_max_levels())
+    return false;
+  if (o.algo == CN_ALGO_SINGLE) return true;
+  const int n = S->H.n;
+  return n < kLargeRows && (o.precision == CN_PREC_MIXED || n >= 50000);
 }
 
-// Launch shape of an IC(0) solve: the handle's (explicit, tuned, or one
-// block for a small system), or, left automatic on a system of at least 1,024
-// free rows, a grid sized by the system and the kernel: about 600 rows a
-// block for the sweeps without grid barriers (below 300,000 rows at most 7/8
-// of the SMs: fewer blocks keep more of a level's rows in each; the
-// 1.05M-row torus wants every SM), about 120 for the level-scheduled kernel
-// (all SMs); 256 threads a block below 20,000 rows.  Measured on B200 across
-// 2k-1M-row tori and cylinders: one block took 1.3-5x longer than these
-// grids from 2k rows on.
-void ic0_shape(const cn_system* S, int k, const cn_solve_opts& o, int* grid, int* block) {
+// Launch shape of a level-scheduled or IC(0) solve: the handle's where the
+// caller fixed it (build options, cn_set_launch, the tuner) or for a system
+// of fewer than 1,024 rows (one block); otherwise sized by the system and
+// the kernel, from measurements on B200 across 2k-1M-row tori and cylinders
+// (one block took 1.3-5x longer than these grids from 2k rows on):
+// * the IC(0) sweeps without grid barriers: about 600 rows a block (below
+//   300,000 rows at most 7/8 of the SMs: fewer blocks keep more of a
+//   level's rows in each), 256 threads a block below 20,000 rows, else 512;
+// * the level-scheduled kernel, IC(0): about 120 rows a block, the same block
+//   sizes, the handle's lanes per row; from 500,000 rows every SM with
+//   1,024-thread blocks, one lane per row in mixed precision (two in FP64);
+// * HSC: one lane per row (the V-cycle's R and P rows are short), 1,024-thread
+//   blocks from 500,000 rows.
+void solve_shape(const cn_system* S, int k, const cn_solve_opts& o, int* grid, int* block, int* lanes) {
   *grid = S->grid;
   *block = S->block;
-  if (S->hsc || S->opts.precond != CN_PRECOND_IC0 || S->shape_set || S->opts.grid > 0 || S->opts.block > 0 ||
-      S->H.n < 1024)
-    return;
+  *lanes = S->lanes;
+  if (S->shape_set || S->opts.grid > 0 || S->opts.block > 0 || S->H.n < 1024) return;
+  const int n = S->H.n;
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, S->device);
-  const bool sync_free = icsf_wanted(S, k, o);
-  const int per = sync_free ? 600 : 120;
-  const int cap = sync_free && S->H.n < 300000 ? std::max(8, sms * 7 / 8) : sms;
-  *grid = std::min(cap, std::max(8, S->H.n / per));
-  *block = S->H.n >= 20000 ? 512 : 256;
+  if (S->hsc) {
+    if (S->opts.lanes <= 0) *lanes = 1;
+    if (n >= kLargeRows) *block = 1024;
+    return;
+  }
+  if (S->opts.precond != CN_PRECOND_IC0) return;
+  if (icsf_wanted(S, k, o)) {
+    const int cap = n < 300000 ? std::max(8, sms * 7 / 8) : sms;
+    *grid = std::min(cap, std::max(8, n / 600));
+    *block = n >= 20000 ? 512 : 256;
+  } else if (n >= kLargeRows) {
+    *grid = sms;
+    *block = 1024;
+    if (S->opts.lanes <= 0) *lanes = o.precision == CN_PREC_MIXED ? 1 : 2;
+  } else {
+    *grid = std::min(sms, std::max(8, n / 120));
+    *block = n >= 20000 ? 512 : 256;
+  }
 }
 
 // ... on a multi-block grid
 bool icsf_path(const cn_system* S, int k, const cn_solve_opts& o) {
-  int grid = 0, block = 0;
-  ic0_shape(S, k, o, &grid, &block);
+  int grid = 0, block = 0, lanes = 0;
+  solve_shape(S, k, o, &grid, &block, &lanes);
   return icsf_wanted(S, k, o) && grid > 1;
 }
 
@@ -764,8 +788,8 @@ cn_status cn_solve_device(cn_handle S, int32_t k, const double* d_targets, doubl
     if (!stats) return CN_OK;
     return fill_stats(S, k, stats);
   }
-  int grid = S->grid, lblock = S->block;
-  ic0_shape(S, k, o, &grid, &lblock);
+  int grid = S->grid, lblock = S->block, llanes = S->lanes;
+  solve_shape(S, k, o, &grid, &lblock, &llanes);
   // IC(0) on a multi-block grid: the sweeps without grid barriers (tagged
   // words) under the single-reduction CG (icsf_wanted: mixed precision, or
   // FP64 on a large system); otherwise the level-scheduled kernel
@@ -788,9 +812,9 @@ cn_status cn_solve_device(cn_handle S, int32_t k, const double* d_targets, doubl
     return fill_stats(S, k, stats);
   }
   if (grid > 1) {
-    const int mg = cn::persistent_max_grid(o.precision, k, S->lanes, lblock);
+    const int mg = cn::persistent_max_grid(o.precision, k, llanes, lblock);
     if (mg <= 0) {
-      set_err("the persistent solve does not fit on this device (lanes %d, block %d)", S->lanes, lblock);
+      set_err("the persistent solve does not fit on this device (lanes %d, block %d)", llanes, lblock);
       return CN_CUDA_ERROR;
     }
     grid = std::min(std::min(grid, mg), S->max_grid_alloc);
@@ -803,7 +827,7 @@ cn_status cn_solve_device(cn_handle S, int32_t k, const double* d_targets, doubl
   }
   CN_CUDA(cudaMemsetAsync(S->d_ctl, 0, sizeof(Control), S->stream));
   CN_CUDA(cudaEventRecord(S->ev0, S->stream));
-  CN_CUDA(cn::launch_persistent_solve(a, o.precision, k, S->lanes, lblock, grid, S->stream));
+  CN_CUDA(cn::launch_persistent_solve(a, o.precision, k, llanes, lblock, grid, S->stream));
   CN_CUDA(cudaEventRecord(S->ev1, S->stream));
   S->have_solution = true;
   if (!stats) return CN_OK;
