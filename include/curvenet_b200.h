@@ -75,12 +75,13 @@ enum { CN_MODE_HARMONIC = 0, CN_MODE_DEFORM = 1, CN_MODE_RHS = 2 };
  * the pipelined CG keeping u = M^-1 r and q = M^-1 s by recurrence, inner
  * solves of at most 1e-3 restarted by the FP64 refinement, with the same
  * fall-back; in FP64 the two-reduction CG.  With IC(0) and k = 1 or 3 on a
- * multi-block grid, in mixed precision and in FP64 from 50,000 free rows on: the
- * triangular sweeps without grid barriers (every published value carries
- * the number of the preconditioner application it belongs to; block
- * barriers between levels) under the single-reduction CG, one grid barrier
- * per iteration; otherwise (smaller FP64 systems, one block) the
- * level-scheduled kernel.  With HSC: the level-scheduled kernel.  CLASSIC:
+ * multi-block grid below 500,000 free rows, in mixed precision and in FP64
+ * from 50,000 rows: the triangular sweeps without grid barriers (every
+ * published value carries the number of the preconditioner application it
+ * belongs to; block barriers between levels) under the single-reduction CG,
+ * one grid barrier per iteration; otherwise (smaller FP64 systems, systems
+ * from 500,000 rows, k = 9, one block) the level-scheduled kernel.  With
+ * HSC: the level-scheduled kernel.  CLASSIC:
  * the two-reduction CG (row-cached kernel; IC(0): the level-scheduled
  * kernel).  PIPELINED: the pipelined CG without fall-back (Jacobi in both
  * precisions, block SSOR in mixed precision).  PLAIN: one kernel per

@@ -52,7 +52,7 @@ def test_sync_free_ic0_matches_oracle_and_level_scheduled(name, kw, k, oracle):
         rt = s.solve(t, mode="harmonic", precision="mixed", tol=1e-11, max_iter=20000)
         rc = s.solve(t, mode="harmonic", precision="mixed", tol=1e-8, max_iter=20000, algo="classic")
         # FP64 takes the sweeps without grid barriers by default from 50,000
-        # rows on; SINGLE asks for them on any size
+        # to 500,000 rows; SINGLE asks for them on any size
         r64 = s.solve(t, mode="harmonic", precision="fp64", tol=1e-13, max_iter=20000, algo="single")
     for r in (rf, rs, rt, rc, r64):
         assert r.status == L.CN_OK
